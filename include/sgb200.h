@@ -1,0 +1,215 @@
+/*
+ * sgb200.h -- C ABI of the B200-native SparseGridGpu hot path.
+ *
+ * A drop-in for openfpm_data's sparse block grid pipeline (insert -> flush into
+ * the block map -> findNeighbours / tagBoundaries -> applyStencils over chunks
+ * with one-point halos).  Every entry point takes plain pointers and sizes,
+ * returns an sgb_status, and runs on the CUDA stream it is given (NULL = the
+ * legacy default stream).  Device pointers are marked "dev", host pointers
+ * "host".  Handles are not thread safe; one handle is used by one host thread
+ * at a time.
+ *
+ * Block-map layout (identical to the reference's memory_traits_inte layout):
+ *   index[n]                int64 chunk ids, sorted ascending
+ *   data_p[(n+1) * bs]      one array per property, chunk major; position n
+ *                           holds the background chunk
+ *   mask[(n+1) * bs]        uint8 per point: bit0 EXIST, bit1 PADDING
+ * with bs = edge^dim points per chunk and the point at local coordinates
+ * (x,y,z) of a chunk at offset x + edge*(y + edge*z).
+ *
+ * Citations name the reference interface each entry point replaces (paths
+ * inside the openfpm_data project).
+ */
+#ifndef SGB200_H
+#define SGB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct sgb_grid sgb_grid;
+typedef struct sgb_batch sgb_batch;
+typedef void* sgb_stream; /* cudaStream_t */
+
+typedef enum {
+    SGB_OK = 0,
+    SGB_EINVAL = 1,   /* bad argument */
+    SGB_ECUDA = 2,    /* CUDA runtime error (see sgb_last_error_string) */
+    SGB_ENOMEM = 3,   /* device allocation failed */
+    SGB_ERANGE = 4,   /* a point lies outside the grid domain */
+    SGB_ESTATE = 5,   /* call not valid in the current state */
+    SGB_ETIMEOUT = 6, /* a device-side bounded wait gave up */
+    SGB_ENOTSUP = 7   /* configuration not supported by this build */
+} sgb_status;
+
+typedef enum { SGB_F32 = 0, SGB_I32 = 1, SGB_F64 = 2, SGB_U8 = 3 } sgb_type;
+
+/* Flush reduction operators: sRight_, sLeft_, sadd_, smax_, smin_,
+ * sBitwiseOr_ (src/Vector/cuda/map_vector_sparse_cuda_kernels.cuh:51-352).
+ * SGB_OP_NONE leaves the property out of the flush. */
+typedef enum {
+    SGB_OP_NONE = 0,
+    SGB_OP_RIGHT = 1,
+    SGB_OP_LEFT = 2,
+    SGB_OP_ADD = 3,
+    SGB_OP_MAX = 4,
+    SGB_OP_MIN = 5,
+    SGB_OP_OR = 6
+} sgb_op;
+
+/* Neighbourhoods: NNStar (faces) and NNFull (3^dim box)
+ * (src/SparseGridGpu/SparseGridGpu_ker_util.hpp:86-167,
+ *  src/SparseGridGpu/SparseGridGpu.hpp:261-360). */
+typedef enum { SGB_NN_STAR = 0, SGB_NN_FULL = 1 } sgb_nn;
+
+/* Fixed-function stencils.
+ *  SGB_HEAT7 : HeatStencil<3,src,dst> (src/SparseGridGpu/tests/utils/
+ *              SparseGridGpu_util_test.cuh:201-345); params {dt}; writes the
+ *              whole destination chunk.
+ *  SGB_GS7   : Gray-Scott written as a conv2_b user function
+ *              (src/SparseGridGpu/SparseGridGpu.hpp:2627-2645); src {u,v},
+ *              dst {u',v'}, params {Du, Dv, F, k, dt}; writes active points.
+ *  SGB_BOX27 : Conv3x3x3<3,src,dst> (src/SparseGridGpu/tests/
+ *              SparseGridGpu_tests.cu:887-952); params = 27 coefficients
+ *              c[i][j][k], i along x; writes active points; NNFull halo. */
+typedef enum { SGB_HEAT7 = 0, SGB_GS7 = 1, SGB_BOX27 = 2 } sgb_stencil;
+
+const char* sgb_status_string(int status);
+const char* sgb_last_error_string(void);
+int sgb_version(void);
+
+/* ---------------------------------------------------------------- grids */
+
+/* SparseGridGpu(const size_t (&res)[dim], stencilSupportRadius = 1)
+ * (src/SparseGridGpu/SparseGridGpu.hpp:1694-1698).  dim == 3, edge 4 or 8,
+ * at most 8 properties. */
+int sgb_create(sgb_grid** out, int dim, int edge, const int64_t* size, int nprop, const int* prop_types,
+               int device);
+int sgb_destroy(sgb_grid* g);
+
+/* setBackgroundValue<p> (SparseGridGpu.hpp:2878-2884); value host. */
+int sgb_set_background(sgb_grid* g, int prop, const void* value_host);
+
+/* Device-side insert<p>(coord) for a batch of points
+ * (src/SparseGridGpu/SparseGridGpu_ker.cuh:446-450 ->
+ *  src/Vector/cuda/map_vector_sparse_cuda_ker.cuh:309-318).
+ * coords dev int32 [n][3]; values[p] dev, one array of n elements per
+ * property (NULL entries leave that property out).  Points are staged in
+ * insertion order until sgb_flush. */
+int sgb_insert(sgb_grid* g, int64_t n, const int32_t* coords_dev, const void* const* values_dev, sgb_stream s);
+
+/* The same with linearised point ids (grid_smb::LinId,
+ * src/Grid/Geometry/grid_smb.hpp:176-190): BlockMapGpu::insert<p>(linId)
+ * (src/SparseGridGpu/BlockMapGpu.hpp:137-150). */
+int sgb_insert_lin(sgb_grid* g, int64_t n, const int64_t* lin_dev, const void* const* values_dev, sgb_stream s);
+
+/* flush<v_reduce...>(ctx, FLUSH_ON_DEVICE) (SparseGridGpu.hpp:772-779,
+ * BlockMapGpu.hpp:289-299, src/Vector/map_vector_sparse.hpp:1784-1795).
+ * ops[nprop]: one sgb_op per property.  Duplicates of one point are reduced
+ * in insertion order, A = first, A = op(A, next); a point that already
+ * exists is then reduced as op(A, old); masks are OR-ed. */
+int sgb_flush(sgb_grid* g, const int* ops_host, sgb_stream s);
+
+/* findNeighbours<NN>() (SparseGridGpu.hpp:2396-2420). */
+int sgb_find_neighbours(sgb_grid* g, int nn, sgb_stream s);
+
+/* Neighbour table in the reference's nn_blocks format (host int64
+ * [n][nNN], nNN = 8 for NNStar, 27 for NNFull): data position of the
+ * neighbour chunk, n when it is absent, -1 in the unused NNStar slots. */
+int sgb_neighbour_table(sgb_grid* g, int nn, int64_t* out_host, sgb_stream s);
+
+/* tagBoundaries<NN>(ctx) (SparseGridGpu.hpp:2290-2394). */
+int sgb_tag_boundaries(sgb_grid* g, int nn, sgb_stream s);
+
+/* applyStencils<S>(box, STENCIL_MODE_INPLACE, args...)
+ * (SparseGridGpu.hpp:2704-2734, 954-1048).  src/dst host arrays of property
+ * ids (1 entry for HEAT7/BOX27, 2 for GS7); params host floats; box host
+ * int64 {lo[3], hi[3]} inclusive, or NULL for the whole grid. */
+int sgb_apply_stencil(sgb_grid* g, int kind, const int* src, const int* dst, const float* params, int nparams,
+                      const int64_t* box, sgb_stream s);
+
+/* nsteps stencil applications alternating src->dst and dst->src (the
+ * reference's ping-pong loop, src/SparseGridGpu/tests/
+ * SparseGridGpu_tests.cu:499-503), launched as one captured CUDA graph.
+ * On return *final_is_dst is 1 when the last step wrote the dst properties. */
+int sgb_run_steps(sgb_grid* g, int kind, const int* src, const int* dst, const float* params, int nparams,
+                  int nsteps, int use_graph, int* final_is_dst, sgb_stream s);
+
+/* Number of chunks (private_get_index_array().size()). */
+int sgb_nchunks(const sgb_grid* g, int64_t* n);
+
+/* Non-owning device views (private_get_index_array / private_get_data_array,
+ * SparseGridGpu.hpp:1959-1990).  Invalidated by sgb_flush. */
+int sgb_index_buffer(sgb_grid* g, const int64_t** dev);
+int sgb_data_buffer(sgb_grid* g, int prop, void** dev);
+int sgb_mask_buffer(sgb_grid* g, uint8_t** dev);
+
+/* Build the block map directly from host arrays (hostToDevice of a map laid
+ * out as above, without the background chunk), replacing the current one.
+ * A NULL data_host[p] fills property p with its background value. */
+int sgb_load_map(sgb_grid* g, int64_t n, const int64_t* keys_host, const void* const* data_host,
+                 const uint8_t* mask_host, sgb_stream s);
+
+/* The same from device arrays. */
+int sgb_load_map_dev(sgb_grid* g, int64_t n, const int64_t* keys_dev, const void* const* data_dev,
+                     const uint8_t* mask_dev, sgb_stream s);
+
+/* deviceToHost: copy keys[n], data_p[(n+1)*bs] and mask[(n+1)*bs] to host
+ * (any pointer may be NULL to skip it). */
+int sgb_download_map(sgb_grid* g, int64_t* keys_host, void* const* data_host, uint8_t* mask_host, sgb_stream s);
+
+/* countExistingElements / countBoundaryElements (SparseGridGpu.hpp:2422-2474). */
+int sgb_count_existing(sgb_grid* g, int64_t* existing, int64_t* padding, sgb_stream s);
+
+/* get<p>(coord) for a batch of points (SparseGridGpu_ker.cuh:409-413):
+ * value if the point exists, background otherwise.  coords dev int32 [n][3],
+ * out dev n elements of the property's type. */
+int sgb_get(sgb_grid* g, int64_t n, const int32_t* coords_dev, int prop, void* out_dev, sgb_stream s);
+
+/* Device-side error word of the last kernels (bounded waits that gave up,
+ * out-of-domain inserts).  Synchronises the stream; clears the word. */
+int sgb_check_device_errors(sgb_grid* g, sgb_stream s);
+
+/* Bytes of device memory held by the grid. */
+int sgb_device_bytes(const sgb_grid* g, int64_t* bytes);
+
+/* Stencil launch configuration: CTAs per SM (1..4) and staging depth
+ * (3..8 chunks in flight per CTA); 0 keeps the current value. */
+int sgb_set_launch_config(sgb_grid* g, int ctas_per_sm, int stages);
+
+/* ---------------------------------------------------------------- batches
+ * Many independent grids advanced by one persistent launch per step over
+ * their concatenated block maps (no reference counterpart: the reference
+ * launches one applyStencils per grid).  All member grids share dim, edge,
+ * property types and stencil kind; each keeps its own parameters and
+ * background values. */
+int sgb_batch_create(sgb_batch** out, int device);
+int sgb_batch_destroy(sgb_batch* b);
+/* Copy a grid's block map and its src/dst properties into the batch; the
+ * grid will take part in the next `nsteps` batch steps (ping-pong src->dst,
+ * dst->src, ...) and then stay idle.  params as for sgb_apply_stencil
+ * (HEAT7 or GS7, no box).  Returns the slot id. */
+int sgb_batch_add(sgb_batch* b, sgb_grid* g, int kind, const int* src, const int* dst, const float* params,
+                  int nparams, int64_t nsteps, int* slot, sgb_stream s);
+/* Drop a slot; its chunks are compacted away before the next step. */
+int sgb_batch_remove(sgb_batch* b, int slot, sgb_stream s);
+/* Advance the batch by nsteps global steps: one persistent launch per step
+ * over all chunks, captured as one CUDA graph when use_graph != 0. */
+int sgb_batch_step(sgb_batch* b, int nsteps, int use_graph, sgb_stream s);
+/* Steps a slot has done so far (<= its nsteps). */
+int sgb_batch_slot_steps(const sgb_batch* b, int slot, int64_t* done);
+/* Copy a slot's fields back into g's src/dst properties (g must have the
+ * block map the slot was added from); *final_is_dst as in sgb_run_steps. */
+int sgb_batch_extract(sgb_batch* b, int slot, sgb_grid* g, int* final_is_dst, sgb_stream s);
+int sgb_batch_info(const sgb_batch* b, int* ngrids, int64_t* nchunks, int64_t* bytes);
+/* Launch configuration of the batched kernels (as sgb_set_launch_config). */
+int sgb_batch_set_launch_config(sgb_batch* b, int ctas_per_sm, int stages);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SGB200_H */

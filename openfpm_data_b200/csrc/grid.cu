@@ -1,0 +1,499 @@
+// Grid handles, buffers, map upload/download, staged inserts and point reads.
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "common.cuh"
+#include "internal.h"
+
+namespace sgb {
+
+static thread_local std::string g_last_error;
+
+void set_error(const std::string& msg) { g_last_error = msg; }
+
+int cuda_status(cudaError_t e, const char* what) {
+    set_error(std::string(what) + ": " + cudaGetErrorString(e));
+    if (e == cudaErrorMemoryAllocation) {
+        cudaGetLastError();
+        return SGB_ENOMEM;
+    }
+    return SGB_ECUDA;
+}
+
+int DevBuf::reserve(size_t need) {
+    if (need <= bytes) return SGB_OK;
+    size_t nb = need + need / 2 + 256;
+    void* q = nullptr;
+    cudaError_t e = cudaMalloc(&q, nb);
+    if (e != cudaSuccess) return cuda_status(e, "cudaMalloc");
+    if (p && bytes) {
+        e = cudaMemcpy(q, p, bytes, cudaMemcpyDeviceToDevice);
+        if (e != cudaSuccess) {
+            cudaFree(q);
+            return cuda_status(e, "cudaMemcpy(grow)");
+        }
+    }
+    if (p) cudaFree(p);
+    p = q;
+    bytes = nb;
+    return SGB_OK;
+}
+
+int DevBuf::ensure(size_t need) {
+    if (need <= bytes) return SGB_OK;
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+    size_t nb = need + need / 4 + 256;
+    cudaError_t e = cudaMalloc(&p, nb);
+    if (e != cudaSuccess) {
+        p = nullptr;
+        return cuda_status(e, "cudaMalloc");
+    }
+    bytes = nb;
+    return SGB_OK;
+}
+
+void DevBuf::release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+}
+
+int HostScratch::ensure(size_t need) {
+    if (need <= bytes) return SGB_OK;
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    bytes = 0;
+    cudaError_t e = cudaMallocHost(&p, need);
+    if (e != cudaSuccess) return cuda_status(e, "cudaMallocHost");
+    bytes = need;
+    return SGB_OK;
+}
+
+void HostScratch::release() {
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    bytes = 0;
+}
+
+// Fill `count` elements of `esize` bytes with one pattern.
+__global__ void k_fill(unsigned char* dst, int64_t count, int esize, uint64_t pattern) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (; i < count; i += stride) {
+        if (esize == 4) reinterpret_cast<uint32_t*>(dst)[i] = (uint32_t)pattern;
+        else if (esize == 8) reinterpret_cast<uint64_t*>(dst)[i] = pattern;
+        else dst[i] = (unsigned char)pattern;
+    }
+}
+
+static int fill(void* dst, int64_t count, int esize, uint64_t pattern, cudaStream_t s) {
+    if (count <= 0) return SGB_OK;
+    int64_t blocks = (count + 255) / 256;
+    if (blocks > 4096) blocks = 4096;
+    k_fill<<<(unsigned)blocks, 256, 0, s>>>((unsigned char*)dst, count, esize, pattern);
+    SGB_CUDA(cudaGetLastError());
+    return SGB_OK;
+}
+
+static uint64_t bck_pattern(const sgb_grid* g, int p) {
+    uint64_t v = 0;
+    std::memcpy(&v, g->bck[p], elem_size(g->ptype[p]));
+    return v;
+}
+
+int write_background(sgb_grid* g, int64_t pos, cudaStream_t s, DevBuf* data, DevBuf& mask) {
+    const int bs = g->geo.bs;
+    for (int p = 0; p < g->nprop; ++p) {
+        int es = elem_size(g->ptype[p]);
+        SGB_TRY(fill(data[p].as<unsigned char>() + (size_t)pos * bs * es, bs, es, bck_pattern(g, p), s));
+    }
+    SGB_CUDA(cudaMemsetAsync(mask.as<unsigned char>() + (size_t)pos * bs, 0, bs, s));
+    return SGB_OK;
+}
+
+int grid_reserve(sgb_grid* g, int64_t chunks, bool keep) {
+    if (chunks <= g->cap && g->keys.p) return SGB_OK;
+    int64_t nc = chunks;
+    if (nc < g->cap + g->cap / 2) nc = g->cap + g->cap / 2;
+    if (nc < 16) nc = 16;
+    const int bs = g->geo.bs;
+    if (keep) {
+        SGB_TRY(g->keys.reserve((size_t)nc * 8));
+        for (int p = 0; p < g->nprop; ++p)
+            SGB_TRY(g->data[p].reserve((size_t)(nc + 1) * bs * elem_size(g->ptype[p])));
+        SGB_TRY(g->mask.reserve((size_t)(nc + 1) * bs));
+    } else {
+        SGB_TRY(g->keys.ensure((size_t)nc * 8));
+        for (int p = 0; p < g->nprop; ++p)
+            SGB_TRY(g->data[p].ensure((size_t)(nc + 1) * bs * elem_size(g->ptype[p])));
+        SGB_TRY(g->mask.ensure((size_t)(nc + 1) * bs));
+    }
+    g->cap = nc;
+    return SGB_OK;
+}
+
+static void invalidate_derived(sgb_grid* g) {
+    g->nn_valid[0] = g->nn_valid[1] = false;
+    g->bits_valid = false;
+}
+
+// grid_smb::LinId on device (src/Grid/Geometry/grid_smb.hpp:176-190), with a
+// domain check that the reference does not do.
+__global__ void k_lin_from_coords(const int32_t* coords, int64_t n, Geometry geo, int64_t* lin, unsigned* err) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int64_t c[3];
+    bool ok = true;
+    for (int d = 0; d < geo.dim; ++d) {
+        c[d] = coords[i * geo.dim + d];
+        ok &= c[d] >= 0 && c[d] < geo.size[d];
+    }
+    if (!ok) {
+        atomicOr(err, kErrOutOfDomain);
+        lin[i] = -1;
+        return;
+    }
+    int64_t b = c[geo.dim - 1] / geo.edge, l = c[geo.dim - 1] % geo.edge;
+    for (int d = geo.dim - 2; d >= 0; --d) {
+        b = b * geo.bsz[d] + c[d] / geo.edge;
+        l = l * geo.edge + c[d] % geo.edge;
+    }
+    lin[i] = b * geo.bs + l;
+}
+
+__global__ void k_check_lin(const int64_t* lin_in, int64_t n, int64_t maxlin, int64_t* lin_out, unsigned* err) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int64_t v = lin_in[i];
+    if (v < 0 || v >= maxlin) {
+        atomicOr(err, kErrOutOfDomain);
+        v = -1;
+    }
+    lin_out[i] = v;
+}
+
+static int stage_values(sgb_grid* g, int64_t n, const void* const* values, cudaStream_t s) {
+    for (int p = 0; p < g->nprop; ++p) {
+        const int es = elem_size(g->ptype[p]);
+        SGB_TRY(g->pend_val[p].reserve((size_t)(g->npend + n) * es));
+        unsigned char* dst = g->pend_val[p].as<unsigned char>() + (size_t)g->npend * es;
+        if (values && values[p]) {
+            SGB_CUDA(cudaMemcpyAsync(dst, values[p], (size_t)n * es, cudaMemcpyDeviceToDevice, s));
+            g->pend_has[p] = true;
+        } else {
+            SGB_TRY(fill(dst, n, es, bck_pattern(g, p), s));
+        }
+    }
+    return SGB_OK;
+}
+
+template <typename T>
+__global__ void k_get(const int32_t* coords, int64_t n, Geometry geo, const int64_t* keys, int64_t nchunks,
+                      const T* data, const uint8_t* mask, T* out) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int64_t c[3];
+    for (int d = 0; d < geo.dim; ++d) c[d] = coords[i * geo.dim + d];
+    int64_t b = c[geo.dim - 1] / geo.edge, l = c[geo.dim - 1] % geo.edge;
+    for (int d = geo.dim - 2; d >= 0; --d) {
+        b = b * geo.bsz[d] + c[d] / geo.edge;
+        l = l * geo.edge + c[d] % geo.edge;
+    }
+    int64_t pos = find_key(keys, nchunks, b);
+    if (pos < 0) pos = nchunks;
+    // BlockMapGpu_ker::get (src/SparseGridGpu/BlockMapGpu_ker.cuh:117-135)
+    const size_t idx = (size_t)pos * geo.bs + l;
+    out[i] = (mask[idx] & 1) ? data[idx] : data[(size_t)nchunks * geo.bs + l];
+}
+
+__global__ void k_count(const uint8_t* mask, int64_t total, unsigned long long* out) {
+    unsigned long long e = 0, p = 0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+        uint8_t m = mask[i];
+        e += m & 1;
+        p += (m & 1) && (m & 2);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        e += __shfl_down_sync(0xffffffffu, e, o);
+        p += __shfl_down_sync(0xffffffffu, p, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(out, e);
+        atomicAdd(out + 1, p);
+    }
+}
+
+}  // namespace sgb
+
+using namespace sgb;
+
+extern "C" {
+
+const char* sgb_status_string(int s) {
+    switch (s) {
+        case SGB_OK: return "ok";
+        case SGB_EINVAL: return "invalid argument";
+        case SGB_ECUDA: return "CUDA error";
+        case SGB_ENOMEM: return "out of device memory";
+        case SGB_ERANGE: return "point outside the grid domain";
+        case SGB_ESTATE: return "invalid state";
+        case SGB_ETIMEOUT: return "device wait timed out";
+        case SGB_ENOTSUP: return "not supported";
+        default: return "unknown status";
+    }
+}
+
+const char* sgb_last_error_string(void) { return g_last_error.c_str(); }
+
+int sgb_version(void) { return 10000; }
+
+int sgb_create(sgb_grid** out, int dim, int edge, const int64_t* size, int nprop, const int* prop_types, int device) {
+    if (!out || !size || (nprop > 0 && !prop_types)) return SGB_EINVAL;
+    *out = nullptr;
+    if (dim != 3) {
+        set_error("only dim == 3 grids are supported on the device");
+        return SGB_ENOTSUP;
+    }
+    if (edge != 4 && edge != 8) {
+        set_error("chunk edge must be 4 or 8");
+        return SGB_ENOTSUP;
+    }
+    if (nprop < 1 || nprop > kMaxProps) return SGB_EINVAL;
+    for (int p = 0; p < nprop; ++p)
+        if (prop_types[p] < SGB_F32 || prop_types[p] > SGB_U8) return SGB_EINVAL;
+    for (int d = 0; d < dim; ++d)
+        if (size[d] <= 0) return SGB_EINVAL;
+    SGB_CUDA(cudaSetDevice(device));
+    sgb_grid* g = new sgb_grid();
+    g->device = device;
+    g->geo.dim = dim;
+    g->geo.edge = edge;
+    g->geo.bs = edge * edge * edge;
+    for (int d = 0; d < 3; ++d) {
+        g->geo.size[d] = d < dim ? size[d] : 1;
+        g->geo.bsz[d] = g->geo.size[d] / edge + ((g->geo.size[d] % edge) != 0);  // grid_smb.hpp:48-57
+    }
+    g->nprop = nprop;
+    for (int p = 0; p < nprop; ++p) g->ptype[p] = prop_types[p];
+    cudaDeviceGetAttribute(&g->num_sms, cudaDevAttrMultiProcessorCount, device);
+    int st = grid_reserve(g, 16, false);
+    if (st == SGB_OK) st = g->err.ensure(16);
+    if (st == SGB_OK && cudaMemset(g->err.p, 0, 16) != cudaSuccess) st = SGB_ECUDA;
+    if (st == SGB_OK) st = write_background(g, 0, 0, g->data, g->mask);
+    if (st == SGB_OK) st = cudaDeviceSynchronize() == cudaSuccess ? SGB_OK : SGB_ECUDA;
+    if (st != SGB_OK) {
+        sgb_destroy(g);
+        return st;
+    }
+    *out = g;
+    return SGB_OK;
+}
+
+int sgb_destroy(sgb_grid* g) {
+    if (!g) return SGB_EINVAL;
+    cudaSetDevice(g->device);
+    g->keys.release();
+    g->keys2.release();
+    g->mask.release();
+    g->mask2.release();
+    for (int p = 0; p < kMaxProps; ++p) {
+        g->data[p].release();
+        g->data2[p].release();
+        g->pend_val[p].release();
+    }
+    g->pend_lin.release();
+    g->nn[0].release();
+    g->nn[1].release();
+    g->bits.release();
+    for (auto& b : g->scratch) b.release();
+    g->hscratch.release();
+    g->err.release();
+    delete g;
+    return SGB_OK;
+}
+
+int sgb_set_background(sgb_grid* g, int prop, const void* value) {
+    if (!g || !value || prop < 0 || prop >= g->nprop) return SGB_EINVAL;
+    std::memcpy(g->bck[prop], value, elem_size(g->ptype[prop]));
+    const int bs = g->geo.bs, es = elem_size(g->ptype[prop]);
+    SGB_TRY(fill(g->data[prop].as<unsigned char>() + (size_t)g->n * bs * es, bs, es, bck_pattern(g, prop), 0));
+    SGB_CUDA(cudaStreamSynchronize(0));
+    return SGB_OK;
+}
+
+int sgb_insert(sgb_grid* g, int64_t n, const int32_t* coords, const void* const* values, sgb_stream stream) {
+    if (!g || n < 0 || (n > 0 && !coords)) return SGB_EINVAL;
+    if (n == 0) return SGB_OK;
+    cudaStream_t s = (cudaStream_t)stream;
+    SGB_TRY(g->pend_lin.reserve((size_t)(g->npend + n) * 8));
+    k_lin_from_coords<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(coords, n, g->geo,
+                                                                   g->pend_lin.as<int64_t>() + g->npend,
+                                                                   g->err.as<unsigned>());
+    SGB_CUDA(cudaGetLastError());
+    SGB_TRY(stage_values(g, n, values, s));
+    g->npend += n;
+    return SGB_OK;
+}
+
+int sgb_insert_lin(sgb_grid* g, int64_t n, const int64_t* lin, const void* const* values, sgb_stream stream) {
+    if (!g || n < 0 || (n > 0 && !lin)) return SGB_EINVAL;
+    if (n == 0) return SGB_OK;
+    cudaStream_t s = (cudaStream_t)stream;
+    SGB_TRY(g->pend_lin.reserve((size_t)(g->npend + n) * 8));
+    const int64_t maxlin = g->geo.bsz[0] * g->geo.bsz[1] * g->geo.bsz[2] * g->geo.bs;
+    k_check_lin<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(lin, n, maxlin, g->pend_lin.as<int64_t>() + g->npend,
+                                                             g->err.as<unsigned>());
+    SGB_CUDA(cudaGetLastError());
+    SGB_TRY(stage_values(g, n, values, s));
+    g->npend += n;
+    return SGB_OK;
+}
+
+int sgb_nchunks(const sgb_grid* g, int64_t* n) {
+    if (!g || !n) return SGB_EINVAL;
+    *n = g->n;
+    return SGB_OK;
+}
+
+int sgb_index_buffer(sgb_grid* g, const int64_t** dev) {
+    if (!g || !dev) return SGB_EINVAL;
+    *dev = g->keys.as<int64_t>();
+    return SGB_OK;
+}
+
+int sgb_data_buffer(sgb_grid* g, int prop, void** dev) {
+    if (!g || !dev || prop < 0 || prop >= g->nprop) return SGB_EINVAL;
+    *dev = g->data[prop].p;
+    return SGB_OK;
+}
+
+int sgb_mask_buffer(sgb_grid* g, uint8_t** dev) {
+    if (!g || !dev) return SGB_EINVAL;
+    *dev = g->mask.as<uint8_t>();
+    return SGB_OK;
+}
+
+static int load_map_impl(sgb_grid* g, int64_t n, const int64_t* keys, const void* const* data, const uint8_t* mask,
+                         cudaMemcpyKind kind, cudaStream_t s) {
+    if (!g || n < 0 || (n > 0 && (!keys || !data || !mask))) return SGB_EINVAL;
+    SGB_TRY(grid_reserve(g, n, false));
+    const int bs = g->geo.bs;
+    if (n > 0) {
+        SGB_CUDA(cudaMemcpyAsync(g->keys.p, keys, (size_t)n * 8, kind, s));
+        for (int p = 0; p < g->nprop; ++p) {
+            const int es = elem_size(g->ptype[p]);
+            if (data[p]) SGB_CUDA(cudaMemcpyAsync(g->data[p].p, data[p], (size_t)n * bs * es, kind, s));
+            else SGB_TRY(fill(g->data[p].p, n * bs, es, bck_pattern(g, p), s));  // not given: background
+        }
+        SGB_CUDA(cudaMemcpyAsync(g->mask.p, mask, (size_t)n * bs, kind, s));
+    }
+    g->n = n;
+    SGB_TRY(write_background(g, n, s, g->data, g->mask));
+    invalidate_derived(g);
+    return SGB_OK;
+}
+
+int sgb_load_map(sgb_grid* g, int64_t n, const int64_t* keys, const void* const* data, const uint8_t* mask,
+                 sgb_stream s) {
+    return load_map_impl(g, n, keys, data, mask, cudaMemcpyHostToDevice, (cudaStream_t)s);
+}
+
+int sgb_load_map_dev(sgb_grid* g, int64_t n, const int64_t* keys, const void* const* data, const uint8_t* mask,
+                     sgb_stream s) {
+    return load_map_impl(g, n, keys, data, mask, cudaMemcpyDeviceToDevice, (cudaStream_t)s);
+}
+
+int sgb_download_map(sgb_grid* g, int64_t* keys, void* const* data, uint8_t* mask, sgb_stream stream) {
+    if (!g) return SGB_EINVAL;
+    cudaStream_t s = (cudaStream_t)stream;
+    const int bs = g->geo.bs;
+    if (keys && g->n) SGB_CUDA(cudaMemcpyAsync(keys, g->keys.p, (size_t)g->n * 8, cudaMemcpyDeviceToHost, s));
+    if (data)
+        for (int p = 0; p < g->nprop; ++p)
+            if (data[p])
+                SGB_CUDA(cudaMemcpyAsync(data[p], g->data[p].p, (size_t)(g->n + 1) * bs * elem_size(g->ptype[p]),
+                                         cudaMemcpyDeviceToHost, s));
+    if (mask) SGB_CUDA(cudaMemcpyAsync(mask, g->mask.p, (size_t)(g->n + 1) * bs, cudaMemcpyDeviceToHost, s));
+    SGB_CUDA(cudaStreamSynchronize(s));
+    return SGB_OK;
+}
+
+int sgb_count_existing(sgb_grid* g, int64_t* existing, int64_t* padding, sgb_stream stream) {
+    if (!g) return SGB_EINVAL;
+    cudaStream_t s = (cudaStream_t)stream;
+    SGB_TRY(g->scratch[11].ensure(16));
+    SGB_CUDA(cudaMemsetAsync(g->scratch[11].p, 0, 16, s));
+    const int64_t total = g->n * g->geo.bs;
+    if (total > 0) {
+        int64_t blocks = (total + 255) / 256;
+        if (blocks > 2048) blocks = 2048;
+        k_count<<<(unsigned)blocks, 256, 0, s>>>(g->mask.as<uint8_t>(), total,
+                                                 g->scratch[11].as<unsigned long long>());
+        SGB_CUDA(cudaGetLastError());
+    }
+    SGB_TRY(g->hscratch.ensure(64));
+    SGB_CUDA(cudaMemcpyAsync(g->hscratch.p, g->scratch[11].p, 16, cudaMemcpyDeviceToHost, s));
+    SGB_CUDA(cudaStreamSynchronize(s));
+    unsigned long long* h = (unsigned long long*)g->hscratch.p;
+    if (existing) *existing = (int64_t)h[0];
+    if (padding) *padding = (int64_t)h[1];
+    return SGB_OK;
+}
+
+int sgb_get(sgb_grid* g, int64_t n, const int32_t* coords, int prop, void* out, sgb_stream stream) {
+    if (!g || n < 0 || prop < 0 || prop >= g->nprop || (n > 0 && (!coords || !out))) return SGB_EINVAL;
+    if (n == 0) return SGB_OK;
+    cudaStream_t s = (cudaStream_t)stream;
+    const unsigned blocks = (unsigned)((n + 255) / 256);
+    const int64_t* k = g->keys.as<int64_t>();
+    const uint8_t* m = g->mask.as<uint8_t>();
+    switch (elem_size(g->ptype[prop])) {
+        case 1: k_get<uint8_t><<<blocks, 256, 0, s>>>(coords, n, g->geo, k, g->n, g->data[prop].as<uint8_t>(), m, (uint8_t*)out); break;
+        case 4: k_get<uint32_t><<<blocks, 256, 0, s>>>(coords, n, g->geo, k, g->n, g->data[prop].as<uint32_t>(), m, (uint32_t*)out); break;
+        default: k_get<uint64_t><<<blocks, 256, 0, s>>>(coords, n, g->geo, k, g->n, g->data[prop].as<uint64_t>(), m, (uint64_t*)out); break;
+    }
+    SGB_CUDA(cudaGetLastError());
+    return SGB_OK;
+}
+
+int sgb_check_device_errors(sgb_grid* g, sgb_stream stream) {
+    if (!g) return SGB_EINVAL;
+    cudaStream_t s = (cudaStream_t)stream;
+    SGB_TRY(g->hscratch.ensure(64));
+    SGB_CUDA(cudaMemcpyAsync(g->hscratch.p, g->err.p, 4, cudaMemcpyDeviceToHost, s));
+    SGB_CUDA(cudaMemsetAsync(g->err.p, 0, 4, s));
+    SGB_CUDA(cudaStreamSynchronize(s));
+    unsigned e = *(unsigned*)g->hscratch.p;
+    if (e & kErrWaitTimeout) {
+        set_error("a device-side bounded wait gave up");
+        return SGB_ETIMEOUT;
+    }
+    if (e & kErrOutOfDomain) {
+        set_error("an inserted point lies outside the grid domain");
+        return SGB_ERANGE;
+    }
+    return SGB_OK;
+}
+
+int sgb_device_bytes(const sgb_grid* g, int64_t* bytes) {
+    if (!g || !bytes) return SGB_EINVAL;
+    size_t b = g->keys.bytes + g->keys2.bytes + g->mask.bytes + g->mask2.bytes + g->pend_lin.bytes + g->nn[0].bytes +
+               g->nn[1].bytes + g->bits.bytes + g->err.bytes;
+    for (int p = 0; p < kMaxProps; ++p) b += g->data[p].bytes + g->data2[p].bytes + g->pend_val[p].bytes;
+    for (auto& s : g->scratch) b += s.bytes;
+    *bytes = (int64_t)b;
+    return SGB_OK;
+}
+
+int sgb_set_launch_config(sgb_grid* g, int ctas_per_sm, int stages) {
+    if (!g || ctas_per_sm < 0 || ctas_per_sm > 4 || stages < 0 || (stages > 0 && (stages < 3 || stages > 8)))
+        return SGB_EINVAL;
+    if (ctas_per_sm) g->ctas_per_sm = ctas_per_sm;
+    if (stages) g->stages = stages;
+    return SGB_OK;
+}
+
+}  // extern "C"

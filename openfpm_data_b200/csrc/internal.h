@@ -1,0 +1,150 @@
+// Internal definitions shared by the CUDA translation units of libsgb200.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/sgb200.h"
+
+namespace sgb {
+
+constexpr int kMaxProps = 8;
+
+// Device error word bits (sgb_check_device_errors).
+enum : unsigned {
+    kErrWaitTimeout = 1u,   // a bounded mbarrier wait gave up
+    kErrOutOfDomain = 2u,   // an inserted point lies outside the domain
+};
+
+inline int elem_size(int t) { return t == SGB_F64 ? 8 : (t == SGB_U8 ? 1 : 4); }
+
+void set_error(const std::string& msg);
+int cuda_status(cudaError_t e, const char* what);
+
+#define SGB_CUDA(call)                                          \
+    do {                                                        \
+        cudaError_t e_ = (call);                                \
+        if (e_ != cudaSuccess) return ::sgb::cuda_status(e_, #call); \
+    } while (0)
+
+#define SGB_TRY(call)                 \
+    do {                              \
+        int s_ = (call);              \
+        if (s_ != SGB_OK) return s_;  \
+    } while (0)
+
+// Grow-only device buffer.
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    int reserve(size_t need);   // keeps contents
+    int ensure(size_t need);    // may drop contents
+    void release();
+    template <typename T>
+    T* as() const { return static_cast<T*>(p); }
+};
+
+// Pinned host staging for small device->host reads.
+struct HostScratch {
+    void* p = nullptr;
+    size_t bytes = 0;
+    int ensure(size_t need);
+    void release();
+};
+
+struct Geometry {
+    int dim = 3, edge = 8, bs = 512;
+    int64_t size[3] = {1, 1, 1};
+    int64_t bsz[3] = {1, 1, 1};
+};
+
+// Launch parameters of the fixed-function stencils.
+struct StencilParams {
+    float dt, Du, Dv, F, nFK;
+    float bck[2];
+    float coeff[27];
+    int64_t box_lo[3], box_hi[3];
+    int has_box;
+};
+
+// Per-grid entry of a stencil launch.  A grid takes part in global step t
+// when start <= t < start + nsteps; it then reads ping-pong buffer
+// (t - start) & 1 and writes the other one.  A single-grid launch is the
+// entry {start 0, nsteps 1} at t = 0.
+struct GridInfo {
+    int64_t start;
+    int64_t nsteps;
+    float dt, Du, Dv, F, nFK;
+    float bck[2];
+    float pad_;
+};
+
+// Field pointers of a launch: [ping-pong buffer][source property].
+struct FieldSet {
+    const float* in[2][2];
+    float* out[2][2];
+};
+
+}  // namespace sgb
+
+struct sgb_grid {
+    sgb::Geometry geo;
+    int device = 0;
+    int nprop = 0;
+    int ptype[sgb::kMaxProps] = {};
+    unsigned char bck[sgb::kMaxProps][8] = {};
+
+    int64_t n = 0;        // chunks
+    int64_t cap = 0;      // chunk capacity of the buffers below (excluding background)
+    sgb::DevBuf keys;     // int64 [cap]
+    sgb::DevBuf data[sgb::kMaxProps];  // [(cap+1) * bs]
+    sgb::DevBuf mask;     // [(cap+1) * bs]
+    // second set of buffers for flushes that add chunks
+    sgb::DevBuf keys2, data2[sgb::kMaxProps], mask2;
+
+    // staged inserts
+    int64_t npend = 0;
+    sgb::DevBuf pend_lin;                    // int64 [npend]
+    sgb::DevBuf pend_val[sgb::kMaxProps];    // [npend]
+    bool pend_has[sgb::kMaxProps] = {};
+
+    // neighbour tables (int32, -1 = absent); index 0 NNStar (8/chunk), 1 NNFull (27/chunk)
+    sgb::DevBuf nn[2];
+    bool nn_valid[2] = {false, false};
+    sgb::DevBuf bits;     // uint64 existence bitmaps, bs/64 words per chunk
+    bool bits_valid = false;
+
+    // flush / scan / sort scratch
+    sgb::DevBuf scratch[12];
+    sgb::HostScratch hscratch;
+
+    sgb::DevBuf err;      // unsigned device error word
+    int num_sms = 148;
+    int ctas_per_sm = 2;
+    int stages = 6;
+};
+
+namespace sgb {
+
+// neighbours.cu
+int ensure_neighbours(sgb_grid* g, int nn, cudaStream_t s);
+int ensure_bits(sgb_grid* g, cudaStream_t s);
+
+// stencil.cu
+int launch_stencil(sgb_grid* g, int kind, const int* src, const int* dst, const StencilParams& prm,
+                   cudaStream_t s);
+int make_params(sgb_grid* g, int kind, const int* src, const int* dst, const float* params, int nparams,
+                const int64_t* box, StencilParams& prm);
+
+// scan.cu
+int scan_exclusive_u32(const uint32_t* in, uint32_t* out, int64_t n, uint32_t* total_dev, DevBuf* tmp,
+                       cudaStream_t s);
+
+// buffers
+int grid_reserve(sgb_grid* g, int64_t chunks, bool keep);
+int write_background(sgb_grid* g, int64_t pos, cudaStream_t s, DevBuf* data, DevBuf& mask);
+
+}  // namespace sgb

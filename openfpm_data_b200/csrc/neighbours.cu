@@ -1,0 +1,248 @@
+// findNeighbours, existence bitmaps and tagBoundaries.
+#include <vector>
+
+#include "common.cuh"
+#include "internal.h"
+
+namespace sgb {
+
+// grid_smb::BlockLinId (src/Grid/Geometry/grid_smb.hpp:280-299): only the
+// upper bound is checked, so a block coordinate of -1 along x or y yields the
+// id of a block one row (or slice) back -- reproduced on purpose, it decides
+// which chunk an NNFull neighbour lookup returns at the low faces.
+__device__ __forceinline__ int64_t block_lin_ref(const Geometry& geo, const int64_t* bc) {
+    int64_t lin = bc[geo.dim - 1];
+    if (lin >= geo.bsz[geo.dim - 1]) return -1;
+    for (int d = geo.dim - 2; d >= 0; --d) {
+        lin *= geo.bsz[d];
+        if (bc[d] >= geo.bsz[d]) return -1;
+        lin += bc[d];
+    }
+    return lin;
+}
+
+// findNeighbours (src/SparseGridGpu/SparseGridGpu_kernels.cuh:1014-1035) with
+// NNStar::getNNpos (SparseGridGpu_ker_util.hpp:91-112, slots -x,+x,-y,+y,-z,+z,
+// two unused) and NNFull::getNNpos (SparseGridGpu.hpp:266-287, slot
+// dx+3dy+9dz over {0,1,2}).  Output: data position, -1 when absent.
+__global__ void k_find_nn(const int64_t* keys, int64_t n, Geometry geo, int kind, int32_t* out) {
+    const int nnn = kind == SGB_NN_STAR ? 8 : 27;
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t chunk = t / nnn;
+    const int o = (int)(t - chunk * nnn);
+    if (chunk >= n) return;
+    int64_t b = keys[chunk];
+    int64_t bc[3];
+    for (int d = 0; d < geo.dim; ++d) {
+        bc[d] = b % geo.bsz[d];
+        b /= geo.bsz[d];
+    }
+    int64_t pos = -1;
+    if (kind == SGB_NN_STAR) {
+        if (o < 2 * geo.dim) {
+            const int d = o / 2;
+            const int64_t dpos = bc[d] + (o % 2) * 2 - 1;
+            if (dpos >= 0) {
+                bc[d] = dpos;
+                const int64_t bl = block_lin_ref(geo, bc);
+                if (bl >= 0) pos = find_key(keys, n, bl);
+            }
+        }
+    } else if (o != nnn / 2) {
+        int cnt = o;
+        for (int d = 0; d < geo.dim; ++d) {
+            bc[d] += cnt % 3 - 1;
+            cnt /= 3;
+        }
+        const int64_t bl = block_lin_ref(geo, bc);
+        if (bl >= 0) pos = find_key(keys, n, bl);
+    }
+    out[t] = (int32_t)pos;
+}
+
+// Existence bitmap of every chunk: point p of a chunk is bit (p & 63) of
+// word (p >> 6).  One warp per chunk, one ballot per 32 mask bytes.
+__global__ void k_bits(const uint8_t* mask, int64_t n, int bs, uint64_t* bits) {
+    const int64_t chunk = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (chunk >= n) return;
+    const uint8_t* m = mask + (size_t)chunk * bs;
+    uint64_t word = 0;
+    for (int r = 0; r < bs / 32; ++r) {
+        const unsigned b = __ballot_sync(0xffffffffu, m[r * 32 + lane] & 1);
+        if (r & 1) {
+            word |= (uint64_t)b << 32;
+            if (lane == 0) bits[(size_t)chunk * (bs / 64) + (r >> 1)] = word;
+        } else {
+            word = b;
+        }
+    }
+}
+
+// tagBoundaries (src/SparseGridGpu/SparseGridGpu_kernels.cuh:676-737) with
+// NNStar::isPadding (SparseGridGpu_ker_util.hpp:141-157) for 8^3 chunks: one
+// warp per chunk; lanes 0..7 hold the 64-bit z-slices of the existence
+// bitmap, neighbours along x/y are word shifts with the facing column / row
+// of the adjacent chunk, along z the adjacent lane's word (shuffle) or the
+// facing slice of the adjacent chunk.  EXIST points get PADDING set when a
+// face neighbour is missing and cleared otherwise; other bytes are untouched.
+__global__ void k_tag_star8(const uint64_t* bits, const int32_t* nn, int64_t n, uint8_t* mask) {
+    const int64_t chunk = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (chunk >= n) return;
+    constexpr uint64_t COL0 = 0x0101010101010101ull, COL7 = COL0 << 7;
+    const int z = lane & 7;
+    const int32_t* nb = nn + chunk * 8;
+    const uint64_t W = bits[chunk * 8 + z];
+    const int32_t xm = nb[0], xp = nb[1], ym = nb[2], yp = nb[3], zm = nb[4], zp = nb[5];
+    const uint64_t XM = xm >= 0 ? bits[(int64_t)xm * 8 + z] : 0;
+    const uint64_t XP = xp >= 0 ? bits[(int64_t)xp * 8 + z] : 0;
+    const uint64_t YM = ym >= 0 ? bits[(int64_t)ym * 8 + z] : 0;
+    const uint64_t YP = yp >= 0 ? bits[(int64_t)yp * 8 + z] : 0;
+    const uint64_t up = __shfl_up_sync(0xffffffffu, W, 1);
+    const uint64_t dn = __shfl_down_sync(0xffffffffu, W, 1);
+    const uint64_t ZMw = z == 0 ? (zm >= 0 ? bits[(int64_t)zm * 8 + 7] : 0) : up;
+    const uint64_t ZPw = z == 7 ? (zp >= 0 ? bits[(int64_t)zp * 8 + 0] : 0) : dn;
+    const uint64_t exm = ((W << 1) & ~COL0) | ((XM & COL7) >> 7);
+    const uint64_t exp_ = ((W >> 1) & ~COL7) | ((XP & COL0) << 7);
+    const uint64_t eym = (W << 8) | (YM >> 56);
+    const uint64_t eyp = (W >> 8) | (YP << 56);
+    const uint64_t pad = W & ~(exm & exp_ & eym & eyp & ZMw & ZPw);
+    // lane l rewrites mask bytes [16l, 16l+16): z-slice l/4, bits 16*(l%4)..
+    const uint64_t pw = __shfl_sync(0xffffffffu, pad, lane >> 2);
+    const unsigned bits16 = (unsigned)(pw >> (16 * (lane & 3))) & 0xffffu;
+    uint4* mp = reinterpret_cast<uint4*>(mask + (size_t)chunk * 512) + lane;
+    uint4 v = *mp;
+    unsigned w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        unsigned out = 0;
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            unsigned m = (w[q] >> (8 * b)) & 0xffu;
+            if (m & 1u) m = ((bits16 >> (q * 4 + b)) & 1u) ? (m | 2u) : (m & ~2u);
+            out |= m << (8 * b);
+        }
+        w[q] = out;
+    }
+    *mp = make_uint4(w[0], w[1], w[2], w[3]);
+}
+
+// Generic tagBoundaries for any edge and both neighbourhoods: one CTA per
+// chunk, the 27 (or 7) neighbouring existence bitmaps staged in shared
+// memory, one thread per point.  NNFull isPadding (SparseGridGpu.hpp:200-228)
+// tests the whole 3x3x3 box.
+__global__ void k_tag_generic(const uint64_t* bits, const int32_t* nn, int64_t n, int edge, int kind, uint8_t* mask) {
+    __shared__ uint64_t nbw[27][8];
+    const int64_t chunk = blockIdx.x;
+    if (chunk >= n) return;
+    const int bs = edge * edge * edge, words = bs / 64;
+    for (int t = threadIdx.x; t < 27 * words; t += blockDim.x) {
+        const int c = t / words, w = t % words;
+        int64_t src = -1;
+        if (c == 13) src = chunk;
+        else if (kind == SGB_NN_FULL) src = nn[chunk * 27 + c];
+        else {
+            // faces only: c = (dx+1) + 3(dy+1) + 9(dz+1)
+            const int slot = c == 12 ? 0 : c == 14 ? 1 : c == 10 ? 2 : c == 16 ? 3 : c == 4 ? 4 : c == 22 ? 5 : -1;
+            src = slot >= 0 ? nn[chunk * 8 + slot] : -1;
+        }
+        nbw[c][w] = src >= 0 ? bits[src * words + w] : 0;
+    }
+    __syncthreads();
+    for (int p = threadIdx.x; p < bs; p += blockDim.x) {
+        uint8_t m = mask[(size_t)chunk * bs + p];
+        if (!(m & 1)) continue;
+        const int x = p % edge, y = (p / edge) % edge, z = p / (edge * edge);
+        bool pad = false;
+        for (int q = 0; q < 27 && !pad; ++q) {
+            const int dx = q % 3 - 1, dy = (q / 3) % 3 - 1, dz = q / 9 - 1;
+            if (kind == SGB_NN_STAR && (dx != 0) + (dy != 0) + (dz != 0) != 1) continue;
+            int nx = x + dx, ny = y + dy, nz = z + dz;
+            const int c = (nx < 0 ? 0 : nx >= edge ? 2 : 1) + 3 * (ny < 0 ? 0 : ny >= edge ? 2 : 1) +
+                          9 * (nz < 0 ? 0 : nz >= edge ? 2 : 1);
+            nx = (nx + edge) % edge;
+            ny = (ny + edge) % edge;
+            nz = (nz + edge) % edge;
+            const int l = nx + edge * (ny + edge * nz);
+            pad |= !((nbw[c][l >> 6] >> (l & 63)) & 1);
+        }
+        mask[(size_t)chunk * bs + p] = pad ? (uint8_t)(m | 2u) : (uint8_t)(m & ~2u);
+    }
+}
+
+int ensure_neighbours(sgb_grid* g, int nn, cudaStream_t s) {
+    if (g->nn_valid[nn]) return SGB_OK;
+    const int nnn = nn == SGB_NN_STAR ? 8 : 27;
+    SGB_TRY(g->nn[nn].ensure((size_t)(g->n + 1) * nnn * 4));
+    if (g->n > 0) {
+        const int64_t total = g->n * nnn;
+        k_find_nn<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(g->keys.as<int64_t>(), g->n, g->geo, nn,
+                                                                   g->nn[nn].as<int32_t>());
+        SGB_CUDA(cudaGetLastError());
+    }
+    g->nn_valid[nn] = true;
+    return SGB_OK;
+}
+
+int ensure_bits(sgb_grid* g, cudaStream_t s) {
+    if (g->bits_valid) return SGB_OK;
+    const int words = g->geo.bs / 64;
+    SGB_TRY(g->bits.ensure((size_t)(g->n + 1) * words * 8));
+    if (g->n > 0) {
+        const int64_t threads = g->n * 32;
+        k_bits<<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(g->mask.as<uint8_t>(), g->n, g->geo.bs,
+                                                                  g->bits.as<uint64_t>());
+        SGB_CUDA(cudaGetLastError());
+    }
+    g->bits_valid = true;
+    return SGB_OK;
+}
+
+}  // namespace sgb
+
+using namespace sgb;
+
+extern "C" {
+
+int sgb_find_neighbours(sgb_grid* g, int nn, sgb_stream s) {
+    if (!g || (nn != SGB_NN_STAR && nn != SGB_NN_FULL)) return SGB_EINVAL;
+    g->nn_valid[nn] = false;
+    return ensure_neighbours(g, nn, (cudaStream_t)s);
+}
+
+int sgb_neighbour_table(sgb_grid* g, int nn, int64_t* out, sgb_stream stream) {
+    if (!g || !out || (nn != SGB_NN_STAR && nn != SGB_NN_FULL)) return SGB_EINVAL;
+    cudaStream_t s = (cudaStream_t)stream;
+    SGB_TRY(ensure_neighbours(g, nn, s));
+    const int nnn = nn == SGB_NN_STAR ? 8 : 27;
+    std::vector<int32_t> h((size_t)g->n * nnn);
+    if (g->n) SGB_CUDA(cudaMemcpyAsync(h.data(), g->nn[nn].p, h.size() * 4, cudaMemcpyDeviceToHost, s));
+    SGB_CUDA(cudaStreamSynchronize(s));
+    for (size_t i = 0; i < h.size(); ++i) {
+        const int o = (int)(i % nnn);
+        if (nn == SGB_NN_STAR && o >= 2 * g->geo.dim) out[i] = -1;  // unused NNStar slots
+        else out[i] = h[i] < 0 ? g->n : h[i];                      // background position
+    }
+    return SGB_OK;
+}
+
+int sgb_tag_boundaries(sgb_grid* g, int nn, sgb_stream stream) {
+    if (!g || (nn != SGB_NN_STAR && nn != SGB_NN_FULL)) return SGB_EINVAL;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (g->n == 0) return SGB_OK;
+    SGB_TRY(ensure_neighbours(g, nn, s));
+    SGB_TRY(ensure_bits(g, s));
+    if (nn == SGB_NN_STAR && g->geo.edge == 8) {
+        const int64_t threads = g->n * 32;
+        k_tag_star8<<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(g->bits.as<uint64_t>(), g->nn[0].as<int32_t>(),
+                                                                      g->n, g->mask.as<uint8_t>());
+    } else {
+        k_tag_generic<<<(unsigned)g->n, 128, 0, s>>>(g->bits.as<uint64_t>(), g->nn[nn].as<int32_t>(), g->n,
+                                                     g->geo.edge, nn, g->mask.as<uint8_t>());
+    }
+    SGB_CUDA(cudaGetLastError());
+    return SGB_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,110 @@
+// Stencil arithmetic and launch description shared by the single-grid and
+// the batched entry points.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+#include "internal.h"
+
+namespace sgb {
+
+constexpr int kConsumerWarps = 8;
+constexpr int kThreads = (kConsumerWarps + 1) * 32;
+
+__device__ __forceinline__ bool in_box(const StencilParams& prm, int64_t cx, int64_t cy, int64_t cz) {
+    return cx >= prm.box_lo[0] && cx <= prm.box_hi[0] && cy >= prm.box_lo[1] && cy <= prm.box_hi[1] &&
+           cz >= prm.box_lo[2] && cz <= prm.box_hi[2];
+}
+
+// HeatStencil update (src/SparseGridGpu/tests/utils/SparseGridGpu_util_test.cuh:256-274):
+//   lap = (float)(-2.0*dim*cur); lap += xm + xp; lap += ym + yp; lap += zm + zp;
+//   res = cur + dt*lap  (contracted to an FMA by nvcc)
+__device__ __forceinline__ float heat_update(float cur, float xm, float xp, float ym, float yp, float zm, float zp,
+                                             float dt) {
+    float lap = __fmul_rn(-6.0f, cur);
+    lap = __fadd_rn(lap, __fadd_rn(xm, xp));
+    lap = __fadd_rn(lap, __fadd_rn(ym, yp));
+    lap = __fadd_rn(lap, __fadd_rn(zm, zp));
+    return __fmaf_rn(dt, lap, cur);
+}
+
+// 7-point Laplacian in HeatStencil's association order.
+__device__ __forceinline__ float lap7(float c, float xm, float xp, float ym, float yp, float zm, float zp) {
+    float lap = __fmul_rn(-6.0f, c);
+    lap = __fadd_rn(lap, __fadd_rn(xm, xp));
+    lap = __fadd_rn(lap, __fadd_rn(ym, yp));
+    return __fadd_rn(lap, __fadd_rn(zm, zp));
+}
+
+// Gray-Scott as a conv2_b user function:
+//   uvv = (u*v)*v
+//   u' = u + dt*fma(F, 1-u, fma(Du, lu, -uvv))
+//   v' = v + dt*fma(-(F+k), v, fma(Dv, lv, uvv))
+__device__ __forceinline__ void gs_update(float u, float v, float lu, float lv, const GridInfo& p, float& un,
+                                          float& vn) {
+    const float uvv = __fmul_rn(__fmul_rn(u, v), v);
+    float du = __fmaf_rn(p.Du, lu, -uvv);
+    du = __fmaf_rn(p.F, __fsub_rn(1.0f, u), du);
+    float dv = __fmaf_rn(p.Dv, lv, uvv);
+    dv = __fmaf_rn(p.nFK, v, dv);
+    un = __fmaf_rn(p.dt, du, u);
+    vn = __fmaf_rn(p.dt, dv, v);
+}
+
+// Everything one stencil launch needs.
+struct LaunchDesc {
+    int kind, edge, use_tile, stages, num_sms;
+    unsigned ctas;
+    FieldSet fs;
+    const uint8_t* mask;
+    const int32_t* nn;
+    const int64_t* keys;
+    const int32_t* gid;      // per chunk grid id (NULL: single grid g0)
+    const GridInfo* grids;   // per grid entries (NULL: single grid g0)
+    GridInfo g0;
+    int64_t n;
+    Geometry geo;
+    StencilParams prm;
+    int64_t t;
+    unsigned* err;
+};
+
+int launch_fields(const LaunchDesc& L, cudaStream_t s);
+GridInfo grid_info_of(const StencilParams& prm);
+
+// Capture `body(stream)` into a CUDA graph, launch it on `s`, wait for it.
+template <typename F>
+int run_graph(F body, cudaStream_t s) {
+    cudaStream_t cap;
+    SGB_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int st = SGB_OK;
+    cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+        st = body(cap);
+        cudaError_t e2 = cudaStreamEndCapture(cap, &graph);
+        if (st == SGB_OK && e2 != cudaSuccess) st = cuda_status(e2, "cudaStreamEndCapture");
+    } else {
+        st = cuda_status(e, "cudaStreamBeginCapture");
+    }
+    if (st == SGB_OK) {
+        e = cudaGraphInstantiate(&exec, graph, 0);
+        if (e != cudaSuccess) st = cuda_status(e, "cudaGraphInstantiate");
+    }
+    if (st == SGB_OK) {
+        e = cudaGraphLaunch(exec, s);
+        if (e != cudaSuccess) st = cuda_status(e, "cudaGraphLaunch");
+    }
+    if (st == SGB_OK) {
+        e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) st = cuda_status(e, "cudaStreamSynchronize");
+    }
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    cudaStreamDestroy(cap);
+    return st;
+}
+
+}  // namespace sgb

@@ -1,0 +1,284 @@
+"""Python host mirror of SparseGridGpu<3, aggregate<...>, edge> over the C ABI.
+
+Method names follow the reference class (src/SparseGridGpu/SparseGridGpu.hpp);
+device data is exchanged as torch CUDA tensors (torch is plumbing here: device
+memory and streams; every computation runs in libsgb200.so).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Iterable, Optional, Sequence
+
+import numpy as np
+import torch
+
+from . import _lib as L
+
+_TYPES = {"f32": L.F32, "float32": L.F32, "i32": L.I32, "int32": L.I32, "f64": L.F64, "float64": L.F64,
+          "u8": L.U8, "uint8": L.U8}
+_NP = {L.F32: np.float32, L.I32: np.int32, L.F64: np.float64, L.U8: np.uint8}
+_TORCH = {L.F32: torch.float32, L.I32: torch.int32, L.F64: torch.float64, L.U8: torch.uint8}
+_TS = {L.F32: "<f4", L.I32: "<i4", L.F64: "<f8", L.U8: "|u1"}
+
+# reference reduction names -> sgb_op
+OPS = {"sRight_": L.OP_RIGHT, "sLeft_": L.OP_LEFT, "sadd_": L.OP_ADD, "smax_": L.OP_MAX, "smin_": L.OP_MIN,
+       "sBitwiseOr_": L.OP_OR, None: L.OP_NONE, "none": L.OP_NONE}
+
+
+def _stream(stream=None) -> int:
+    if stream is None:
+        return torch.cuda.current_stream().cuda_stream
+    return stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream)
+
+
+def _i32arr(vals):
+    return (C.c_int * len(vals))(*vals)
+
+
+class _DevView:
+    """Zero-copy torch view of a device buffer owned by the library."""
+
+    def __init__(self, ptr: int, shape, typestr: str):
+        self.__cuda_array_interface__ = {"shape": tuple(shape), "typestr": typestr, "data": (ptr, False),
+                                         "version": 3, "strides": None}
+
+
+class SparseGridGpu:
+    """SparseGridGpu(size, props, edge): a 3-D sparse block grid on one GPU."""
+
+    def __init__(self, size: Sequence[int], props: Sequence[str] = ("f32",), edge: int = 8, device: int = 0):
+        lib = L.load()
+        self.size = tuple(int(s) for s in size)
+        self.edge = int(edge)
+        self.bs = self.edge ** 3
+        self.ptypes = [_TYPES[p] if isinstance(p, str) else int(p) for p in props]
+        self.device = device
+        sz = (C.c_int64 * 3)(*self.size)
+        pt = _i32arr(self.ptypes)
+        h = C.c_void_p()
+        L.check(lib.sgb_create(C.byref(h), 3, self.edge, sz, len(self.ptypes), pt, device), "sgb_create")
+        self._h = h
+        self._lib = lib
+        self.bck = [0] * len(self.ptypes)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.sgb_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    # ---------------------------------------------------------------- setup
+    def setBackgroundValue(self, p: int, value) -> None:
+        v = np.array([value], dtype=_NP[self.ptypes[p]])
+        L.check(self._lib.sgb_set_background(self._h, p, v.ctypes.data_as(C.c_void_p)), "sgb_set_background")
+        self.bck[p] = value
+
+    def setLaunchConfig(self, ctas_per_sm: int = 0, stages: int = 0) -> None:
+        L.check(self._lib.sgb_set_launch_config(self._h, ctas_per_sm, stages), "sgb_set_launch_config")
+
+    # ---------------------------------------------------------------- insert / flush
+    def _values(self, values):
+        ptrs = (C.c_void_p * len(self.ptypes))()
+        keep = []
+        for p, t in enumerate(self.ptypes):
+            v = None if values is None else values[p] if p < len(values) else None
+            if v is None:
+                ptrs[p] = None
+                continue
+            v = v.to(device=f"cuda:{self.device}", dtype=_TORCH[t]).contiguous()
+            keep.append(v)
+            ptrs[p] = v.data_ptr()
+        return ptrs, keep
+
+    def insert(self, coords: torch.Tensor, values: Sequence[Optional[torch.Tensor]], stream=None) -> None:
+        """Stage points (int32 [n,3] on the device) with one value per property."""
+        c = coords.to(device=f"cuda:{self.device}", dtype=torch.int32).contiguous()
+        ptrs, keep = self._values(values)
+        L.check(self._lib.sgb_insert(self._h, c.shape[0], c.data_ptr(), ptrs, _stream(stream)), "sgb_insert")
+        self._keep = (c, keep)  # the staging copy is stream ordered; keep inputs alive until then
+
+    def insert_lin(self, lin: torch.Tensor, values, stream=None) -> None:
+        l = lin.to(device=f"cuda:{self.device}", dtype=torch.int64).contiguous()
+        ptrs, keep = self._values(values)
+        L.check(self._lib.sgb_insert_lin(self._h, l.shape[0], l.data_ptr(), ptrs, _stream(stream)), "sgb_insert_lin")
+        self._keep = (l, keep)
+
+    def flush(self, ops: Iterable, stream=None) -> None:
+        """flush<ops...>: one reduction per property (sgb_op ids or reference names)."""
+        o = [OPS[x] if (isinstance(x, str) or x is None) else int(x) for x in ops]
+        o += [L.OP_NONE] * (len(self.ptypes) - len(o))
+        L.check(self._lib.sgb_flush(self._h, _i32arr(o), _stream(stream)), "sgb_flush")
+
+    # ---------------------------------------------------------------- neighbours / tag
+    def findNeighbours(self, nn: int = L.NN_STAR, stream=None) -> None:
+        L.check(self._lib.sgb_find_neighbours(self._h, nn, _stream(stream)), "sgb_find_neighbours")
+
+    def neighbour_table(self, nn: int = L.NN_STAR, stream=None) -> np.ndarray:
+        k = 8 if nn == L.NN_STAR else 27
+        out = np.empty(self.nchunks * k, dtype=np.int64)
+        L.check(self._lib.sgb_neighbour_table(self._h, nn, out.ctypes.data_as(C.c_void_p), _stream(stream)),
+                "sgb_neighbour_table")
+        return out.reshape(self.nchunks, k)
+
+    def tagBoundaries(self, nn: int = L.NN_STAR, stream=None) -> None:
+        L.check(self._lib.sgb_tag_boundaries(self._h, nn, _stream(stream)), "sgb_tag_boundaries")
+
+    # ---------------------------------------------------------------- stencils
+    @staticmethod
+    def _box(box):
+        if box is None:
+            return None
+        lo, hi = box
+        return (C.c_int64 * 6)(*(list(lo) + list(hi)))
+
+    def applyStencils(self, kind: int, src: Sequence[int], dst: Sequence[int], params: Sequence[float],
+                      box=None, stream=None, tiled: bool = False) -> None:
+        prm = (C.c_float * len(params))(*params)
+        fn = self._lib.sgb_apply_stencil_tiled if tiled else self._lib.sgb_apply_stencil
+        L.check(fn(self._h, kind, _i32arr(src), _i32arr(dst), prm, len(params), self._box(box), _stream(stream)),
+                "sgb_apply_stencil")
+
+    def run_steps(self, kind: int, src, dst, params, nsteps: int, use_graph: bool = True, stream=None) -> bool:
+        """nsteps ping-pong applications; returns True when the result is in dst."""
+        prm = (C.c_float * len(params))(*params)
+        fin = C.c_int(0)
+        L.check(self._lib.sgb_run_steps(self._h, kind, _i32arr(src), _i32arr(dst), prm, len(params), nsteps,
+                                        int(use_graph), C.byref(fin), _stream(stream)), "sgb_run_steps")
+        return bool(fin.value)
+
+    def check_device_errors(self, stream=None) -> None:
+        L.check(self._lib.sgb_check_device_errors(self._h, _stream(stream)), "device error word")
+
+    # ---------------------------------------------------------------- data access
+    @property
+    def nchunks(self) -> int:
+        n = C.c_int64()
+        L.check(self._lib.sgb_nchunks(self._h, C.byref(n)), "sgb_nchunks")
+        return n.value
+
+    def private_get_index_array(self) -> torch.Tensor:
+        p = C.c_void_p()
+        L.check(self._lib.sgb_index_buffer(self._h, C.byref(p)), "sgb_index_buffer")
+        return torch.as_tensor(_DevView(p.value or 0, (self.nchunks,), "<i8"), device=f"cuda:{self.device}")
+
+    def private_get_data_array(self, prop: int) -> torch.Tensor:
+        """Chunk data of one property, (nchunks + 1) * bs elements, background chunk last."""
+        p = C.c_void_p()
+        L.check(self._lib.sgb_data_buffer(self._h, prop, C.byref(p)), "sgb_data_buffer")
+        return torch.as_tensor(_DevView(p.value, ((self.nchunks + 1) * self.bs,), _TS[self.ptypes[prop]]),
+                               device=f"cuda:{self.device}")
+
+    def private_get_mask_array(self) -> torch.Tensor:
+        p = C.c_void_p()
+        L.check(self._lib.sgb_mask_buffer(self._h, C.byref(p)), "sgb_mask_buffer")
+        return torch.as_tensor(_DevView(p.value, ((self.nchunks + 1) * self.bs,), "|u1"), device=f"cuda:{self.device}")
+
+    def load_map(self, keys: np.ndarray, data: Sequence[np.ndarray], mask: np.ndarray, stream=None) -> None:
+        """hostToDevice of a whole block map (sorted keys, chunk data without
+        background); a None entry fills that property with its background."""
+        keys = np.ascontiguousarray(keys, dtype=np.int64)
+        data = [None if d is None else np.ascontiguousarray(d, dtype=_NP[t]) for d, t in zip(data, self.ptypes)]
+        data += [None] * (len(self.ptypes) - len(data))
+        mask = np.ascontiguousarray(mask, dtype=np.uint8)
+        ptrs = (C.c_void_p * len(data))(*[None if d is None else d.ctypes.data for d in data])
+        L.check(self._lib.sgb_load_map(self._h, len(keys), keys.ctypes.data_as(C.c_void_p), ptrs,
+                                       mask.ctypes.data_as(C.c_void_p), _stream(stream)), "sgb_load_map")
+
+    def load_map_dev(self, keys: torch.Tensor, data: Sequence[torch.Tensor], mask: torch.Tensor, stream=None) -> None:
+        ptrs = (C.c_void_p * len(data))(*[d.data_ptr() for d in data])
+        L.check(self._lib.sgb_load_map_dev(self._h, keys.shape[0], keys.data_ptr(), ptrs, mask.data_ptr(),
+                                           _stream(stream)), "sgb_load_map_dev")
+
+    def deviceToHost(self, stream=None):
+        """(keys[n], [data_p[(n+1)*bs]], mask[(n+1)*bs]) as numpy arrays."""
+        n = self.nchunks
+        keys = np.empty(n, dtype=np.int64)
+        data = [np.empty((n + 1) * self.bs, dtype=_NP[t]) for t in self.ptypes]
+        mask = np.empty((n + 1) * self.bs, dtype=np.uint8)
+        ptrs = (C.c_void_p * len(data))(*[d.ctypes.data for d in data])
+        L.check(self._lib.sgb_download_map(self._h, keys.ctypes.data_as(C.c_void_p), ptrs,
+                                           mask.ctypes.data_as(C.c_void_p), _stream(stream)), "sgb_download_map")
+        return keys, data, mask
+
+    def countExistingElements(self, stream=None) -> int:
+        e = C.c_int64()
+        L.check(self._lib.sgb_count_existing(self._h, C.byref(e), None, _stream(stream)), "sgb_count_existing")
+        return e.value
+
+    def countBoundaryElements(self, stream=None) -> int:
+        p = C.c_int64()
+        L.check(self._lib.sgb_count_existing(self._h, None, C.byref(p), _stream(stream)), "sgb_count_existing")
+        return p.value
+
+    def get(self, prop: int, coords: torch.Tensor, stream=None) -> torch.Tensor:
+        c = coords.to(device=f"cuda:{self.device}", dtype=torch.int32).contiguous()
+        out = torch.empty(c.shape[0], dtype=_TORCH[self.ptypes[prop]], device=f"cuda:{self.device}")
+        L.check(self._lib.sgb_get(self._h, c.shape[0], c.data_ptr(), prop, out.data_ptr(), _stream(stream)), "sgb_get")
+        return out
+
+    def device_bytes(self) -> int:
+        b = C.c_int64()
+        L.check(self._lib.sgb_device_bytes(self._h, C.byref(b)), "sgb_device_bytes")
+        return b.value
+
+
+class Batch:
+    """Many grids advanced by one persistent launch per step (sgb_batch_*)."""
+
+    def __init__(self, device: int = 0):
+        lib = L.load()
+        h = C.c_void_p()
+        L.check(lib.sgb_batch_create(C.byref(h), device), "sgb_batch_create")
+        self._h, self._lib = h, lib
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.sgb_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_launch_config(self, ctas_per_sm: int = 0, stages: int = 0):
+        L.check(self._lib.sgb_batch_set_launch_config(self._h, ctas_per_sm, stages), "sgb_batch_set_launch_config")
+
+    def add(self, g: SparseGridGpu, kind: int, src, dst, params, nsteps: int, stream=None) -> int:
+        prm = (C.c_float * len(params))(*params)
+        slot = C.c_int(-1)
+        L.check(self._lib.sgb_batch_add(self._h, g.handle, kind, _i32arr(src), _i32arr(dst), prm, len(params),
+                                        int(nsteps), C.byref(slot), _stream(stream)), "sgb_batch_add")
+        return slot.value
+
+    def remove(self, slot: int, stream=None):
+        L.check(self._lib.sgb_batch_remove(self._h, slot, _stream(stream)), "sgb_batch_remove")
+
+    def step(self, nsteps: int = 1, use_graph: bool = True, stream=None):
+        L.check(self._lib.sgb_batch_step(self._h, nsteps, int(use_graph), _stream(stream)), "sgb_batch_step")
+
+    def slot_steps(self, slot: int) -> int:
+        d = C.c_int64()
+        L.check(self._lib.sgb_batch_slot_steps(self._h, slot, C.byref(d)), "sgb_batch_slot_steps")
+        return d.value
+
+    def extract(self, slot: int, g: SparseGridGpu, stream=None) -> bool:
+        fin = C.c_int(0)
+        L.check(self._lib.sgb_batch_extract(self._h, slot, g.handle, C.byref(fin), _stream(stream)),
+                "sgb_batch_extract")
+        return bool(fin.value)
+
+    def info(self):
+        ng, nc, nb = C.c_int(), C.c_int64(), C.c_int64()
+        L.check(self._lib.sgb_batch_info(self._h, C.byref(ng), C.byref(nc), C.byref(nb)), "sgb_batch_info")
+        return ng.value, nc.value, nb.value

@@ -1,0 +1,267 @@
+"""ctypes bindings for the CPU oracle and the CPU baseline.
+
+TEST / BENCHMARK INFRASTRUCTURE ONLY.  Only tests/, ``__graft_entry__.smoke()``
+and bench.py's CPU-baseline leg import this module, as the checker.  The
+product path (``openfpm_data_b200``) never imports it.
+
+``OracleGrid`` mirrors the reference's block map (sorted chunk keys, SoA chunk
+data with a trailing background chunk, one mask byte per point) and exposes
+the restated flush / findNeighbours / tagBoundaries / stencil semantics of
+``oracle/sgb_oracle.cpp``.  ``CpuSgrid`` is the sgrid_cpu-style baseline of
+``oracle/sgrid_cpu_baseline.cpp``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+BUILD = os.path.join(HERE, "_build")
+
+T_F32, T_I32, T_F64, T_U8 = 0, 1, 2, 3
+OP_NONE, OP_RIGHT, OP_LEFT, OP_ADD, OP_MAX, OP_MIN, OP_OR = range(7)
+NN_STAR, NN_FULL = 0, 1
+_NP = {T_F32: np.float32, T_I32: np.int32, T_F64: np.float64, T_U8: np.uint8}
+
+
+def build(force: bool = False) -> None:
+    """Compile the oracle libraries with the committed Makefile."""
+    need = force or not all(
+        os.path.exists(os.path.join(BUILD, f)) for f in ("libsgb_oracle.so", "libsgrid_cpu.so")
+    )
+    if need:
+        subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+_lib = None
+_cpu = None
+
+
+def _load():
+    global _lib, _cpu
+    if _lib is None:
+        build()
+        _lib = C.CDLL(os.path.join(BUILD, "libsgb_oracle.so"))
+        _cpu = C.CDLL(os.path.join(BUILD, "libsgrid_cpu.so"))
+        vp, i64, i32 = C.c_void_p, C.c_int64, C.c_int
+        _lib.sgo_create.restype = vp
+        _lib.sgo_create.argtypes = [i32, i32, vp, i32, vp]
+        _lib.sgo_destroy.argtypes = [vp]
+        _lib.sgo_set_background.argtypes = [vp, i32, vp]
+        _lib.sgo_nchunks.restype = i64
+        _lib.sgo_nchunks.argtypes = [vp]
+        _lib.sgo_lin_ids.argtypes = [vp, i64, vp, vp]
+        _lib.sgo_inv_lin.argtypes = [vp, i64, vp, vp]
+        _lib.sgo_load_map.argtypes = [vp, i64, vp, vp, vp]
+        _lib.sgo_export_map.argtypes = [vp, vp, vp, vp]
+        _lib.sgo_flush_chunks.argtypes = [vp, i64, vp, vp, vp, vp]
+        _lib.sgo_flush_points.argtypes = [vp, i64, vp, vp, vp, vp]
+        _lib.sgo_find_neighbours.restype = i32
+        _lib.sgo_find_neighbours.argtypes = [vp, i32, vp]
+        _lib.sgo_tag_boundaries.argtypes = [vp, i32]
+        f = C.c_float
+        _lib.sgo_heat7.argtypes = [vp, i32, i32, f, vp]
+        _lib.sgo_gs7.argtypes = [vp, i32, i32, i32, i32, f, f, f, f, f, vp]
+        _lib.sgo_box27.argtypes = [vp, i32, i32, vp, vp]
+        d = C.c_double
+        _lib.sgo_heat7_f64.argtypes = [vp, vp, vp, d, d, i32]
+        _lib.sgo_gs7_f64.argtypes = [vp, vp, vp, vp, vp, d, d, d, d, d, d, d, i32]
+        _cpu.cpub_create.restype = vp
+        _cpu.cpub_create.argtypes = [vp, i32, vp]
+        _cpu.cpub_destroy.argtypes = [vp]
+        _cpu.cpub_nchunks.restype = C.c_int32
+        _cpu.cpub_nchunks.argtypes = [vp]
+        _cpu.cpub_insert.argtypes = [vp, i64, vp, vp]
+        _cpu.cpub_get.argtypes = [vp, i64, vp, i32, vp]
+        _cpu.cpub_heat.restype = i32
+        _cpu.cpub_heat.argtypes = [vp, i32, i32, f, i32, i32]
+        _cpu.cpub_gs.restype = i32
+        _cpu.cpub_gs.argtypes = [vp, i32, i32, i32, i32, f, f, f, f, f, i32, i32]
+    return _lib, _cpu
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def _ptr_array(arrs):
+    return (C.c_void_p * len(arrs))(*[a.ctypes.data for a in arrs])
+
+
+class OracleGrid:
+    """CPU restatement of one SparseGridGpu block map."""
+
+    def __init__(self, size, edge=8, ptypes=(T_F32,), dim=None):
+        lib, _ = _load()
+        self.dim = dim if dim is not None else len(size)
+        self.edge = edge
+        self.bs = edge ** self.dim
+        self.size = tuple(int(s) for s in size) + (1,) * (3 - len(size))
+        self.ptypes = list(ptypes)
+        sz = np.array(self.size, dtype=np.int64)
+        pt = np.array(self.ptypes, dtype=np.int32)
+        self._h = lib.sgo_create(self.dim, edge, _ptr(sz), len(self.ptypes), _ptr(pt))
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.sgo_destroy(self._h)
+            self._h = None
+
+    # -- layout ------------------------------------------------------------
+    def set_background(self, p, value):
+        v = np.array([value], dtype=_NP[self.ptypes[p]])
+        _lib.sgo_set_background(self._h, p, _ptr(v))
+
+    @property
+    def nchunks(self) -> int:
+        return int(_lib.sgo_nchunks(self._h))
+
+    def lin_ids(self, coords) -> np.ndarray:
+        c = np.ascontiguousarray(coords, dtype=np.int64).reshape(-1, self.dim)
+        out = np.empty(len(c), dtype=np.int64)
+        _lib.sgo_lin_ids(self._h, len(c), _ptr(c), _ptr(out))
+        return out
+
+    def inv_lin(self, lin) -> np.ndarray:
+        l = np.ascontiguousarray(lin, dtype=np.int64)
+        out = np.empty((len(l), self.dim), dtype=np.int64)
+        _lib.sgo_inv_lin(self._h, len(l), _ptr(l), _ptr(out))
+        return out
+
+    def load_map(self, keys, data, mask):
+        keys = np.ascontiguousarray(keys, dtype=np.int64)
+        data = [np.ascontiguousarray(d, dtype=_NP[t]) for d, t in zip(data, self.ptypes)]
+        mask = np.ascontiguousarray(mask, dtype=np.uint8)
+        _lib.sgo_load_map(self._h, len(keys), _ptr(keys), _ptr_array(data), _ptr(mask))
+
+    def export(self):
+        """(keys[n], [data_p[(n+1)*bs]], mask[(n+1)*bs]) including the background chunk."""
+        n = self.nchunks
+        keys = np.empty(n, dtype=np.int64)
+        data = [np.empty((n + 1) * self.bs, dtype=_NP[t]) for t in self.ptypes]
+        mask = np.empty((n + 1) * self.bs, dtype=np.uint8)
+        _lib.sgo_export_map(self._h, _ptr(keys), _ptr_array(data), _ptr(mask))
+        return keys, data, mask
+
+    # -- flush -------------------------------------------------------------
+    def flush_chunks(self, slot_keys, slot_data, slot_mask, ops):
+        k = np.ascontiguousarray(slot_keys, dtype=np.int64)
+        d = [np.ascontiguousarray(x, dtype=_NP[t]) for x, t in zip(slot_data, self.ptypes)]
+        m = np.ascontiguousarray(slot_mask, dtype=np.uint8)
+        o = np.array(ops, dtype=np.int32)
+        _lib.sgo_flush_chunks(self._h, len(k), _ptr(k), _ptr_array(d), _ptr(m), _ptr(o))
+
+    def flush_points(self, lin, vals, ops, pmask=None):
+        l = np.ascontiguousarray(lin, dtype=np.int64)
+        v = [np.ascontiguousarray(x, dtype=_NP[t]) for x, t in zip(vals, self.ptypes)]
+        o = np.array(ops, dtype=np.int32)
+        pm = None if pmask is None else np.ascontiguousarray(pmask, dtype=np.uint8)
+        _lib.sgo_flush_points(self._h, len(l), _ptr(l), _ptr_array(v),
+                              None if pm is None else _ptr(pm), _ptr(o))
+
+    def insert_flush(self, coords, vals, ops):
+        self.flush_points(self.lin_ids(coords), vals, ops)
+
+    # -- neighbours / tag --------------------------------------------------
+    def find_neighbours(self, kind=NN_STAR) -> np.ndarray:
+        k = (1 << self.dim) if kind == NN_STAR else 3 ** self.dim
+        out = np.empty(self.nchunks * k, dtype=np.int64)
+        _lib.sgo_find_neighbours(self._h, kind, _ptr(out))
+        return out.reshape(self.nchunks, k)
+
+    def tag_boundaries(self, kind=NN_STAR):
+        _lib.sgo_tag_boundaries(self._h, kind)
+
+    # -- stencils ----------------------------------------------------------
+    @staticmethod
+    def _box(box):
+        if box is None:
+            return None
+        b = np.array(list(box[0]) + list(box[1]) + [0] * (6 - 2 * len(box[0])), dtype=np.int64)
+        return b
+
+    def heat7(self, src, dst, dt, box=None):
+        b = self._box(box)
+        _lib.sgo_heat7(self._h, src, dst, dt, None if b is None else _ptr(b))
+
+    def gs7(self, pu, pv, pu2, pv2, Du, Dv, F, k, dt, box=None):
+        b = self._box(box)
+        _lib.sgo_gs7(self._h, pu, pv, pu2, pv2, Du, Dv, F, k, dt, None if b is None else _ptr(b))
+
+    def box27(self, src, dst, coeff, box=None):
+        c = np.ascontiguousarray(coeff, dtype=np.float32).reshape(27)
+        b = self._box(box)
+        _lib.sgo_box27(self._h, src, dst, _ptr(c), None if b is None else _ptr(b))
+
+    def heat7_f64(self, field, dt, bck, steps):
+        a = np.ascontiguousarray(field, dtype=np.float64).copy()
+        b = a.copy()
+        _lib.sgo_heat7_f64(self._h, _ptr(a), _ptr(b), dt, bck, steps)
+        return a
+
+    def gs7_f64(self, u, v, Du, Dv, F, k, dt, bcku, bckv, steps):
+        u = np.ascontiguousarray(u, dtype=np.float64).copy()
+        v = np.ascontiguousarray(v, dtype=np.float64).copy()
+        u2, v2 = u.copy(), v.copy()
+        _lib.sgo_gs7_f64(self._h, _ptr(u), _ptr(v), _ptr(u2), _ptr(v2), Du, Dv, F, k, dt, bcku, bckv, steps)
+        return u, v
+
+    # -- point access (host get<p>(coord), BlockMapGpu.hpp:108-126) --------
+    def get(self, p, coords):
+        keys, data, mask = self.export()
+        lin = self.lin_ids(coords)
+        bkey, off = lin // self.bs, lin % self.bs
+        pos = np.searchsorted(keys, bkey)
+        pos = np.where((pos < len(keys)) & (keys[np.minimum(pos, len(keys) - 1)] == bkey), pos, len(keys))
+        idx = pos * self.bs + off
+        vals = data[p][idx]
+        bck = data[p][len(keys) * self.bs]
+        return np.where(mask[idx] & 1, vals, bck)
+
+    def mask_at(self, coords):
+        keys, _, mask = self.export()
+        lin = self.lin_ids(coords)
+        bkey, off = lin // self.bs, lin % self.bs
+        pos = np.searchsorted(keys, bkey)
+        found = (pos < len(keys)) & (keys[np.minimum(pos, max(len(keys) - 1, 0))] == bkey)
+        return np.where(found, mask[np.where(found, pos, len(keys)) * self.bs + off], 0)
+
+
+class CpuSgrid:
+    """sgrid_cpu-style CPU baseline (16^3 hashed chunks)."""
+
+    def __init__(self, size, nprop, bck):
+        _, cpu = _load()
+        sz = np.array(size, dtype=np.int64)
+        b = np.array(bck, dtype=np.float32)
+        self.nprop = nprop
+        self._h = cpu.cpub_create(_ptr(sz), nprop, _ptr(b))
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _cpu is not None:
+            _cpu.cpub_destroy(self._h)
+            self._h = None
+
+    @property
+    def nchunks(self):
+        return int(_cpu.cpub_nchunks(self._h))
+
+    def insert(self, coords, vals):
+        c = np.ascontiguousarray(coords, dtype=np.int64).reshape(-1, 3)
+        v = [np.ascontiguousarray(x, dtype=np.float32) for x in vals]
+        _cpu.cpub_insert(self._h, len(c), _ptr(c), _ptr_array(v))
+
+    def get(self, p, coords):
+        c = np.ascontiguousarray(coords, dtype=np.int64).reshape(-1, 3)
+        out = np.empty(len(c), dtype=np.float32)
+        _cpu.cpub_get(self._h, len(c), _ptr(c), p, _ptr(out))
+        return out
+
+    def heat(self, src, dst, dt, steps, threads=1) -> int:
+        return int(_cpu.cpub_heat(self._h, src, dst, dt, steps, threads))
+
+    def gs(self, pu, pv, pu2, pv2, Du, Dv, F, k, dt, steps, threads=1) -> int:
+        return int(_cpu.cpub_gs(self._h, pu, pv, pu2, pv2, Du, Dv, F, k, dt, steps, threads))
