@@ -164,10 +164,29 @@ int sgb_download_map(sgb_grid* g, int64_t* keys_host, void* const* data_host, ui
 /* countExistingElements / countBoundaryElements (SparseGridGpu.hpp:2422-2474). */
 int sgb_count_existing(sgb_grid* g, int64_t* existing, int64_t* padding, sgb_stream s);
 
+/* Per-chunk offsets of the existing points: offsets_dev[i] = number of EXIST
+ * points in chunks 0..i-1, offsets_dev[n] = total (int64, n + 1 entries).
+ * The calc_exist_points + scan step of tagBoundaries(...,
+ * CALCULATE_EXISTING_POINTS) (SparseGridGpu.hpp:2355-2387,
+ * SparseGridGpu_kernels.cuh:1194-1225); totals below 2^32 points. */
+int sgb_existing_offsets(sgb_grid* g, int64_t* offsets_dev, sgb_stream s);
+
 /* get<p>(coord) for a batch of points (SparseGridGpu_ker.cuh:409-413):
  * value if the point exists, background otherwise.  coords dev int32 [n][3],
  * out dev n elements of the property's type. */
 int sgb_get(sgb_grid* g, int64_t n, const int32_t* coords_dev, int prop, void* out_dev, sgb_stream s);
+
+/* Scene builder (no reference counterpart; reference users insert points
+ * from their own kernels): replace the block map by the union of nballs
+ * balls (host float [nballs][4] = cx, cy, cz, r; a point exists when
+ * |p - c|^2 <= r^2), and fill the listed properties (host ids):
+ *   init 0 (SGB_INIT_UNIFORM):    props[0] = U[0,1) from a hash of (seed, point id)
+ *   init 1 (SGB_INIT_GRAY_SCOTT): props[0] = u = 1, props[1] = v = 0, except
+ *        in the 6^3 cube [floor(c)-3, floor(c)+3) of every ball centre:
+ *        u = 0.5(1 + 0.01a), v = 0.25(1 + 0.01b), a, b ~ U[-1,1)
+ * Every other property is set to its background.  At most 64 balls. */
+int sgb_build_balls(sgb_grid* g, int nballs, const float* balls_host, int init, uint64_t seed, const int* props,
+                    sgb_stream s);
 
 /* Device-side error word of the last kernels (bounded waits that gave up,
  * out-of-domain inserts).  Synchronises the stream; clears the word. */
@@ -204,6 +223,11 @@ int sgb_batch_slot_steps(const sgb_batch* b, int slot, int64_t* done);
 /* Copy a slot's fields back into g's src/dst properties (g must have the
  * block map the slot was added from); *final_is_dst as in sgb_run_steps. */
 int sgb_batch_extract(sgb_batch* b, int slot, sgb_grid* g, int* final_is_dst, sgb_stream s);
+/* Copy a slot's block map and current fields to host memory (any pointer may
+ * be NULL): keys[n], mask[n*bs], fields[j][n*bs] for the np source fields,
+ * holding the state after the steps the slot has done. */
+int sgb_batch_read(sgb_batch* b, int slot, int64_t* keys_host, uint8_t* mask_host, float* const* fields_host,
+                   int64_t* nchunks, sgb_stream s);
 int sgb_batch_info(const sgb_batch* b, int* ngrids, int64_t* nchunks, int64_t* bytes);
 /* Launch configuration of the batched kernels (as sgb_set_launch_config). */
 int sgb_batch_set_launch_config(sgb_batch* b, int ctas_per_sm, int stages);

@@ -49,7 +49,9 @@ SIGNATURES = {
     "sgb_load_map_dev": (_i32, [_vp, _i64, _vp, _vp, _vp, _vp]),
     "sgb_download_map": (_i32, [_vp, _vp, _vp, _vp, _vp]),
     "sgb_count_existing": (_i32, [_vp, _vp, _vp, _vp]),
+    "sgb_existing_offsets": (_i32, [_vp, _vp, _vp]),
     "sgb_get": (_i32, [_vp, _i64, _vp, _i32, _vp, _vp]),
+    "sgb_build_balls": (_i32, [_vp, _i32, _vp, _i32, C.c_uint64, _vp, _vp]),
     "sgb_check_device_errors": (_i32, [_vp, _vp]),
     "sgb_device_bytes": (_i32, [_vp, _vp]),
     "sgb_set_launch_config": (_i32, [_vp, _i32, _i32]),
@@ -60,6 +62,7 @@ SIGNATURES = {
     "sgb_batch_step": (_i32, [_vp, _i32, _i32, _vp]),
     "sgb_batch_slot_steps": (_i32, [_vp, _i32, _vp]),
     "sgb_batch_extract": (_i32, [_vp, _i32, _vp, _vp, _vp]),
+    "sgb_batch_read": (_i32, [_vp, _i32, _vp, _vp, _vp, _vp, _vp]),
     "sgb_batch_info": (_i32, [_vp, _vp, _vp, _vp]),
     "sgb_batch_set_launch_config": (_i32, [_vp, _i32, _i32]),
 }

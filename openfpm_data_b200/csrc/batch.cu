@@ -222,6 +222,10 @@ int sgb_batch_add(sgb_batch* b, sgb_grid* g, int kind, const int* src, const int
     }
     SGB_TRY(batch_compact(b, s));
     SGB_TRY(ensure_neighbours(g, SGB_NN_STAR, s));
+    for (int p = 0; p < b->np; ++p) {  // batched kernels rely on background-filled empty points
+        SGB_TRY(ensure_clean(g, src[p], s));
+        SGB_TRY(ensure_clean(g, dst[p], s));
+    }
     const int bs = g->geo.bs;
     SGB_TRY(batch_reserve(b, b->n + g->n));
     const int64_t off = b->n;
@@ -355,3 +359,26 @@ int sgb_batch_info(const sgb_batch* b, int* ngrids, int64_t* nchunks, int64_t* b
 }
 
 }  // extern "C"
+
+extern "C" int sgb_batch_read(sgb_batch* b, int slot, int64_t* keys, uint8_t* mask, float* const* fields,
+                              int64_t* nchunks, sgb_stream stream) {
+    if (!b || slot < 0 || slot >= (int)b->slots.size() || !b->slots[slot].live) return SGB_EINVAL;
+    const auto& sl = b->slots[slot];
+    cudaStream_t s = (cudaStream_t)stream;
+    const int bs = b->edge * b->edge * b->edge;
+    if (nchunks) *nchunks = sl.n;
+    int64_t done = 0;
+    sgb_batch_slot_steps(b, slot, &done);
+    const int cur = (int)(done & 1);  // buffer holding the latest state
+    if (sl.n > 0) {
+        if (keys) SGB_CUDA(cudaMemcpyAsync(keys, b->keys.as<int64_t>() + sl.off, sl.n * 8, cudaMemcpyDeviceToHost, s));
+        if (mask) SGB_CUDA(cudaMemcpyAsync(mask, b->mask.as<uint8_t>() + sl.off * bs, sl.n * bs, cudaMemcpyDeviceToHost, s));
+        if (fields)
+            for (int p = 0; p < b->np; ++p)
+                if (fields[p])
+                    SGB_CUDA(cudaMemcpyAsync(fields[p], b->field[cur][p].as<float>() + sl.off * bs, sl.n * bs * 4,
+                                             cudaMemcpyDeviceToHost, s));
+    }
+    SGB_CUDA(cudaStreamSynchronize(s));
+    return SGB_OK;
+}

@@ -1,4 +1,5 @@
 // Grid handles, buffers, map upload/download, staged inserts and point reads.
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -28,7 +29,9 @@ int DevBuf::reserve(size_t need) {
     cudaError_t e = cudaMalloc(&q, nb);
     if (e != cudaSuccess) return cuda_status(e, "cudaMalloc");
     if (p && bytes) {
-        e = cudaMemcpy(q, p, bytes, cudaMemcpyDeviceToDevice);
+        // work queued on any stream may still write the old buffer
+        e = cudaDeviceSynchronize();
+        if (e == cudaSuccess) e = cudaMemcpy(q, p, bytes, cudaMemcpyDeviceToDevice);
         if (e != cudaSuccess) {
             cudaFree(q);
             return cuda_status(e, "cudaMemcpy(grow)");
@@ -140,6 +143,49 @@ static void invalidate_derived(sgb_grid* g) {
     g->bits_valid = false;
 }
 
+// Points whose mask byte is 0 take the background value: 16 mask bytes per
+// thread step, element stores only where needed.
+template <typename T>
+__global__ void k_sanitize(const uint8_t* mask, T* data, int64_t total, T bck) {
+    const int64_t words = total / 16;
+    for (int64_t w = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; w < words; w += (int64_t)gridDim.x * blockDim.x) {
+        const uint4 m = reinterpret_cast<const uint4*>(mask)[w];
+        const unsigned mw[4] = {m.x, m.y, m.z, m.w};
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            if (mw[q] == 0x01010101u) continue;
+#pragma unroll
+            for (int b = 0; b < 4; ++b)
+                if (((mw[q] >> (8 * b)) & 0xffu) == 0) data[w * 16 + q * 4 + b] = bck;
+        }
+    }
+}
+
+int sanitize_prop(sgb_grid* g, int p, cudaStream_t s) {
+    const int64_t total = g->n * (int64_t)g->geo.bs;  // bs is a multiple of 16
+    if (total > 0) {
+        const unsigned blocks = (unsigned)std::min<int64_t>(8192, (total / 16 + 255) / 256);
+        const uint8_t* m = g->mask.as<uint8_t>();
+        switch (elem_size(g->ptype[p])) {
+            case 1: k_sanitize<uint8_t><<<blocks, 256, 0, s>>>(m, g->data[p].as<uint8_t>(), total, (uint8_t)bck_pattern(g, p)); break;
+            case 4: k_sanitize<uint32_t><<<blocks, 256, 0, s>>>(m, g->data[p].as<uint32_t>(), total, (uint32_t)bck_pattern(g, p)); break;
+            default: k_sanitize<uint64_t><<<blocks, 256, 0, s>>>(m, g->data[p].as<uint64_t>(), total, bck_pattern(g, p)); break;
+        }
+        SGB_CUDA(cudaGetLastError());
+    }
+    g->clean[p] = true;
+    return SGB_OK;
+}
+
+int ensure_clean(sgb_grid* g, int p, cudaStream_t s) { return g->clean[p] ? SGB_OK : sanitize_prop(g, p, s); }
+
+int fill_background_all(sgb_grid* g, int p, cudaStream_t s) {
+    const int es = elem_size(g->ptype[p]);
+    SGB_TRY(fill(g->data[p].p, (g->n + 1) * g->geo.bs, es, bck_pattern(g, p), s));
+    g->clean[p] = true;
+    return SGB_OK;
+}
+
 // grid_smb::LinId on device (src/Grid/Geometry/grid_smb.hpp:176-190), with a
 // domain check that the reference does not do.
 __global__ void k_lin_from_coords(const int32_t* coords, int64_t n, Geometry geo, int64_t* lin, unsigned* err) {
@@ -207,6 +253,24 @@ __global__ void k_get(const int32_t* coords, int64_t n, Geometry geo, const int6
     // BlockMapGpu_ker::get (src/SparseGridGpu/BlockMapGpu_ker.cuh:117-135)
     const size_t idx = (size_t)pos * geo.bs + l;
     out[i] = (mask[idx] & 1) ? data[idx] : data[(size_t)nchunks * geo.bs + l];
+}
+
+// EXIST points per chunk: one warp per chunk, one ballot per 32 mask bytes
+// (calc_exist_points, SparseGridGpu_kernels.cuh:1194-1225).
+__global__ void k_chunk_counts(const uint8_t* mask, int64_t n, int bs, uint32_t* counts) {
+    const int64_t chunk = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (chunk >= n) return;
+    const uint8_t* m = mask + (size_t)chunk * bs;
+    uint32_t c = 0;
+    for (int r = 0; r < bs / 32; ++r) c += __popc(__ballot_sync(0xffffffffu, m[r * 32 + lane] & 1));
+    if (lane == 0) counts[chunk] = c;
+}
+
+__global__ void k_offsets_i64(const uint32_t* scanned, const uint32_t* total, int64_t n, int64_t* out) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n) out[i] = scanned[i];
+    else if (i == n) out[n] = *total;
 }
 
 __global__ void k_count(const uint8_t* mask, int64_t total, unsigned long long* out) {
@@ -320,6 +384,7 @@ int sgb_set_background(sgb_grid* g, int prop, const void* value) {
     std::memcpy(g->bck[prop], value, elem_size(g->ptype[prop]));
     const int bs = g->geo.bs, es = elem_size(g->ptype[prop]);
     SGB_TRY(fill(g->data[prop].as<unsigned char>() + (size_t)g->n * bs * es, bs, es, bck_pattern(g, prop), 0));
+    SGB_TRY(sanitize_prop(g, prop, 0));  // points without EXIST read the new background
     SGB_CUDA(cudaStreamSynchronize(0));
     return SGB_OK;
 }
@@ -367,12 +432,15 @@ int sgb_index_buffer(sgb_grid* g, const int64_t** dev) {
 int sgb_data_buffer(sgb_grid* g, int prop, void** dev) {
     if (!g || !dev || prop < 0 || prop >= g->nprop) return SGB_EINVAL;
     *dev = g->data[prop].p;
+    g->clean[prop] = false;  // the caller may write any point
     return SGB_OK;
 }
 
 int sgb_mask_buffer(sgb_grid* g, uint8_t** dev) {
     if (!g || !dev) return SGB_EINVAL;
     *dev = g->mask.as<uint8_t>();
+    for (int p = 0; p < g->nprop; ++p) g->clean[p] = false;  // existence may change
+    g->bits_valid = false;
     return SGB_OK;
 }
 
@@ -392,6 +460,7 @@ static int load_map_impl(sgb_grid* g, int64_t n, const int64_t* keys, const void
     }
     g->n = n;
     SGB_TRY(write_background(g, n, s, g->data, g->mask));
+    for (int p = 0; p < g->nprop; ++p) SGB_TRY(sanitize_prop(g, p, s));
     invalidate_derived(g);
     return SGB_OK;
 }
@@ -440,6 +509,26 @@ int sgb_count_existing(sgb_grid* g, int64_t* existing, int64_t* padding, sgb_str
     unsigned long long* h = (unsigned long long*)g->hscratch.p;
     if (existing) *existing = (int64_t)h[0];
     if (padding) *padding = (int64_t)h[1];
+    return SGB_OK;
+}
+
+int sgb_existing_offsets(sgb_grid* g, int64_t* offsets, sgb_stream stream) {
+    if (!g || !offsets) return SGB_EINVAL;
+    cudaStream_t s = (cudaStream_t)stream;
+    const int64_t n = g->n;
+    DevBuf& counts = g->scratch[7];
+    DevBuf& scanned = g->scratch[8];
+    SGB_TRY(counts.ensure((size_t)(n + 1) * 4));
+    SGB_TRY(scanned.ensure((size_t)(n + 2) * 4));
+    if (n > 0) {
+        k_chunk_counts<<<(unsigned)((n * 32 + 255) / 256), 256, 0, s>>>(g->mask.as<uint8_t>(), n, g->geo.bs,
+                                                                       counts.as<uint32_t>());
+        SGB_CUDA(cudaGetLastError());
+    }
+    uint32_t* total = scanned.as<uint32_t>() + n + 1;
+    SGB_TRY(scan_exclusive_u32(counts.as<uint32_t>(), scanned.as<uint32_t>(), n, total, &g->scratch[6], s));
+    k_offsets_i64<<<(unsigned)((n + 1 + 255) / 256), 256, 0, s>>>(scanned.as<uint32_t>(), total, n, offsets);
+    SGB_CUDA(cudaGetLastError());
     return SGB_OK;
 }
 

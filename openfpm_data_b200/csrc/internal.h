@@ -117,6 +117,13 @@ struct sgb_grid {
     sgb::DevBuf bits;     // uint64 existence bitmaps, bs/64 words per chunk
     bool bits_valid = false;
 
+    // clean[p]: every point of property p whose mask byte is 0 holds the
+    // background value.  The reference substitutes the background for such
+    // points whenever it reads them (loadGhostBlock, BlockMapGpu_ker::get);
+    // keeping them filled lets the stencils read chunk data without a mask
+    // test per neighbour.  Cleared when the caller gets a writable pointer.
+    bool clean[sgb::kMaxProps] = {true, true, true, true, true, true, true, true};
+
     // flush / scan / sort scratch
     sgb::DevBuf scratch[12];
     sgb::HostScratch hscratch;
@@ -145,6 +152,11 @@ int scan_exclusive_u32(const uint32_t* in, uint32_t* out, int64_t n, uint32_t* t
 
 // buffers
 int grid_reserve(sgb_grid* g, int64_t chunks, bool keep);
+// fill the mask-0 points of property p with its background (sets clean[p])
+int sanitize_prop(sgb_grid* g, int p, cudaStream_t s);
+// fill every point (n + 1 chunks) of property p with its background
+int fill_background_all(sgb_grid* g, int p, cudaStream_t s);
+int ensure_clean(sgb_grid* g, int p, cudaStream_t s);
 int write_background(sgb_grid* g, int64_t pos, cudaStream_t s, DevBuf* data, DevBuf& mask);
 
 }  // namespace sgb

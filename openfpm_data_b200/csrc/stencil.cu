@@ -6,15 +6,9 @@
 // the 10^3 tile with one scalar load per point, the user functor computes,
 // storeBlock writes back.
 //
-// Here (8^3 chunks, 7-point): a persistent, warp-specialised kernel.  Each CTA
-// owns a contiguous range of chunk positions.  One producer warp streams, per
-// chunk, the source tiles and the mask tile with 1-D bulk copies (TMA engine,
-// cp.async.bulk) and the four y/z halo faces with cp.async into an S-stage
-// shared-memory ring guarded by mbarriers.  The x halo is never fetched: when
-// the -x / +x neighbour chunk exists it is the previous / next position of
-// the sorted index (its id differs by one), which sits in the ring already,
-// so the consumers keep a stage until the chunk after it is done.  Eight
-// consumer warps compute from shared memory and store straight to HBM.
+// Here 7-point stencils on 8^3 chunks run the pipelined kernel of
+// stencil8.cu; this file holds the generic one-chunk-per-CTA tile kernel
+// (BOX27, 4^3 chunks, cross-checks), parameter handling and dispatch.
 //
 // The same kernels run a batch of grids concatenated into one block map: a
 // per-chunk grid id selects the grid's parameters and its ping-pong buffer
@@ -36,210 +30,6 @@
 #include "stencil.cuh"
 
 namespace sgb {
-
-// ------------------------------------------------------------------ 8^3 pipelined kernel
-template <int NP>
-struct alignas(16) Stage8 {
-    float tile[NP][512];
-    float ym[NP][64], yp[NP][64], zm[NP][64], zp[NP][64];
-    uint8_t mt[512];
-    uint8_t mym[64], myp[64], mzm[64], mzp[64];
-    GridInfo gi;
-    int32_t nn[8];
-    int64_t key;
-    int32_t par, active;
-};
-
-template <int KIND, int NP>
-__global__ void __launch_bounds__(kThreads, 2)
-    k_stencil7_e8(FieldSet fs, const uint8_t* __restrict__ mask, const int32_t* __restrict__ nn,
-                  const int64_t* __restrict__ keys, const int32_t* __restrict__ gid, const GridInfo* __restrict__ grids,
-                  GridInfo g0, int64_t n, Geometry geo, StencilParams prm, int64_t t, int S, unsigned* err) {
-    extern __shared__ __align__(128) unsigned char smem_raw[];
-    Stage8<NP>* stage = reinterpret_cast<Stage8<NP>*>(smem_raw);
-    uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + (size_t)S * sizeof(Stage8<NP>));
-    uint64_t* empty = full + S;
-
-    const int64_t nct = gridDim.x;
-    const int64_t c0 = n * blockIdx.x / nct, c1 = n * (blockIdx.x + 1) / nct;
-    const int64_t lo = c0 > 0 ? c0 - 1 : 0, hi = c1 + 1 < n ? c1 + 1 : n;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-
-    if (threadIdx.x == 0) {
-        for (int s = 0; s < S; ++s) {
-            mbar_init(&full[s], 33);               // 32 cp.async arrivals + 1 expect_tx arrival
-            mbar_init(&empty[s], kConsumerWarps);  // one arrival per consumer warp
-        }
-        mbar_fence_init();
-    }
-    __syncthreads();
-    if (c0 >= c1) return;
-
-    if (warp == kConsumerWarps) {
-        // ------------------------------------------------------------ producer
-        int64_t q = 0;
-        bool ok = true;
-        for (; q < hi - lo; ++q) {
-            const int64_t c = lo + q;
-            const int s = (int)(q % S);
-            const uint32_t k = (uint32_t)(q / S);
-            if (q >= S && !mbar_wait_bounded(&empty[s], (k - 1) & 1u, err)) {
-                ok = false;
-                break;
-            }
-            Stage8<NP>& st = stage[s];
-            const GridInfo gi = grids ? grids[gid[c]] : g0;
-            const bool active = t >= gi.start && t < gi.start + gi.nsteps;
-            const int par = (int)((t - gi.start) & 1);
-            const int32_t nbv = lane < 8 ? nn[c * 8 + lane] : -1;
-            if (lane < 8) st.nn[lane] = nbv;
-            if (lane == 0) {
-                st.key = keys[c];
-                st.gi = gi;
-                st.par = par;
-                st.active = active;
-            }
-            const int32_t nby0 = __shfl_sync(0xffffffffu, nbv, 2), nby1 = __shfl_sync(0xffffffffu, nbv, 3),
-                          nby2 = __shfl_sync(0xffffffffu, nbv, 4), nby3 = __shfl_sync(0xffffffffu, nbv, 5);
-            __syncwarp();
-            if (active) {
-                const float* s0 = fs.in[par][0];
-                const float* s1 = fs.in[par][NP - 1];
-                if (lane == 0) {
-                    mbar_arrive_expect_tx(&full[s], NP * 2048 + 512);
-                    bulk_g2s(st.tile[0], s0 + c * 512, 2048, &full[s]);
-                    if (NP == 2) bulk_g2s(st.tile[NP - 1], s1 + c * 512, 2048, &full[s]);
-                    bulk_g2s(st.mt, mask + c * 512, 512, &full[s]);
-                }
-                for (int tk = lane; tk < NP * 64 + 24; tk += 32) {
-                    if (tk < NP * 64) {
-                        const int p = tk >> 6, r = tk & 63, f = r >> 4, piece = r & 15;
-                        const int32_t nb = f == 0 ? nby0 : f == 1 ? nby1 : f == 2 ? nby2 : nby3;
-                        if (nb < 0) continue;
-                        const float* base = (p == 0 ? s0 : s1) + (int64_t)nb * 512;
-                        const int zz = piece >> 1, hh = (piece & 1) * 4;
-                        if (f == 0) cp_async16(&st.ym[p][zz * 8 + hh], base + zz * 64 + 56 + hh);
-                        else if (f == 1) cp_async16(&st.yp[p][zz * 8 + hh], base + zz * 64 + hh);
-                        else if (f == 2) cp_async16(&st.zm[p][piece * 4], base + 448 + piece * 4);
-                        else cp_async16(&st.zp[p][piece * 4], base + piece * 4);
-                    } else {
-                        const int r = tk - NP * 64;
-                        const int f = r < 8 ? 0 : r < 16 ? 1 : r < 20 ? 2 : 3;
-                        const int32_t nb = f == 0 ? nby0 : f == 1 ? nby1 : f == 2 ? nby2 : nby3;
-                        if (nb < 0) continue;
-                        const uint8_t* base = mask + (int64_t)nb * 512;
-                        if (f == 0) cp_async8(&st.mym[r * 8], base + r * 64 + 56);
-                        else if (f == 1) cp_async8(&st.myp[(r - 8) * 8], base + (r - 8) * 64);
-                        else if (f == 2) cp_async16(&st.mzm[(r - 16) * 16], base + 448 + (r - 16) * 16);
-                        else cp_async16(&st.mzp[(r - 20) * 16], base + (r - 20) * 16);
-                    }
-                }
-            } else if (lane == 0) {
-                mbar_arrive(&full[s]);
-            }
-            cp_async_arrive_noinc(&full[s]);
-        }
-        if (!ok) {
-            // drain own copies in flight before leaving
-            cp_async_wait_all();
-            for (int64_t r = q - 1; r >= 0 && r >= q - S; --r)
-                mbar_wait_bounded(&full[r % S], (uint32_t)(r / S) & 1u, err, 100000000ull);
-        }
-        return;
-    }
-
-    // ---------------------------------------------------------------- consumers
-    const int tid = threadIdx.x;
-    const int z = tid >> 5, y = (tid >> 2) & 7, x0 = (tid & 3) << 1;
-    const int o0 = z * 64 + y * 8 + x0;
-    for (int64_t i = c0; i < c1; ++i) {
-        const int64_t q = i - lo;
-        const int s = (int)(q % S);
-        if (!mbar_wait_bounded(&full[s], (uint32_t)(q / S) & 1u, err)) break;
-        const bool has_next = i + 1 < hi;
-        const int sn = (int)((q + 1) % S);
-        if (has_next && !mbar_wait_bounded(&full[sn], (uint32_t)((q + 1) / S) & 1u, err)) break;
-        const Stage8<NP>& st = stage[s];
-        if (st.active) {
-            const Stage8<NP>& pv = stage[(s + S - 1) % S];
-            const Stage8<NP>& nx = stage[sn];
-            const bool xm_ok = st.nn[0] == (int32_t)(i - 1);
-            const bool xp_ok = st.nn[1] == (int32_t)(i + 1);
-            const bool ym_ok = st.nn[2] >= 0, yp_ok = st.nn[3] >= 0, zm_ok = st.nn[4] >= 0, zp_ok = st.nn[5] >= 0;
-            const float bck[2] = {st.gi.bck[0], st.gi.bck[1]};
-            bool act[2];
-            {
-                int64_t cx = 0, cy = 0, cz = 0;
-                if (prm.has_box) {
-                    const int64_t key = st.key;
-                    cx = (key % geo.bsz[0]) * 8;
-                    cy = ((key / geo.bsz[0]) % geo.bsz[1]) * 8;
-                    cz = (key / (geo.bsz[0] * geo.bsz[1])) * 8;
-                }
-#pragma unroll
-                for (int j = 0; j < 2; ++j) {
-                    const uint8_t m = st.mt[o0 + j];
-                    act[j] = (m & 1) && !(m & 2);
-                    if (prm.has_box) act[j] = act[j] && in_box(prm, cx + x0 + j, cy + y, cz + z);
-                }
-            }
-            const bool need = KIND == SGB_HEAT7 || act[0] || act[1];
-            float res[NP][2];
-            if (need) {
-#pragma unroll
-                for (int p = 0; p < NP; ++p) {
-                    float cv[2], xmv[2], xpv[2], ymv[2], ypv[2], zmv[2], zpv[2];
-#pragma unroll
-                    for (int j = 0; j < 2; ++j) {
-                        const int x = x0 + j, o = o0 + j;
-                        cv[j] = st.mt[o] ? st.tile[p][o] : bck[p];
-                        if (x > 0) xmv[j] = st.mt[o - 1] ? st.tile[p][o - 1] : bck[p];
-                        else xmv[j] = (xm_ok && pv.mt[o + 7]) ? pv.tile[p][o + 7] : bck[p];
-                        if (x < 7) xpv[j] = st.mt[o + 1] ? st.tile[p][o + 1] : bck[p];
-                        else xpv[j] = (xp_ok && nx.mt[o - 7]) ? nx.tile[p][o - 7] : bck[p];
-                        if (y > 0) ymv[j] = st.mt[o - 8] ? st.tile[p][o - 8] : bck[p];
-                        else ymv[j] = (ym_ok && st.mym[z * 8 + x]) ? st.ym[p][z * 8 + x] : bck[p];
-                        if (y < 7) ypv[j] = st.mt[o + 8] ? st.tile[p][o + 8] : bck[p];
-                        else ypv[j] = (yp_ok && st.myp[z * 8 + x]) ? st.yp[p][z * 8 + x] : bck[p];
-                        if (z > 0) zmv[j] = st.mt[o - 64] ? st.tile[p][o - 64] : bck[p];
-                        else zmv[j] = (zm_ok && st.mzm[y * 8 + x]) ? st.zm[p][y * 8 + x] : bck[p];
-                        if (z < 7) zpv[j] = st.mt[o + 64] ? st.tile[p][o + 64] : bck[p];
-                        else zpv[j] = (zp_ok && st.mzp[y * 8 + x]) ? st.zp[p][y * 8 + x] : bck[p];
-                    }
-#pragma unroll
-                    for (int j = 0; j < 2; ++j) {
-                        if (KIND == SGB_HEAT7)
-                            res[p][j] = act[j] ? heat_update(cv[j], xmv[j], xpv[j], ymv[j], ypv[j], zmv[j], zpv[j],
-                                                             st.gi.dt)
-                                               : cv[j];
-                        else
-                            res[p][j] = lap7(cv[j], xmv[j], xpv[j], ymv[j], ypv[j], zmv[j], zpv[j]);
-                    }
-                }
-            }
-            const int64_t gidx = i * 512 + o0;
-            float* d0 = fs.out[st.par][0];
-            if (KIND == SGB_HEAT7) {
-                *reinterpret_cast<float2*>(d0 + gidx) = make_float2(res[0][0], res[0][1]);
-            } else if (need) {
-                float* d1 = fs.out[st.par][NP - 1];
-#pragma unroll
-                for (int j = 0; j < 2; ++j) {
-                    if (!act[j]) continue;
-                    const float u = st.tile[0][o0 + j], v = st.tile[NP - 1][o0 + j];
-                    float un, vn;
-                    gs_update(u, v, res[0][j], res[NP - 1][j], st.gi, un, vn);
-                    d0[gidx + j] = un;
-                    d1[gidx + j] = vn;
-                }
-            }
-        }
-        if (i - 1 >= lo) {
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&empty[(s + S - 1) % S]);
-        }
-    }
-}
 
 // ------------------------------------------------------------------ generic tile kernel
 // Any edge, any of the three stencils: one CTA per chunk (grid-stride), the
@@ -396,25 +186,7 @@ GridInfo grid_info_of(const StencilParams& prm) {
 
 int launch_fields(const LaunchDesc& L, cudaStream_t s) {
     if (L.n == 0) return SGB_OK;
-    const int np = L.kind == SGB_GS7 ? 2 : 1;
-    if (L.kind != SGB_BOX27 && L.edge == 8 && !L.use_tile) {
-        const int S = L.stages;
-        if (np == 2) {
-            const size_t smem = (size_t)S * sizeof(Stage8<2>) + 2 * S * 8;
-            auto kern = k_stencil7_e8<SGB_GS7, 2>;
-            SGB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            kern<<<L.ctas, kThreads, smem, s>>>(L.fs, L.mask, L.nn, L.keys, L.gid, L.grids, L.g0, L.n, L.geo, L.prm,
-                                                L.t, S, L.err);
-        } else {
-            const size_t smem = (size_t)S * sizeof(Stage8<1>) + 2 * S * 8;
-            auto kern = k_stencil7_e8<SGB_HEAT7, 1>;
-            SGB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            kern<<<L.ctas, kThreads, smem, s>>>(L.fs, L.mask, L.nn, L.keys, L.gid, L.grids, L.g0, L.n, L.geo, L.prm,
-                                                L.t, S, L.err);
-        }
-        SGB_CUDA(cudaGetLastError());
-        return SGB_OK;
-    }
+    if (L.kind != SGB_BOX27 && L.edge == 8 && !L.use_tile) return launch_e8(L, s);
     const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>(L.n, (int64_t)L.num_sms * 8));
 #define SGB_TILE(K, E) \
     k_stencil_tile<K, E><<<blocks, 256, 0, s>>>(L.fs, L.mask, L.nn, L.keys, L.gid, L.grids, L.g0, L.n, L.geo, L.prm, L.t)
@@ -439,6 +211,7 @@ int launch_stencil_impl(sgb_grid* g, int kind, const int* src, const int* dst, c
     const int nnk = kind == SGB_BOX27 ? SGB_NN_FULL : SGB_NN_STAR;
     SGB_TRY(ensure_neighbours(g, nnk, s));
     const int np = kind == SGB_GS7 ? 2 : 1;
+    for (int j = 0; j < np; ++j) SGB_TRY(ensure_clean(g, src[j], s));
     LaunchDesc L;
     std::memset(&L, 0, sizeof(L));
     L.kind = kind;
@@ -463,7 +236,9 @@ int launch_stencil_impl(sgb_grid* g, int kind, const int* src, const int* dst, c
     L.prm = prm;
     L.t = 0;
     L.err = g->err.as<unsigned>();
-    return launch_fields(L, s);
+    SGB_TRY(launch_fields(L, s));
+    if (kind == SGB_HEAT7) g->clean[dst[0]] = true;  // every point of dst was written from the tile
+    return SGB_OK;
 }
 
 int launch_stencil(sgb_grid* g, int kind, const int* src, const int* dst, const StencilParams& prm, cudaStream_t s) {
@@ -504,6 +279,11 @@ int sgb_run_steps(sgb_grid* g, int kind, const int* src, const int* dst, const f
     if (final_is_dst) *final_is_dst = nsteps % 2;
     if (nsteps == 0 || g->n == 0) return SGB_OK;
     SGB_TRY(ensure_neighbours(g, kind == SGB_BOX27 ? SGB_NN_FULL : SGB_NN_STAR, s));
+    // both halves of the ping-pong are read as sources; no sanitising inside a capture
+    for (int j = 0; j < (kind == SGB_GS7 ? 2 : 1); ++j) {
+        SGB_TRY(ensure_clean(g, src[j], s));
+        SGB_TRY(ensure_clean(g, dst[j], s));
+    }
     if (!use_graph) {
         for (int k = 0; k < nsteps; ++k) {
             if (k % 2 == 0) SGB_TRY(launch_stencil(g, kind, src, dst, fwd, s));

@@ -71,6 +71,7 @@ struct LaunchDesc {
 };
 
 int launch_fields(const LaunchDesc& L, cudaStream_t s);
+int launch_e8(const LaunchDesc& L, cudaStream_t s);  // pipelined 8^3 kernel (stencil8.cu)
 GridInfo grid_info_of(const StencilParams& prm);
 
 // Capture `body(stream)` into a CUDA graph, launch it on `s`, wait for it.

@@ -219,6 +219,19 @@ class SparseGridGpu:
         L.check(self._lib.sgb_count_existing(self._h, None, C.byref(p), _stream(stream)), "sgb_count_existing")
         return p.value
 
+    def build_balls(self, balls: np.ndarray, init: int, seed: int, props: Sequence[int], stream=None) -> None:
+        """Replace the block map by a union of balls [k,4] = (cx, cy, cz, r) (sgb_build_balls)."""
+        b = np.ascontiguousarray(balls, dtype=np.float32).reshape(-1, 4)
+        L.check(self._lib.sgb_build_balls(self._h, len(b), b.ctypes.data_as(C.c_void_p), int(init),
+                                          C.c_uint64(int(seed) & (2 ** 64 - 1)), _i32arr(list(props)),
+                                          _stream(stream)), "sgb_build_balls")
+
+    def existing_offsets(self, stream=None) -> torch.Tensor:
+        """int64 [nchunks + 1]: existing points before each chunk, total last."""
+        out = torch.empty(self.nchunks + 1, dtype=torch.int64, device=f"cuda:{self.device}")
+        L.check(self._lib.sgb_existing_offsets(self._h, out.data_ptr(), _stream(stream)), "sgb_existing_offsets")
+        return out
+
     def get(self, prop: int, coords: torch.Tensor, stream=None) -> torch.Tensor:
         c = coords.to(device=f"cuda:{self.device}", dtype=torch.int32).contiguous()
         out = torch.empty(c.shape[0], dtype=_TORCH[self.ptypes[prop]], device=f"cuda:{self.device}")
@@ -277,6 +290,23 @@ class Batch:
         L.check(self._lib.sgb_batch_extract(self._h, slot, g.handle, C.byref(fin), _stream(stream)),
                 "sgb_batch_extract")
         return bool(fin.value)
+
+    def nchunks(self, slot: int) -> int:
+        n = C.c_int64()
+        L.check(self._lib.sgb_batch_read(self._h, slot, None, None, None, C.byref(n), None), "sgb_batch_read")
+        return n.value
+
+    def read(self, slot: int, nfields: int, bs: int = 512, stream=None):
+        """(keys, mask, [fields]) of a slot's current state as numpy arrays."""
+        n = self.nchunks(slot)
+        keys = np.empty(n, np.int64)
+        mask = np.empty(n * bs, np.uint8)
+        fields = [np.empty(n * bs, np.float32) for _ in range(nfields)]
+        ptrs = (C.c_void_p * nfields)(*[f.ctypes.data for f in fields])
+        L.check(self._lib.sgb_batch_read(self._h, slot, keys.ctypes.data_as(C.c_void_p),
+                                         mask.ctypes.data_as(C.c_void_p), ptrs, None, _stream(stream)),
+                "sgb_batch_read")
+        return keys, mask, fields
 
     def info(self):
         ng, nc, nb = C.c_int(), C.c_int64(), C.c_int64()

@@ -356,3 +356,18 @@ def test_batch_continuous_add_remove(sgb):
         got = gb.deviceToHost()[1]
         for a, b in zip(ref, got):
             assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("edge", [8, 4])
+def test_existing_offsets_and_counts(sgb, edge):
+    rng = np.random.default_rng(17)
+    g, o, pts = _sparse_grid(sgb, rng, (64, 56, 72), edge, 30000, ptypes=(O.T_F32,))
+    g.tagBoundaries(O.NN_STAR)
+    o.tag_boundaries(O.NN_STAR)
+    _, _, m = o.export()
+    n = g.nchunks
+    per = (m[: n * g.bs] & 1).reshape(n, g.bs).sum(1)
+    exp = np.concatenate([[0], np.cumsum(per)])
+    assert np.array_equal(g.existing_offsets().cpu().numpy(), exp)
+    assert g.countExistingElements() == int(exp[-1]) == len(pts)
+    assert g.countBoundaryElements() == int(((m & 3) == 3).sum())
