@@ -152,6 +152,7 @@ static int batch_launch(sgb_batch* b, int64_t t, cudaStream_t s) {
     L.gid = b->gid.as<int32_t>();
     L.grids = b->grids.as<GridInfo>();
     L.n = b->n;
+    L.arr_chunks = b->n;
     L.geo.edge = b->edge;
     L.geo.bs = b->edge * b->edge * b->edge;
     L.t = t;

@@ -232,6 +232,7 @@ int launch_stencil_impl(sgb_grid* g, int kind, const int* src, const int* dst, c
     L.grids = nullptr;
     L.g0 = grid_info_of(prm);
     L.n = g->n;
+    L.arr_chunks = g->n + 1;
     L.geo = g->geo;
     L.prm = prm;
     L.t = 0;

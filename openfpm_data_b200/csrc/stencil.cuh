@@ -64,6 +64,7 @@ struct LaunchDesc {
     const GridInfo* grids;   // per grid entries (NULL: single grid g0)
     GridInfo g0;
     int64_t n;
+    int64_t arr_chunks;      // chunks held by the field arrays (n + background chunk for grids)
     Geometry geo;
     StencilParams prm;
     int64_t t;

@@ -20,6 +20,9 @@
 // that invariant per property, see sgb_grid::clean), so a neighbour value is
 // read as stored; the background is substituted only for neighbour chunks
 // that do not exist.  Arithmetic is that of stencil.cuh.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include <algorithm>
 #include <cstring>
 
@@ -30,7 +33,7 @@
 namespace sgb {
 
 template <int NP>
-struct alignas(16) Stage8 {
+struct alignas(128) Stage8 {
     float tile[NP][512];
     float ym[NP][64], yp[NP][64];  // [z*8 + x]: y = 7 row of the -y chunk / y = 0 row of the +y chunk
     float zm[NP][64], zp[NP][64];  // [y*8 + x]: z = 7 slice of the -z chunk / z = 0 slice of the +z chunk
@@ -41,11 +44,59 @@ struct alignas(16) Stage8 {
     int32_t par, active;
 };
 
+// The y faces of a chunk are 8 rows of 32 B, 256 B apart: one 3-D tensor
+// copy each.  A field is viewed as a tensor [chunks*8 (z)][8 (y)][8 (x)] of
+// float, box {8, 1, 8}; the x coordinate is always 0 (16-byte aligned).
+struct TmapSet {
+    CUtensorMap yface[2][2];  // [ping-pong buffer][field]
+};
+
+__device__ __forceinline__ void tma_yface(void* dst, const CUtensorMap* map, int y, int z, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+        "[%5];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(0), "r"(y), "r"(z), "r"(smem_u32(bar))
+        : "memory");
+}
+
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
+}
+
+static int encode_yface(CUtensorMap* map, const float* base, int64_t chunks) {
+    auto enc = tensor_map_encoder();
+    if (!enc) {
+        set_error("cuTensorMapEncodeTiled is not available from the driver");
+        return SGB_ECUDA;
+    }
+    const cuuint64_t dims[3] = {8, 8, (cuuint64_t)std::max<int64_t>(chunks, 1) * 8};
+    const cuuint64_t strides[2] = {8 * sizeof(float), 64 * sizeof(float)};
+    const cuuint32_t box[3] = {8, 1, 8};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(base), dims, strides, box, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        set_error("cuTensorMapEncodeTiled failed");
+        return SGB_ECUDA;
+    }
+    return SGB_OK;
+}
+
 template <int KIND, int NP>
 __global__ void __launch_bounds__(kThreads, 2)
-    k_stencil7_e8(FieldSet fs, const uint8_t* __restrict__ mask, const int32_t* __restrict__ nn,
-                  const int64_t* __restrict__ keys, const int32_t* __restrict__ gid, const GridInfo* __restrict__ grids,
-                  GridInfo g0, int64_t n, Geometry geo, StencilParams prm, int64_t t, int S, unsigned* err) {
+    k_stencil7_e8(FieldSet fs, const __grid_constant__ TmapSet tm, const uint8_t* __restrict__ mask,
+                  const int32_t* __restrict__ nn, const int64_t* __restrict__ keys, const int32_t* __restrict__ gid,
+                  const GridInfo* __restrict__ grids, GridInfo g0, int64_t n, Geometry geo, StencilParams prm,
+                  int64_t t, int S, unsigned* err) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     Stage8<NP>* stage = reinterpret_cast<Stage8<NP>*>(smem_raw);
     uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + (size_t)S * sizeof(Stage8<NP>));
@@ -128,22 +179,19 @@ __global__ void __launch_bounds__(kThreads, 2)
                 if (lane == 0) mbar_arrive_expect_tx(&full[s], NP * (2048 + 256 * faces) + 512);
                 __syncwarp();
                 const float* sp[2] = {fs.in[par][0], fs.in[par][NP - 1]};
-                for (int tk = lane; tk < NP * 19 + 1; tk += 32) {
-                    if (tk == NP * 19) {
+                // per field: own tile, two z faces (contiguous), two y faces (tensor boxes); then the mask tile
+                if (lane < NP * 5 + 1) {
+                    const int tk = lane;
+                    if (tk == NP * 5) {
                         bulk_g2s(st.mt, mask + c * 512, 512, &full[s]);
-                        continue;
-                    }
-                    const int p = tk / 19, r = tk % 19;
-                    const float* src = p == 0 ? sp[0] : sp[1];
-                    if (r == 0) bulk_g2s(st.tile[p], src + c * 512, 2048, &full[s]);
-                    else if (r == 1) { if (fzm >= 0) bulk_g2s(st.zm[p], src + (int64_t)fzm * 512 + 448, 256, &full[s]); }
-                    else if (r == 2) { if (fzp >= 0) bulk_g2s(st.zp[p], src + (int64_t)fzp * 512, 256, &full[s]); }
-                    else if (r < 11) {
-                        const int z = r - 3;
-                        if (fym >= 0) bulk_g2s(&st.ym[p][z * 8], src + (int64_t)fym * 512 + z * 64 + 56, 32, &full[s]);
                     } else {
-                        const int z = r - 11;
-                        if (fyp >= 0) bulk_g2s(&st.yp[p][z * 8], src + (int64_t)fyp * 512 + z * 64, 32, &full[s]);
+                        const int p = tk / 5, r = tk % 5;
+                        const float* src = p == 0 ? sp[0] : sp[1];
+                        if (r == 0) bulk_g2s(st.tile[p], src + c * 512, 2048, &full[s]);
+                        else if (r == 1) { if (fzm >= 0) bulk_g2s(st.zm[p], src + (int64_t)fzm * 512 + 448, 256, &full[s]); }
+                        else if (r == 2) { if (fzp >= 0) bulk_g2s(st.zp[p], src + (int64_t)fzp * 512, 256, &full[s]); }
+                        else if (r == 3) { if (fym >= 0) tma_yface(st.ym[p], &tm.yface[par][p], 7, fym * 8, &full[s]); }
+                        else { if (fyp >= 0) tma_yface(st.yp[p], &tm.yface[par][p], 0, fyp * 8, &full[s]); }
                     }
                 }
             } else if (lane == 0) {
@@ -241,18 +289,23 @@ __global__ void __launch_bounds__(kThreads, 2)
 
 int launch_e8(const LaunchDesc& L, cudaStream_t s) {
     const int S = L.stages;
+    const int np = L.kind == SGB_GS7 ? 2 : 1;
+    TmapSet tm;
+    std::memset(&tm, 0, sizeof(tm));
+    for (int b = 0; b < 2; ++b)
+        for (int p = 0; p < np; ++p) SGB_TRY(encode_yface(&tm.yface[b][p], L.fs.in[b][p], L.arr_chunks));
     if (L.kind == SGB_GS7) {
         const size_t smem = (size_t)S * sizeof(Stage8<2>) + 2 * S * 8;
         auto kern = k_stencil7_e8<SGB_GS7, 2>;
         SGB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        kern<<<L.ctas, kThreads, smem, s>>>(L.fs, L.mask, L.nn, L.keys, L.gid, L.grids, L.g0, L.n, L.geo, L.prm, L.t,
-                                            S, L.err);
+        kern<<<L.ctas, kThreads, smem, s>>>(L.fs, tm, L.mask, L.nn, L.keys, L.gid, L.grids, L.g0, L.n, L.geo, L.prm,
+                                            L.t, S, L.err);
     } else {
         const size_t smem = (size_t)S * sizeof(Stage8<1>) + 2 * S * 8;
         auto kern = k_stencil7_e8<SGB_HEAT7, 1>;
         SGB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        kern<<<L.ctas, kThreads, smem, s>>>(L.fs, L.mask, L.nn, L.keys, L.gid, L.grids, L.g0, L.n, L.geo, L.prm, L.t,
-                                            S, L.err);
+        kern<<<L.ctas, kThreads, smem, s>>>(L.fs, tm, L.mask, L.nn, L.keys, L.gid, L.grids, L.g0, L.n, L.geo, L.prm,
+                                            L.t, S, L.err);
     }
     SGB_CUDA(cudaGetLastError());
     return SGB_OK;
