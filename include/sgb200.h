@@ -171,6 +171,17 @@ int sgb_count_existing(sgb_grid* g, int64_t* existing, int64_t* padding, sgb_str
  * SparseGridGpu_kernels.cuh:1194-1225); totals below 2^32 points. */
 int sgb_existing_offsets(sgb_grid* g, int64_t* offsets_dev, sgb_stream s);
 
+/* The same offsets without allocating device memory (no counterpart in the
+ * reference).  For callers that may not allocate: applications whose device
+ * memory belongs to their own pool allocator, and loops that may not call
+ * cudaMalloc because it can synchronise the device.  The scan scratch is a
+ * fixed file-scope device array (4 KiB, kept by every GPU that loads the
+ * library until exit), so grids of more than 1,048,576 chunks are rejected
+ * with SGB_ERANGE.  The first call on a device looks up that array's device
+ * address; make that first call before any stream capture.  All calls share
+ * the array: calls that overlap on the GPU race on it. */
+int sgb_existing_offsets_noalloc(const sgb_grid* g, int64_t* offsets_dev, sgb_stream s);
+
 /* get<p>(coord) for a batch of points (SparseGridGpu_ker.cuh:409-413):
  * value if the point exists, background otherwise.  coords dev int32 [n][3],
  * out dev n elements of the property's type. */

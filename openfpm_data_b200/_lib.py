@@ -50,6 +50,7 @@ SIGNATURES = {
     "sgb_download_map": (_i32, [_vp, _vp, _vp, _vp, _vp]),
     "sgb_count_existing": (_i32, [_vp, _vp, _vp, _vp]),
     "sgb_existing_offsets": (_i32, [_vp, _vp, _vp]),
+    "sgb_existing_offsets_noalloc": (_i32, [_vp, _vp, _vp]),
     "sgb_get": (_i32, [_vp, _i64, _vp, _i32, _vp, _vp]),
     "sgb_build_balls": (_i32, [_vp, _i32, _vp, _i32, C.c_uint64, _vp, _vp]),
     "sgb_check_device_errors": (_i32, [_vp, _vp]),
