@@ -42,6 +42,9 @@ L2_BYTES = 126 * 2 ** 20
 METRIC = "stencil Gpts/s (Gray-Scott 7-point, 512^3 sparse grid)"
 UNIT = "Gpts/s"
 ALG_BYTES_PER_PT = 17
+# the library's default launch configuration of the pipelined 8^3 kernel
+DEFAULT_CTAS_PER_SM, DEFAULT_STAGES = 4, 8
+WORKLOADS = ("gs512", "heat128", "insert1024", "batched256", "served")
 
 
 def parse():
@@ -56,6 +59,10 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ctas-per-sm", type=int, default=0)
     ap.add_argument("--stages", type=int, default=0)
+    ap.add_argument("--workload", choices=list(WORKLOADS), default="gs512",
+                    help="gs512 (the headline line) or one of the other workloads")
+    ap.add_argument("--serve-seconds", type=float, default=60.0, help="served: arrival window")
+    ap.add_argument("--plain-sample", type=int, default=64, help="served: requests solved alone for the baseline")
     return ap.parse_args()
 
 
@@ -289,11 +296,296 @@ def run_ours(args, dist: Dist):
         "config": {"workload": "gray_scott_512^3_chunk8^3_40balls_seed1", "active_points_per_gpu": npts,
                    "chunks": g.nchunks, "fields": "u,v float32 + ping-pong", "parallelism": f"replicas x{dist.world}",
                    "l2": f"inputs {footprint / 2**20:.0f} MiB > L2 {L2_BYTES / 2**20:.0f} MiB, no flush",
-                   "launch": {"ctas_per_sm": args.ctas_per_sm or 2, "stages": args.stages or 6}},
+                   "launch": {"ctas_per_sm": args.ctas_per_sm or DEFAULT_CTAS_PER_SM,
+                              "stages": args.stages or DEFAULT_STAGES}},
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": args.steps,
         "clocks": clk,
     }
     return line
+
+
+# ---------------------------------------------------------------- other workloads
+def _events():
+    import torch
+    return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+def _line(metric, value, unit, dist, args, steps, t, config, **extra):
+    d = {"metric": metric, "value": value, "unit": unit, "n_gpus": dist.world, "steps": steps,
+         "warmup": args.warmup, "ms_per_step": round(t / max(steps, 1) * 1e3, 5), "higher_is_better": True,
+         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded, workloads.py)",
+         "config": config}
+    d.update(extra)
+    return d
+
+
+def run_heat128(args, dist: Dist):
+    """Heat on the 128^3 shell (103,694 points, 379 chunks).  The grid fits in
+    L2, so an L2-flushing write (256 MiB) separates the timed steps and only
+    the stencil launches are timed (events around each)."""
+    import torch
+
+    import openfpm_data_b200 as sgb
+    from openfpm_data_b200 import workloads as W
+    torch.cuda.set_device(dist.local)
+    ps = W.heat_shell()
+    keys, data, mask = W.build_block_map(ps.coords, ps.values, ps.size, 8, ps.bck)
+    npts = len(ps.coords)
+    g = sgb.SparseGridGpu(ps.size, ["f32", "f32"], edge=8, device=dist.local)
+    g.load_map(keys, data + [data[0].copy()], mask)
+    flush = torch.empty(256 * 2 ** 20 // 4, dtype=torch.float32, device="cuda")
+    for k in range(max(3, args.warmup)):
+        g.applyStencils(sgb.HEAT7, [k % 2], [1 - k % 2], [W.HEAT_DT])
+    torch.cuda.synchronize()
+    clocks = ClockSampler(dist.local)
+    dist.barrier()
+    evs = []
+    for k in range(args.steps):
+        flush.fill_(float(k))
+        e0, e1 = _events()
+        e0.record()
+        g.applyStencils(sgb.HEAT7, [k % 2], [1 - k % 2], [W.HEAT_DT])
+        e1.record()
+        evs.append((e0, e1))
+    torch.cuda.synchronize()
+    dist.barrier()
+    clk = clocks.stop()
+    g.check_device_errors()
+    t = dist.max(sum(a.elapsed_time(b) for a, b in evs) / 1e3)
+    value = dist.world * npts * args.steps / t / 1e9
+    peak, pk = _peak_hbm()
+    ach = 9 * npts / (t / args.steps) / 1e9
+    roof = {"bound": "hbm", "achieved": round(ach, 1), "peak": peak, "unit": "GB/s", "frac": round(ach / peak, 4),
+            "traffic": None, "peak_kind": pk, "alg_bytes_per_launch": 9 * npts}
+    # e2e: one solve = upload, 100 steps (one graph), download
+    pin = lambda a: torch.from_numpy(a).pin_memory().numpy()  # noqa: E731
+    hk, hu, hm = pin(keys), pin(data[0]), pin(mask)
+    out = torch.empty((len(keys) + 1) * 512, dtype=torch.float32).pin_memory()
+    e0, e1 = _events()
+    e0.record()
+    nsolve = 5
+    for _ in range(nsolve):
+        g.load_map(hk, [hu, None], hm)
+        fin = g.run_steps(sgb.HEAT7, [0], [1], [W.HEAT_DT], 100, use_graph=True)
+        out.copy_(g.private_get_data_array(1 if fin else 0), non_blocking=True)
+    e1.record()
+    torch.cuda.synchronize()
+    te = dist.max(e0.elapsed_time(e1) / 1e3)
+    e2e = {"value": round(dist.world * npts * 100 * nsolve / te / 1e9, 3), "unit": "Gpts/s",
+           "h2d_bytes_per_step": int(hk.nbytes + hu.nbytes + hm.nbytes), "d2h_bytes_per_step": int(out.numel() * 4),
+           "step": "one solve: upload, 100 heat steps in one CUDA graph, download"}
+    cpu = None
+    if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
+        from oracle import oracle as O
+        O.build()
+        c = O.CpuSgrid(ps.size, 2, [0.0, 0.0])
+        c.insert(ps.coords, [ps.values[0], ps.values[0]])
+        t0 = time.perf_counter()
+        c.heat(0, 1, W.HEAT_DT, steps=100, threads=1)
+        dt = time.perf_counter() - t0
+        cpu = {"value": round(npts * 100 / dt / 1e9, 5), "unit": "Gpts/s", "cores": 1, "kind": "port",
+               "sample": f"100 heat steps on the 128^3 shell ({npts} points), 1 thread, {dt:.2f} s"}
+    return _line("stencil Gpts/s (heat 7-point, 128^3 shell)", round(value, 3), "Gpts/s", dist, args, args.steps, t,
+                 {"workload": "heat_128^3_shell_r20-32_chunk8^3_seed0", "active_points_per_gpu": npts,
+                  "chunks": g.nchunks, "l2": "256 MiB L2-flushing write between timed steps (grid fits in L2)"},
+                 roofline=roof, cpu_baseline=cpu, e2e=e2e, gpu_launches=args.steps, clocks=clk)
+
+
+def run_insert1024(args, dist: Dist):
+    """Insert / flush / tag / 27-point stress, 1024^3: one step = insert 2M
+    clustered points (30% duplicates), flush sRight_ (float32 + int32),
+    tagBoundaries NNStar, one 27-point box average (NNFull).  Inputs for
+    every step are generated beforehand and resident in HBM."""
+    import torch
+
+    import openfpm_data_b200 as sgb
+    from openfpm_data_b200 import workloads as W
+    torch.cuda.set_device(dist.local)
+    nsteps = args.steps if args.steps <= 200 else 20
+    nwarm = max(3, min(args.warmup, 5))
+    size = (1024, 1024, 1024)
+    g = sgb.SparseGridGpu(size, ["f32", "i32", "f32"], edge=8, device=dist.local)
+    coeff = [1.0 / 27.0] * 27
+    inputs = []
+    for it in range(nwarm + nsteps):
+        pts, fv, iv = W.insert_batch(it + 1000 * dist.rank)
+        inputs.append((torch.from_numpy(pts.astype(np.int32)).cuda(), torch.from_numpy(fv).cuda(),
+                       torch.from_numpy(iv).cuda()))
+    npts = inputs[0][0].shape[0]
+    phases = {"insert": 0.0, "flush": 0.0, "tag": 0.0, "box27": 0.0}
+    flush_alg = 0.0
+
+    def one(inp, timed):
+        nonlocal flush_alg
+        ev = [_events()[0] for _ in range(5)]
+        n_before = g.nchunks
+        ev[0].record()
+        g.insert(inp[0], [inp[1], inp[2], None])
+        ev[1].record()
+        g.flush(["sRight_", "sRight_"])
+        ev[2].record()
+        g.tagBoundaries(sgb.NN_STAR)
+        ev[3].record()
+        g.applyStencils(sgb.BOX27, [0], [2], coeff)
+        ev[4].record()
+        if timed:
+            torch.cuda.synchronize()
+            for k, name in enumerate(phases):
+                phases[name] += ev[k].elapsed_time(ev[k + 1]) / 1e3
+            # staged key + 2 values in, old chunks read, merged chunks written (3 fields + mask)
+            flush_alg += 16 * npts + 512 * 13 * (n_before + g.nchunks)
+
+    for it in range(nwarm):
+        one(inputs[it], False)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(dist.local)
+    dist.barrier()
+    e0, e1 = _events()
+    e0.record()
+    for it in range(nsteps):
+        one(inputs[nwarm + it], True)
+    e1.record()
+    torch.cuda.synchronize()
+    dist.barrier()
+    clk = clocks.stop()
+    g.check_device_errors()
+    t = dist.max(e0.elapsed_time(e1) / 1e3)
+    value = dist.world * npts * nsteps / t / 1e6
+    peak, pk = _peak_hbm()
+    ach = flush_alg / phases["flush"] / 1e9
+    roof = {"bound": "hbm", "kernel": "flush (sort + merge)", "achieved": round(ach, 1), "peak": peak,
+            "unit": "GB/s", "frac": round(ach / peak, 4), "traffic": None, "peak_kind": pk,
+            "alg_bytes_per_launch": round(flush_alg / nsteps)}
+    return _line("insert+flush+tag+box27 Mpts/s (1024^3, 2M points per step)", round(value, 2), "Mpts/s", dist,
+                 args, nsteps, t, {"workload": "insert_stress_1024^3_2M_64clusters_sigma24_dup30_seed2",
+                                   "points_per_step": npts, "chunks_at_end": g.nchunks,
+                                   "phase_seconds": {k: round(v, 4) for k, v in phases.items()},
+                                   "l2": "inputs > L2 (48 MiB of points per step, map > 1 GB)"},
+                 roofline=roof, cpu_baseline=None, e2e=None, gpu_launches=None, clocks=clk)
+
+
+def _batched_specs(n=256):
+    from openfpm_data_b200 import autotune as A
+    from openfpm_data_b200 import workloads as W
+    edges, radii, seeds = W.batch_grids(n)
+    return [A.Spec(int(e), np.array([[e / 2.0, e / 2.0, e / 2.0, r]], np.float32), 0, int(s))
+            for e, r, s in zip(edges, radii, seeds)]
+
+
+def run_batched256(args, dist: Dist):
+    """256 heat grids of uneven size (edges log-uniform in [32, 384], one
+    centred ball of radius 0.25-0.5 edge, seed 3), 200 steps per solve.
+    value: solves/s of the batched form (one persistent launch per step over
+    the concatenated block maps, each solve's 200 steps one CUDA graph) with
+    the autotuned launch; beside it the same solves with per-grid plain
+    launches (one sgb_run_steps per grid, no graph)."""
+    import torch
+
+    import openfpm_data_b200 as sgb
+    from openfpm_data_b200 import autotune as A
+    from openfpm_data_b200 import workloads as W
+    torch.cuda.set_device(dist.local)
+    specs = _batched_specs()
+    steps_per_solve = 200
+    tune = A.autotune(specs[::8], sgb.HEAT7, [W.HEAT_DT], steps=10, device=dist.local)
+    nsolves = max(1, min(args.steps, 20))
+    nwarm = 1
+    b, pts = A.build_batch(specs, sgb.HEAT7, [W.HEAT_DT], steps_per_solve * (nsolves + nwarm), tune.chunk_edge,
+                           dist.local)
+    b.set_launch_config(tune.ctas_per_sm, tune.stages)
+    b.step(steps_per_solve * nwarm, use_graph=True)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(dist.local)
+    dist.barrier()
+    e0, e1 = _events()
+    e0.record()
+    for _ in range(nsolves):
+        b.step(steps_per_solve, use_graph=True)
+    e1.record()
+    torch.cuda.synchronize()
+    dist.barrier()
+    clk = clocks.stop()
+    t = dist.max(e0.elapsed_time(e1) / 1e3)
+    ngr, nch, nbytes = b.info()
+    b.close()
+    batched = dist.world * len(specs) * nsolves / t
+    # per-grid plain launches, the same grids and steps (8^3 chunks, default launch)
+    grids = []
+    for sp in specs:
+        g = sgb.SparseGridGpu((sp.edge,) * 3, ["f32", "f32"], edge=8, device=dist.local)
+        g.build_balls(sp.balls, sp.init, sp.seed, [0])
+        grids.append(g)
+    for g in grids[:4]:
+        g.run_steps(sgb.HEAT7, [0], [1], [W.HEAT_DT], 4, use_graph=False)
+    torch.cuda.synchronize()
+    p0, p1 = _events()
+    p0.record()
+    for g in grids:
+        g.run_steps(sgb.HEAT7, [0], [1], [W.HEAT_DT], steps_per_solve, use_graph=False)
+    p1.record()
+    torch.cuda.synchronize()
+    tp = dist.max(p0.elapsed_time(p1) / 1e3)
+    for g in grids:
+        g.close()
+    plain = dist.world * len(specs) / tp
+    peak, pk = _peak_hbm()
+    ach = 9 * pts * steps_per_solve * nsolves / (t / dist.world) / 1e9 if dist.world == 1 else None
+    roof = {"bound": "hbm", "achieved": round(ach, 1) if ach else None, "peak": peak, "unit": "GB/s",
+            "frac": round(ach / peak, 4) if ach else None, "traffic": None, "peak_kind": pk,
+            "alg_bytes_per_launch": 9 * pts}
+    return _line("batched solves/s (256 heat grids, 200 steps each)", round(batched, 3), "solves/s", dist, args,
+                 nsolves, t, {"workload": "batched_256_heat_grids_edge32-384_logu_seed3", "active_points": pts,
+                              "chunks": nch, "resident_bytes": nbytes,
+                              "autotune": {"chunk_edge": tune.chunk_edge, "ctas_per_sm": tune.ctas_per_sm,
+                                           "stages": tune.stages, "threads_per_chunk": tune.threads_per_chunk,
+                                           "table": tune.table},
+                              "plain_solves_per_s": round(plain, 3), "batched_over_plain": round(batched / plain, 2),
+                              "l2": "resident fields >> L2"},
+                 roofline=roof, cpu_baseline=None, e2e=None, gpu_launches=steps_per_solve * nsolves, clocks=clk)
+
+
+def run_served(args, dist: Dist):
+    """Served form: Poisson arrivals at 2000 requests/s (seed 4), heat or
+    Gray-Scott 50/50, edges log-uniform in [32, 256], 1-8 balls of radius
+    0.1-0.3 edge, 50-500 steps; admitted under a 150 GB HBM budget and
+    advanced in shared batched launches.  value: completed solves/s over the
+    run; p50/p99 latency from arrival to read-back; beside it a sample of the
+    same requests solved alone with per-grid plain launches."""
+    import torch
+
+    from openfpm_data_b200 import serve as S
+    from openfpm_data_b200 import workloads as W
+    torch.cuda.set_device(dist.local)
+    reqs = W.requests(duration=args.serve_seconds, seed=4 + 1000 * dist.rank)
+    warm = W.requests(duration=0.05, seed=99)
+    srv = S.Server(budget_bytes=150e9, device=dist.local)
+    srv.run(warm, realtime=False)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(dist.local)
+    dist.barrier()
+    st = srv.run(reqs, realtime=True)
+    torch.cuda.synchronize()
+    dist.barrier()
+    clk = clocks.stop()
+    srv.close()
+    summ = st.summary()
+    sample = reqs[: args.plain_sample]
+    t0 = time.perf_counter()
+    for r in sample:
+        S.solve_alone(r, device=dist.local)
+    torch.cuda.synchronize()
+    tp = time.perf_counter() - t0
+    plain = len(sample) / tp
+    served = dist.world * summ["completed"] / st.wall
+    return _line("served solves/s (heat + Gray-Scott requests, Poisson 2000/s)", round(served, 2), "solves/s",
+                 dist, args, summ["completed"], st.wall,
+                 {"workload": f"served_poisson2000_{args.serve_seconds:g}s_edge32-256_seed4", "requests": len(reqs),
+                  "serve": summ, "plain_sample": len(sample), "plain_solves_per_s": round(plain, 3),
+                  "served_over_plain": round(served / plain, 2), "budget_bytes": 150e9},
+                 roofline=None, cpu_baseline=None,
+                 e2e={"value": round(served, 2), "unit": "solves/s", "h2d_bytes_per_step": None,
+                      "d2h_bytes_per_step": None, "step": "one request: build on device, steps, read back"},
+                 gpu_launches=None, clocks=clk)
 
 
 def run_reference(args, dist: Dist):
@@ -318,7 +610,12 @@ def main():
     args = parse()
     dist = Dist(args.gpus)
     try:
-        line = run_reference(args, dist) if args.impl == "reference" else run_ours(args, dist)
+        if args.impl == "reference":
+            line = run_reference(args, dist)
+        else:
+            runners = {"gs512": run_ours, "heat128": run_heat128, "insert1024": run_insert1024,
+                       "batched256": run_batched256, "served": run_served}
+            line = runners[args.workload](args, dist)
         if line is not None and dist.rank == 0:
             print(json.dumps(line), flush=True)
     finally:

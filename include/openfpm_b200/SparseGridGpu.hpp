@@ -1,0 +1,588 @@
+// C++ drop-in front-end for the SparseGridGpu hot path over libsgb200.
+//
+// Mirrors the reference class template
+//   SparseGridGpu<dim, aggregate<T...>, blockEdgeSize, threadBlockSize, indexT>
+// (src/SparseGridGpu/SparseGridGpu.hpp:483-493) for dim = 3 and 8^3 / 4^3
+// chunks: the host methods keep the reference's names and argument meaning,
+// the device view returned by toKernel() offers init / insert<p> /
+// flush_block_insert / get<p> to user kernels, and the conv family takes user
+// __device__ lambdas.  Fixed-function stencils (HeatStencil, Conv3x3x3) run
+// the library's kernels; conv lambdas run a header kernel instantiated in the
+// caller's translation unit.  Compile user code with nvcc (-std=c++17,
+// --extended-lambda) and link libsgb200.so.
+//
+// Errors: every failing library call throws openfpm_b200::sgb_error carrying
+// the sgb_status and the library's message (the reference prints and
+// continues, SparseGridGpu.hpp:2347-2352).
+#pragma once
+
+#if !defined(__CUDACC__)
+#error "SparseGridGpu.hpp holds device code: compile with nvcc"
+#endif
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <tuple>
+#include <type_traits>
+#include <vector>
+
+#include "../sgb200.h"
+
+namespace openfpm_b200 {
+
+// ------------------------------------------------------------------ support types
+struct sgb_error : std::runtime_error {
+    int status;
+    sgb_error(int s, const std::string& what)
+        : std::runtime_error(what + ": " + sgb_status_string(s) + " (" + sgb_last_error_string() + ")"), status(s) {}
+};
+
+inline void check(int s, const char* what) {
+    if (s != SGB_OK) throw sgb_error(s, what);
+}
+
+template <typename... T>
+struct aggregate {
+    using type = std::tuple<T...>;
+    static constexpr unsigned max_prop = sizeof...(T);
+};
+
+template <unsigned dim, typename T = long>
+struct grid_key_dx {
+    T k[dim];
+    __host__ __device__ grid_key_dx() : k{} {}
+    __host__ __device__ grid_key_dx(std::initializer_list<T> l) : k{} {
+        unsigned i = 0;
+        for (T v : l)
+            if (i < dim) k[i++] = v;
+    }
+    __host__ __device__ T get(unsigned i) const { return k[i]; }
+    __host__ __device__ void set_d(unsigned i, T v) { k[i] = v; }
+};
+
+template <unsigned dim, typename T>
+struct Box {
+    T lo[dim], hi[dim];
+    __host__ __device__ T getLow(unsigned i) const { return lo[i]; }
+    __host__ __device__ T getHigh(unsigned i) const { return hi[i]; }
+    __host__ __device__ void setLow(unsigned i, T v) { lo[i] = v; }
+    __host__ __device__ void setHigh(unsigned i, T v) { hi[i] = v; }
+};
+
+namespace gpu {
+struct ofp_context_t {};
+}  // namespace gpu
+
+enum flush_type { FLUSH_ON_HOST = 0, FLUSH_ON_DEVICE = 1 };
+enum StencilMode { STENCIL_MODE_INPLACE = 1, STENCIL_MODE_INPLACE_NO_SHARED = 3 };
+enum mask_sparse { NOT_EXIST = 0, EXIST = 1, PADDING = 2, EXIST_AND_PADDING = 3 };
+
+template <unsigned dim>
+struct NNStar {
+    static constexpr int kind = SGB_NN_STAR;
+};
+template <unsigned dim>
+struct NNFull {
+    static constexpr int kind = SGB_NN_FULL;
+};
+
+// flush reductions (src/Vector/cuda/map_vector_sparse_cuda_kernels.cuh:51-352)
+template <unsigned p> struct sRight_ { static constexpr unsigned prop = p; static constexpr int op = SGB_OP_RIGHT; };
+template <unsigned p> struct sLeft_ { static constexpr unsigned prop = p; static constexpr int op = SGB_OP_LEFT; };
+template <unsigned p> struct sadd_ { static constexpr unsigned prop = p; static constexpr int op = SGB_OP_ADD; };
+template <unsigned p> struct smax_ { static constexpr unsigned prop = p; static constexpr int op = SGB_OP_MAX; };
+template <unsigned p> struct smin_ { static constexpr unsigned prop = p; static constexpr int op = SGB_OP_MIN; };
+template <unsigned p> struct sBitwiseOr_ { static constexpr unsigned prop = p; static constexpr int op = SGB_OP_OR; };
+
+// fixed-function stencils of the reference's tests
+template <unsigned dim, unsigned p_src, unsigned p_dst>
+struct HeatStencil {
+    static constexpr int kind = SGB_HEAT7;
+    static constexpr unsigned src = p_src, dst = p_dst;
+};
+template <unsigned dim, unsigned p_src, unsigned p_dst>
+struct Conv3x3x3 {
+    static constexpr int kind = SGB_BOX27;
+    static constexpr unsigned src = p_src, dst = p_dst;
+};
+struct conv_coeff {
+    float coeff[3][3][3];
+};
+
+template <unsigned dim, typename T>
+struct cross_stencil {
+    T xm[dim];
+    T xp[dim];
+};
+
+// halo-indexed tile accessor (src/SparseGrid/cp_block.hpp:14-97): u(i, j, k)
+// for local coordinates i, j, k in [-1, edge]
+template <typename T, int E>
+struct cp_block {
+    T* ptr;
+    __device__ T& operator()(int i, int j, int k) const { return ptr[(i + 1) + (E + 2) * ((j + 1) + (E + 2) * (k + 1))]; }
+};
+
+// chunk data handle passed to conv2_b functions: block.template get<p>()[offset]
+template <int NPROP>
+struct data_block {
+    void* const* data;
+    int64_t chunk;
+    int bs;
+    template <unsigned p, typename T = float>
+    __device__ T* get() const {
+        return static_cast<T*>(data[p]) + chunk * bs;
+    }
+};
+
+namespace detail {
+template <typename T> struct sgb_type_of;
+template <> struct sgb_type_of<float> { static constexpr int value = SGB_F32; };
+template <> struct sgb_type_of<int> { static constexpr int value = SGB_I32; };
+template <> struct sgb_type_of<double> { static constexpr int value = SGB_F64; };
+template <> struct sgb_type_of<unsigned char> { static constexpr int value = SGB_U8; };
+
+template <typename Tuple> struct types_of;
+template <typename... T>
+struct types_of<std::tuple<T...>> {
+    static std::vector<int> get() { return {sgb_type_of<T>::value...}; }
+};
+
+__device__ __forceinline__ int64_t find_key(const int64_t* keys, int64_t n, int64_t key) {
+    int64_t lo = 0, hi = n;
+    while (lo < hi) {
+        const int64_t mid = (lo + hi) >> 1;
+        if (keys[mid] < key) lo = mid + 1;
+        else hi = mid;
+    }
+    return (lo < n && keys[lo] == key) ? lo : -1;
+}
+
+// per-CTA slot counter of the insert pools (vct_atomic_add in the reference)
+static __shared__ int sgb_pool_counter;
+
+// Generic conv kernel: one CTA per chunk, (E+2)^3 tiles of the NP source
+// fields in shared memory (faces always, edges and corners with an NNFull
+// table), the user function called for every active point inside the box.
+template <int E, int NP, int MODE, typename F>
+__global__ void conv_kernel(sgb_view v, int src0, int src1, int dst0, int dst1, Box<3, int> box, F f) {
+    constexpr int T = E + 2, TT = T * T * T, BS = E * E * E;
+    __shared__ float tile[NP][TT];
+    const float* src[2] = {static_cast<const float*>(v.data[src0]), static_cast<const float*>(v.data[src1])};
+    float* dst[2] = {static_cast<float*>(v.data[dst0]), static_cast<float*>(v.data[dst1])};
+    const float bck[2] = {src[0][v.n * BS], src[1][v.n * BS]};  // background chunk
+    for (int64_t chunk = blockIdx.x; chunk < v.n; chunk += gridDim.x) {
+        for (int cell = threadIdx.x; cell < TT; cell += blockDim.x) {
+            const int tx = cell % T, ty = (cell / T) % T, tz = cell / (T * T);
+            const int dx = tx == 0 ? -1 : (tx == T - 1 ? 1 : 0), dy = ty == 0 ? -1 : (ty == T - 1 ? 1 : 0),
+                      dz = tz == 0 ? -1 : (tz == T - 1 ? 1 : 0);
+            const int nz = (dx != 0) + (dy != 0) + (dz != 0);
+            int64_t sc = chunk;
+            if (nz) {
+                if (v.nn_kind == SGB_NN_FULL) sc = v.nn[chunk * 27 + (dx + 1) + 3 * (dy + 1) + 9 * (dz + 1)];
+                else if (nz == 1) sc = v.nn[chunk * 8 + (dx ? (dx < 0 ? 0 : 1) : dy ? (dy < 0 ? 2 : 3) : (dz < 0 ? 4 : 5))];
+                else sc = -1;
+            }
+            const int lx = (tx - 1 + E) % E, ly = (ty - 1 + E) % E, lz = (tz - 1 + E) % E;
+            const int64_t idx = sc * BS + lx + E * (ly + E * lz);
+            for (int p = 0; p < NP; ++p) tile[p][cell] = sc >= 0 ? src[p][idx] : bck[p];
+        }
+        __syncthreads();
+        const int64_t key = v.keys[chunk];
+        const int64_t bx = key % v.bsz[0], by = (key / v.bsz[0]) % v.bsz[1], bz = key / (v.bsz[0] * v.bsz[1]);
+        for (int pnt = threadIdx.x; pnt < BS; pnt += blockDim.x) {
+            const int i = pnt % E, j = (pnt / E) % E, k = pnt / (E * E);
+            const uint8_t m = v.mask[chunk * BS + pnt];
+            const int64_t gx = bx * E + i, gy = by * E + j, gz = bz * E + k;
+            const bool in = gx >= box.lo[0] && gx <= box.hi[0] && gy >= box.lo[1] && gy <= box.hi[1] &&
+                            gz >= box.lo[2] && gz <= box.hi[2];
+            const bool act = (m & 1) && !(m & 2) && in;
+            const int c = (i + 1) + T * ((j + 1) + T * (k + 1));
+            const int64_t g = chunk * BS + pnt;
+            if constexpr (MODE == 0) {  // conv_cross: storeBlock of the whole chunk
+                float res = tile[0][c];
+                if (act) {
+                    cross_stencil<3, float> cs;
+                    cs.xm[0] = tile[0][c - 1];
+                    cs.xp[0] = tile[0][c + 1];
+                    cs.xm[1] = tile[0][c - T];
+                    cs.xp[1] = tile[0][c + T];
+                    cs.xm[2] = tile[0][c - T * T];
+                    cs.xp[2] = tile[0][c + T * T];
+                    float u = tile[0][c];
+                    res = f(u, cs);
+                }
+                dst[0][g] = res;
+            } else if (act) {
+                cp_block<float, E> u{tile[0]}, w{tile[NP - 1]};
+                if constexpr (MODE == 1) {  // conv
+                    dst[0][g] = f(u, i, j, k);
+                } else if constexpr (MODE == 2) {  // conv2
+                    float r1 = 0, r2 = 0;
+                    f(r1, r2, u, w, i, j, k);
+                    dst[0][g] = r1;
+                    dst[1][g] = r2;
+                } else {  // conv2_b
+                    float r1 = 0, r2 = 0;
+                    data_block<8> blk{v.data, chunk, BS};
+                    f(r1, r2, u, w, blk, pnt, i, j, k);
+                    dst[0][g] = r1;
+                    dst[1][g] = r2;
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+}  // namespace detail
+
+// ------------------------------------------------------------------ device view
+// Returned by SparseGridGpu::toKernel(); passed by value to user kernels.
+template <typename AggregateT, unsigned E>
+struct SparseGridGpu_ker {
+    sgb_view v;
+    int64_t* pool_lin;
+    void* pool_val[8];
+    int32_t* pool_cnt;
+    int nslot;
+    using props = typename AggregateT::type;
+    static constexpr unsigned blockEdgeSize_ = E;
+
+    __host__ __device__ static constexpr unsigned getBlockEdgeSize() { return E; }
+
+    // grid_smb::LinId (src/Grid/Geometry/grid_smb.hpp:176-190)
+    template <typename CoordT>
+    __device__ int64_t getLinId(const grid_key_dx<3, CoordT>& c) const {
+        int64_t b = c.get(2) / E, l = c.get(2) % E;
+        b = b * v.bsz[1] + c.get(1) / E;
+        l = l * E + c.get(1) % E;
+        b = b * v.bsz[0] + c.get(0) / E;
+        l = l * E + c.get(0) % E;
+        return b * (E * E * E) + l;
+    }
+
+    // vector_sparse_gpu_ker::init (map_vector_sparse_cuda_ker.cuh:129-140)
+    __device__ void init() const {
+        if (threadIdx.x == 0 && threadIdx.y == 0 && threadIdx.z == 0) detail::sgb_pool_counter = 0;
+        __syncthreads();
+    }
+
+    // insert<p>(coord): one slot of this CTA's pool (map_vector_sparse_cuda_ker.cuh:309-318)
+    template <unsigned p, typename CoordT>
+    __device__ typename std::tuple_element<p, props>::type& insert(const grid_key_dx<3, CoordT>& coord) const {
+        using T = typename std::tuple_element<p, props>::type;
+        const int64_t blk = blockIdx.x + (int64_t)gridDim.x * (blockIdx.y + (int64_t)gridDim.y * blockIdx.z);
+        int slot = atomicAdd(&detail::sgb_pool_counter, 1);
+        const bool ok = slot < nslot;
+        slot = ok ? slot : nslot - 1;  // an overflowing pool is reported at flush
+        const int64_t idx = blk * nslot + slot;
+        pool_lin[idx] = getLinId(coord);
+        return static_cast<T*>(pool_val[p])[idx];
+    }
+
+    // flush_block_insert (map_vector_sparse_cuda_ker.cuh:424-439)
+    __device__ void flush_block_insert() const {
+        __syncthreads();
+        if (threadIdx.x == 0 && threadIdx.y == 0 && threadIdx.z == 0) {
+            const int64_t blk = blockIdx.x + (int64_t)gridDim.x * (blockIdx.y + (int64_t)gridDim.y * blockIdx.z);
+            pool_cnt[blk] = detail::sgb_pool_counter;
+        }
+    }
+
+    // get<p>(coord): value, or the background when the point does not exist
+    template <unsigned p, typename CoordT>
+    __device__ typename std::tuple_element<p, props>::type get(const grid_key_dx<3, CoordT>& coord) const {
+        using T = typename std::tuple_element<p, props>::type;
+        const int64_t lin = getLinId(coord), bs = E * E * E;
+        int64_t pos = detail::find_key(v.keys, v.n, lin / bs);
+        if (pos < 0) pos = v.n;
+        const int64_t idx = pos * bs + lin % bs;
+        return (v.mask[idx] & 1) ? static_cast<const T*>(v.data[p])[idx]
+                                 : static_cast<const T*>(v.data[p])[v.n * bs + lin % bs];
+    }
+
+    template <typename CoordT>
+    __device__ bool isPadding(const grid_key_dx<3, CoordT>& coord) const {
+        const int64_t lin = getLinId(coord), bs = E * E * E;
+        const int64_t pos = detail::find_key(v.keys, v.n, lin / bs);
+        return pos >= 0 && (v.mask[pos * bs + lin % bs] & 3) == 3;
+    }
+};
+
+// ------------------------------------------------------------------ host class
+template <unsigned dim, typename AggregateT, unsigned blockEdgeSize = 8, unsigned threadBlockSize = 512,
+          typename indexT = long>
+class SparseGridGpu {
+    static_assert(dim == 3, "this build runs 3-D sparse grids");
+    static_assert(blockEdgeSize == 8 || blockEdgeSize == 4, "chunk edge 8 or 4");
+    using props = typename AggregateT::type;
+    static constexpr unsigned nprop = std::tuple_size<props>::value;
+    static constexpr unsigned bs = blockEdgeSize * blockEdgeSize * blockEdgeSize;
+
+    sgb_grid* g_ = nullptr;
+    size_t size_[3];
+    int nn_kind_ = SGB_NN_STAR;  // setNNType
+    // device insert pools
+    int64_t npools_ = 0, nslot_ = 0;
+    int64_t* pool_lin_ = nullptr;
+    void* pool_val_[8] = {};
+    int32_t* pool_cnt_ = nullptr;
+    // host copies filled by deviceToHost
+    std::vector<int64_t> h_keys_;
+    std::vector<std::vector<unsigned char>> h_data_;
+    std::vector<uint8_t> h_mask_;
+
+    void free_pools() {
+        if (pool_lin_) cudaFree(pool_lin_);
+        for (auto& p : pool_val_)
+            if (p) cudaFree(p), p = nullptr;
+        if (pool_cnt_) cudaFree(pool_cnt_);
+        pool_lin_ = nullptr;
+        pool_cnt_ = nullptr;
+        npools_ = nslot_ = 0;
+    }
+
+    template <typename... ops>
+    static std::vector<int> op_list() {
+        std::vector<int> o(nprop, SGB_OP_NONE);
+        int dummy[] = {0, (o[ops::prop] = ops::op, 0)...};
+        (void)dummy;
+        return o;
+    }
+
+   public:
+    static constexpr unsigned dims = dim;
+    static constexpr unsigned blockEdgeSize_ = blockEdgeSize;
+    using device_grid_type = SparseGridGpu_ker<AggregateT, blockEdgeSize>;
+
+    // SparseGridGpu(const size_t (&res)[dim], unsigned stencilSupportRadius = 1) (SparseGridGpu.hpp:1694-1698)
+    explicit SparseGridGpu(const size_t (&res)[dim], unsigned stencilSupportRadius = 1, int device = 0) {
+        if (stencilSupportRadius != 1) throw sgb_error(SGB_ENOTSUP, "stencilSupportRadius");
+        int64_t sz[3];
+        for (unsigned d = 0; d < 3; ++d) size_[d] = res[d], sz[d] = (int64_t)res[d];
+        auto types = detail::types_of<props>::get();
+        check(sgb_create(&g_, 3, blockEdgeSize, sz, (int)nprop, types.data(), device), "sgb_create");
+    }
+    SparseGridGpu(const SparseGridGpu&) = delete;
+    SparseGridGpu& operator=(const SparseGridGpu&) = delete;
+    ~SparseGridGpu() {
+        free_pools();
+        if (g_) sgb_destroy(g_);
+    }
+
+    sgb_grid* handle() const { return g_; }
+    static constexpr unsigned getBlockEdgeSize() { return blockEdgeSize; }
+    constexpr unsigned getBlockSize() const { return bs; }
+
+    template <unsigned p>
+    void setBackgroundValue(typename std::tuple_element<p, props>::type v) {
+        check(sgb_set_background(g_, p, &v), "setBackgroundValue");
+    }
+
+    // setGPUInsertBuffer(nBlock, nSlot) (SparseGridGpu.hpp:2270-2277)
+    void setGPUInsertBuffer(int64_t nBlock, int64_t nSlot) {
+        free_pools();
+        npools_ = nBlock;
+        nslot_ = nSlot;
+        const size_t n = (size_t)nBlock * nSlot;
+        if (cudaMalloc(&pool_lin_, n * 8) != cudaSuccess || cudaMalloc(&pool_cnt_, nBlock * 4) != cudaSuccess)
+            throw sgb_error(SGB_ENOMEM, "setGPUInsertBuffer");
+        auto types = detail::types_of<props>::get();
+        for (unsigned p = 0; p < nprop; ++p) {
+            const size_t es = types[p] == SGB_F64 ? 8 : (types[p] == SGB_U8 ? 1 : 4);
+            if (cudaMalloc(&pool_val_[p], n * es) != cudaSuccess) throw sgb_error(SGB_ENOMEM, "setGPUInsertBuffer");
+        }
+        cudaMemset(pool_cnt_, 0, nBlock * 4);
+    }
+    void setGPUInsertBuffer(dim3 nBlock, dim3 nSlot) {
+        setGPUInsertBuffer((int64_t)nBlock.x * nBlock.y * nBlock.z, (int64_t)nSlot.x * nSlot.y * nSlot.z);
+    }
+
+    device_grid_type toKernel() {
+        device_grid_type k{};
+        check(sgb_get_view(g_, nn_kind_, &k.v, nullptr), "toKernel");
+        k.pool_lin = pool_lin_;
+        for (int p = 0; p < 8; ++p) k.pool_val[p] = pool_val_[p];
+        k.pool_cnt = pool_cnt_;
+        k.nslot = (int)nslot_;
+        return k;
+    }
+
+    // flush<v_reduce...>(ctx, opt) (SparseGridGpu.hpp:772-779)
+    template <typename... v_reduce>
+    void flush(gpu::ofp_context_t&, flush_type = FLUSH_ON_DEVICE) {
+        if (npools_) {
+            check(sgb_insert_pools(g_, npools_, nslot_, pool_cnt_, pool_lin_, pool_val_, nullptr), "flush (pools)");
+            cudaMemset(pool_cnt_, 0, npools_ * 4);
+        }
+        auto ops = op_list<v_reduce...>();
+        check(sgb_flush(g_, ops.data(), nullptr), "flush");
+    }
+
+    template <typename NN = NNStar<dim>>
+    void findNeighbours() {
+        check(sgb_find_neighbours(g_, NN::kind, nullptr), "findNeighbours");
+    }
+    template <typename NN>
+    void setNNType() {
+        nn_kind_ = NN::kind;
+    }
+    template <typename NN = NNStar<dim>>
+    void tagBoundaries(gpu::ofp_context_t&) {
+        check(sgb_tag_boundaries(g_, NN::kind, nullptr), "tagBoundaries");
+        cudaDeviceSynchronize();  // as the reference (SparseGridGpu.hpp:2393)
+    }
+
+    Box<dim, int> getBox() const {
+        Box<dim, int> b;
+        for (unsigned d = 0; d < dim; ++d) b.lo[d] = 0, b.hi[d] = (int)size_[d];
+        return b;
+    }
+
+    // applyStencils<S>(box, mode, args...) for the fixed-function stencils
+    template <typename S>
+    void applyStencils(const Box<dim, int>& box, StencilMode, float dt) {
+        static_assert(S::kind == SGB_HEAT7, "HeatStencil takes dt");
+        run_fixed(S::kind, S::src, S::dst, &dt, 1, box);
+    }
+    template <typename S>
+    void applyStencils(const Box<dim, int>& box, StencilMode, const conv_coeff& cc) {
+        static_assert(S::kind == SGB_BOX27, "Conv3x3x3 takes conv_coeff");
+        float c[27];
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j)
+                for (int k = 0; k < 3; ++k) c[i * 9 + j * 3 + k] = cc.coeff[i][j][k];
+        run_fixed(S::kind, S::src, S::dst, c, 27, box);
+    }
+
+    // conv family with user __device__ functions (SparseGridGpu.hpp:2568-2683)
+    template <unsigned p_src, unsigned p_dst, unsigned stencil_size, typename F>
+    void conv_cross(grid_key_dx<3> start, grid_key_dx<3> stop, F f) {
+        launch_conv<1, 0>(p_src, p_src, p_dst, p_dst, start, stop, f);
+    }
+    template <unsigned p_src, unsigned p_dst, unsigned stencil_size, typename F>
+    void conv(grid_key_dx<3> start, grid_key_dx<3> stop, F f) {
+        launch_conv<1, 1>(p_src, p_src, p_dst, p_dst, start, stop, f);
+    }
+    template <unsigned s1, unsigned s2, unsigned d1, unsigned d2, unsigned stencil_size, typename F>
+    void conv2(grid_key_dx<3> start, grid_key_dx<3> stop, F f) {
+        launch_conv<2, 2>(s1, s2, d1, d2, start, stop, f);
+    }
+    template <unsigned s1, unsigned s2, unsigned d1, unsigned d2, unsigned stencil_size, typename F>
+    void conv2_b(grid_key_dx<3> start, grid_key_dx<3> stop, F f) {
+        launch_conv<2, 3>(s1, s2, d1, d2, start, stop, f);
+    }
+
+    // deviceToHost<p...>(): the block map and listed properties to host copies
+    template <unsigned... prp>
+    void deviceToHost() {
+        int64_t n;
+        sgb_nchunks(g_, &n);
+        h_keys_.resize(n);
+        h_mask_.resize((n + 1) * bs);
+        auto types = detail::types_of<props>::get();
+        h_data_.assign(nprop, {});
+        std::vector<void*> ptrs(nprop, nullptr);
+        for (unsigned p = 0; p < nprop; ++p) {
+            const size_t es = types[p] == SGB_F64 ? 8 : (types[p] == SGB_U8 ? 1 : 4);
+            h_data_[p].resize((n + 1) * bs * es);
+            ptrs[p] = h_data_[p].data();
+        }
+        check(sgb_download_map(g_, h_keys_.data(), ptrs.data(), h_mask_.data(), nullptr), "deviceToHost");
+    }
+
+    // host get<p>(coord) after deviceToHost (BlockMapGpu.hpp:108-126)
+    template <unsigned p, typename CoordT>
+    typename std::tuple_element<p, props>::type get(const grid_key_dx<dim, CoordT>& c) const {
+        using T = typename std::tuple_element<p, props>::type;
+        int64_t bsz[3];
+        for (int d = 0; d < 3; ++d) bsz[d] = ((int64_t)size_[d] + blockEdgeSize - 1) / blockEdgeSize;
+        const int64_t b = ((c.get(2) / blockEdgeSize) * bsz[1] + c.get(1) / blockEdgeSize) * bsz[0] + c.get(0) / blockEdgeSize;
+        const int64_t l = ((c.get(2) % blockEdgeSize) * blockEdgeSize + c.get(1) % blockEdgeSize) * blockEdgeSize +
+                          c.get(0) % blockEdgeSize;
+        const int64_t n = (int64_t)h_keys_.size();
+        int64_t lo = 0, hi = n;
+        while (lo < hi) {
+            int64_t mid = (lo + hi) / 2;
+            if (h_keys_[mid] < b) lo = mid + 1;
+            else hi = mid;
+        }
+        const int64_t pos = (lo < n && h_keys_[lo] == b) ? lo : n;
+        const T* d = reinterpret_cast<const T*>(h_data_[p].data());
+        return (h_mask_[pos * bs + l] & 1) ? d[pos * bs + l] : d[n * bs + l];
+    }
+    template <typename CoordT>
+    unsigned char getFlag(const grid_key_dx<dim, CoordT>& c) const {
+        int64_t bsz[3];
+        for (int d = 0; d < 3; ++d) bsz[d] = ((int64_t)size_[d] + blockEdgeSize - 1) / blockEdgeSize;
+        const int64_t b = ((c.get(2) / blockEdgeSize) * bsz[1] + c.get(1) / blockEdgeSize) * bsz[0] + c.get(0) / blockEdgeSize;
+        const int64_t l = ((c.get(2) % blockEdgeSize) * blockEdgeSize + c.get(1) % blockEdgeSize) * blockEdgeSize +
+                          c.get(0) % blockEdgeSize;
+        for (size_t i = 0; i < h_keys_.size(); ++i)
+            if (h_keys_[i] == b) return h_mask_[i * bs + l];
+        return 0;
+    }
+
+    size_t countExistingElements() const {
+        int64_t e = 0;
+        check(sgb_count_existing(g_, &e, nullptr, nullptr), "countExistingElements");
+        return (size_t)e;
+    }
+    size_t countBoundaryElements() const {
+        int64_t p = 0;
+        check(sgb_count_existing(g_, nullptr, &p, nullptr), "countBoundaryElements");
+        return (size_t)p;
+    }
+    size_t size() const { return countExistingElements(); }
+
+    // device buffers (private_get_index_array / private_get_data_array)
+    const int64_t* private_get_index_array() const {
+        const int64_t* p = nullptr;
+        sgb_index_buffer(g_, &p);
+        return p;
+    }
+    template <unsigned p>
+    void* private_get_data_array() const {
+        void* d = nullptr;
+        sgb_data_buffer(g_, p, &d);
+        return d;
+    }
+    int64_t nchunks() const {
+        int64_t n = 0;
+        sgb_nchunks(g_, &n);
+        return n;
+    }
+
+   private:
+    void run_fixed(int kind, unsigned s, unsigned d, const float* prm, int nprm, const Box<dim, int>& box) {
+        int src[2] = {(int)s, 0}, dst[2] = {(int)d, 0};
+        int64_t b[6];
+        for (unsigned i = 0; i < 3; ++i) b[i] = box.lo[i], b[3 + i] = box.hi[i];
+        check(sgb_apply_stencil(g_, kind, src, dst, prm, nprm, b, nullptr), "applyStencils");
+    }
+
+    template <int NP, int MODE, typename F>
+    void launch_conv(unsigned s1, unsigned s2, unsigned d1, unsigned d2, grid_key_dx<3> start, grid_key_dx<3> stop,
+                     F f) {
+        sgb_view v;
+        check(sgb_get_view(g_, nn_kind_, &v, nullptr), "conv");
+        if (v.n == 0) return;
+        Box<3, int> box;
+        for (int i = 0; i < 3; ++i) box.lo[i] = (int)start.get(i), box.hi[i] = (int)stop.get(i);
+        const unsigned blocks = (unsigned)(v.n < 148 * 8 ? v.n : 148 * 8);
+        detail::conv_kernel<blockEdgeSize, NP, MODE><<<blocks, 256>>>(v, (int)s1, (int)s2, (int)d1, (int)d2, box, f);
+        check(cudaGetLastError() == cudaSuccess ? SGB_OK : SGB_ECUDA, "conv launch");
+        if (MODE == 0) {
+            // storeBlock semantics put source values into the destination's
+            // non-existing points: have the library restore its backgrounds
+            void* d = nullptr;
+            check(sgb_data_buffer(g_, (int)d1, &d), "conv");
+        }
+    }
+};
+
+}  // namespace openfpm_b200

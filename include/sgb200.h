@@ -106,6 +106,33 @@ int sgb_insert(sgb_grid* g, int64_t n, const int32_t* coords_dev, const void* co
  * (src/SparseGridGpu/BlockMapGpu.hpp:137-150). */
 int sgb_insert_lin(sgb_grid* g, int64_t n, const int64_t* lin_dev, const void* const* values_dev, sgb_stream s);
 
+/* Stage the contents of per-CTA insert pools written by a user kernel
+ * (setGPUInsertBuffer(nBlock, nSlot) + insert<p> + flush_block_insert,
+ * src/Vector/map_vector_sparse.hpp:1883-1890,
+ * src/Vector/cuda/map_vector_sparse_cuda_ker.cuh:309-318, 424-439; compacted
+ * pool after pool like make_continuos, map_vector_sparse.hpp:880-946).
+ * counts_dev int32[npools]; lin_dev int64[npools*nslot] linearised point
+ * ids; values_dev[p] [npools*nslot] per property (NULL: background).  A
+ * count above nslot (a pool that overflowed) makes the next sgb_flush fail
+ * with SGB_ERANGE and drop the staged points. */
+int sgb_insert_pools(sgb_grid* g, int64_t npools, int64_t nslot, const int32_t* counts_dev, const int64_t* lin_dev,
+                     const void* const* values_dev, sgb_stream s);
+
+/* Device view of a grid for user kernels (SparseGridGpu::toKernelNN,
+ * SparseGridGpu.hpp:1749-1789): block map pointers and the neighbour table
+ * of nn_kind (int32, -1 absent), valid until the next flush or map upload.
+ * Points whose mask byte is 0 hold the background value. */
+typedef struct {
+    int64_t n;
+    int edge, bs, nprop, nn_kind;
+    int64_t size[3], bsz[3];
+    const int64_t* keys;
+    void* data[8];
+    const uint8_t* mask;
+    const int32_t* nn;
+} sgb_view;
+int sgb_get_view(sgb_grid* g, int nn_kind, sgb_view* out, sgb_stream s);
+
 /* flush<v_reduce...>(ctx, FLUSH_ON_DEVICE) (SparseGridGpu.hpp:772-779,
  * BlockMapGpu.hpp:289-299, src/Vector/map_vector_sparse.hpp:1784-1795).
  * ops[nprop]: one sgb_op per property.  Duplicates of one point are reduced
@@ -206,8 +233,9 @@ int sgb_check_device_errors(sgb_grid* g, sgb_stream s);
 /* Bytes of device memory held by the grid. */
 int sgb_device_bytes(const sgb_grid* g, int64_t* bytes);
 
-/* Stencil launch configuration: CTAs per SM (1..4) and staging depth
- * (3..8 chunks in flight per CTA); 0 keeps the current value. */
+/* Stencil launch configuration: CTAs per SM (1..8) and staging depth
+ * (3..16 chunks in flight per CTA; the 8^3 kernel uses at least 6 and at
+ * most what fits in one CTA's shared memory); 0 keeps the current value. */
 int sgb_set_launch_config(sgb_grid* g, int ctas_per_sm, int stages);
 
 /* ---------------------------------------------------------------- batches

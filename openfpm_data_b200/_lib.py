@@ -35,6 +35,8 @@ SIGNATURES = {
     "sgb_set_background": (_i32, [_vp, _i32, _vp]),
     "sgb_insert": (_i32, [_vp, _i64, _vp, _vp, _vp]),
     "sgb_insert_lin": (_i32, [_vp, _i64, _vp, _vp, _vp]),
+    "sgb_insert_pools": (_i32, [_vp, _i64, _i64, _vp, _vp, _vp, _vp]),
+    "sgb_get_view": (_i32, [_vp, _i32, _vp, _vp]),
     "sgb_flush": (_i32, [_vp, _vp, _vp]),
     "sgb_find_neighbours": (_i32, [_vp, _i32, _vp]),
     "sgb_neighbour_table": (_i32, [_vp, _i32, _vp, _vp]),

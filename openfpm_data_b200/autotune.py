@@ -1,7 +1,7 @@
 """Launch autotuner for the batched stencil step.
 
-Candidates: chunk edge 8 (pipelined kernel: 256 consumer threads per
-512-point chunk, 1-4 CTAs per SM, 4-8 staging slots) and chunk edge 4
+Candidates: chunk edge 8 (pipelined kernel: one 32-thread consumer warp
+per 512-point chunk, 2-4 CTAs per SM, 6-12 staging slots) and chunk edge 4
 (one-chunk-per-CTA tile kernel: 256 threads per 64-point chunk).  Each
 candidate runs a few timed batch steps (CUDA events) on a sample of the
 grids, rebuilt with its chunk edge; the fastest per active point wins.
@@ -71,7 +71,7 @@ def _time_steps(b: Batch, steps: int) -> float:
 
 
 def autotune(specs: Sequence[Spec], kind: int, params, steps: int = 10, device: int = 0,
-             ctas=(1, 2, 3, 4), stages=(4, 6, 8), edges=(8, 4)) -> TuneResult:
+             ctas=(2, 3, 4), stages=(6, 8, 12), edges=(8, 4)) -> TuneResult:
     table = []
     best = None
     for ce in edges:
@@ -82,11 +82,12 @@ def autotune(specs: Sequence[Spec], kind: int, params, steps: int = 10, device: 
                 b.set_launch_config(c, s)
             t = _time_steps(b, steps)
             nsps = t / steps / max(pts, 1) * 1e9
-            row = {"chunk_edge": ce, "ctas_per_sm": c, "stages": s, "threads_per_chunk": 256,
+            # 8^3: one consumer warp per chunk in the pipelined kernel; 4^3: one 256-thread CTA per chunk
+            row = {"chunk_edge": ce, "ctas_per_sm": c, "stages": s, "threads_per_chunk": 32 if ce == 8 else 256,
                    "ns_per_point_step": round(nsps, 5)}
             table.append(row)
             if best is None or nsps < best["ns_per_point_step"]:
                 best = row
         b.close()
-    return TuneResult(best["chunk_edge"], best["ctas_per_sm"] or 2, best["stages"] or 6, best["threads_per_chunk"],
+    return TuneResult(best["chunk_edge"], best["ctas_per_sm"] or 4, best["stages"] or 8, best["threads_per_chunk"],
                       best["ns_per_point_step"], table)

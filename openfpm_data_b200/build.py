@@ -50,6 +50,34 @@ def build(force: bool = False, verbose: bool = False) -> str:
     return LIB
 
 
+DROPIN_SRC = os.path.join(ROOT, "tests", "cpp", "test_dropin.cu")
+DROPIN_BIN = os.path.join(ROOT, "tests", "cpp", "_build", "test_dropin")
+
+
+def build_dropin_test(force: bool = False, verbose: bool = False) -> str:
+    """Compile the C++ drop-in test (user code against include/openfpm_b200/SparseGridGpu.hpp)."""
+    lib = build(verbose=verbose)
+    deps = [DROPIN_SRC, lib] + glob.glob(os.path.join(ROOT, "include", "**", "*.h*"), recursive=True)
+    if not force and os.path.exists(DROPIN_BIN) and all(os.path.getmtime(d) <= os.path.getmtime(DROPIN_BIN)
+                                                         for d in deps):
+        return DROPIN_BIN
+    os.makedirs(os.path.dirname(DROPIN_BIN), exist_ok=True)
+    nvcc = os.environ.get("NVCC", "nvcc")
+    tmp = DROPIN_BIN + ".tmp"
+    cmd = [nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-O2", "-lineinfo", "-std=c++17",
+           "--extended-lambda", "-ftz=true", "-fmad=true", "-I", os.path.join(ROOT, "include"),
+           "-o", tmp, DROPIN_SRC, "-L", HERE, "-lsgb200",
+           # the binary sits in tests/cpp/_build; the library three levels up in openfpm_data_b200/
+           "-Xlinker", "-rpath,$ORIGIN/../../../openfpm_data_b200"]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+    os.replace(tmp, DROPIN_BIN)
+    return DROPIN_BIN
+
+
 if __name__ == "__main__":
     build(force="--force" in sys.argv, verbose=True)
     print(LIB)
+    if "--dropin" in sys.argv:
+        print(build_dropin_test(force="--force" in sys.argv, verbose=True))

@@ -434,10 +434,13 @@ extern "C" int sgb_flush(sgb_grid* g, const int* ops, sgb_stream stream) {
     SGB_TRY(g->hscratch.ensure(64));
     SGB_CUDA(cudaMemcpyAsync(g->hscratch.p, g->err.p, 4, cudaMemcpyDeviceToHost, s));
     SGB_CUDA(cudaStreamSynchronize(s));
-    if (*(unsigned*)g->hscratch.p & kErrOutOfDomain) {
+    const unsigned e = *(unsigned*)g->hscratch.p;
+    if (e & (kErrOutOfDomain | kErrPoolOverflow)) {
         SGB_CUDA(cudaMemsetAsync(g->err.p, 0, 4, s));
         g->npend = 0;
-        set_error("an inserted point lies outside the grid domain; the staged inserts were dropped");
+        set_error((e & kErrOutOfDomain)
+                      ? "an inserted point lies outside the grid domain; the staged inserts were dropped"
+                      : "an insert pool counted more points than its slots; the staged inserts were dropped");
         return SGB_ERANGE;
     }
     const int64_t maxlin = g->geo.bsz[0] * g->geo.bsz[1] * g->geo.bsz[2] * g->geo.bs;

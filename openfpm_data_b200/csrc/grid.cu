@@ -255,6 +255,53 @@ __global__ void k_get(const int32_t* coords, int64_t n, Geometry geo, const int6
     out[i] = (mask[idx] & 1) ? data[idx] : data[(size_t)nchunks * geo.bs + l];
 }
 
+// Pool counts clamped to the pool capacity (an overflowing pool raises the
+// out-of-domain error word: its extra inserts had nowhere to go).
+__global__ void k_clamp_counts(const int32_t* counts, int64_t npools, int32_t nslot, uint32_t* out, unsigned* err) {
+    int64_t b = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (b >= npools) return;
+    int32_t c = counts[b];
+    if (c < 0 || c > nslot) {
+        atomicOr(err, kErrPoolOverflow);
+        c = c < 0 ? 0 : nslot;
+    }
+    out[b] = (uint32_t)c;
+}
+
+struct PoolCopy {
+    const unsigned char* src[kMaxProps];
+    unsigned char* dst[kMaxProps];
+    int es[kMaxProps];
+    uint64_t bck[kMaxProps];
+    int nprop;
+};
+
+// One CTA per pool: its first counts[b] slots, in slot order, after the
+// pools before it.
+__global__ void k_pool_copy(const uint32_t* counts, const uint32_t* off, int64_t nslot, const int64_t* lin,
+                            int64_t maxlin, int64_t* out_lin, PoolCopy pc, unsigned* err) {
+    const int64_t b = blockIdx.x;
+    const uint32_t c = counts[b], o = off[b];
+    for (uint32_t k = threadIdx.x; k < c; k += blockDim.x) {
+        const int64_t src = b * nslot + k, dst = (int64_t)o + k;
+        int64_t v = lin[src];
+        if (v < 0 || v >= maxlin) {
+            atomicOr(err, kErrOutOfDomain);
+            v = -1;
+        }
+        out_lin[dst] = v;
+        for (int p = 0; p < pc.nprop; ++p) {
+            const int es = pc.es[p];
+            unsigned char* d = pc.dst[p] + dst * es;
+            if (pc.src[p]) {
+                for (int q = 0; q < es; ++q) d[q] = pc.src[p][src * es + q];
+            } else {
+                for (int q = 0; q < es; ++q) d[q] = (unsigned char)(pc.bck[p] >> (8 * q));
+            }
+        }
+    }
+}
+
 // EXIST points per chunk: one warp per chunk, one ballot per 32 mask bytes
 // (calc_exist_points, SparseGridGpu_kernels.cuh:1194-1225).
 __global__ void k_chunk_counts(const uint8_t* mask, int64_t n, int bs, uint32_t* counts) {
@@ -417,6 +464,67 @@ int sgb_insert_lin(sgb_grid* g, int64_t n, const int64_t* lin, const void* const
     return SGB_OK;
 }
 
+int sgb_insert_pools(sgb_grid* g, int64_t npools, int64_t nslot, const int32_t* counts, const int64_t* lin,
+                     const void* const* values, sgb_stream stream) {
+    if (!g || npools < 0 || nslot < 0 || (npools > 0 && (!counts || !lin))) return SGB_EINVAL;
+    if (npools == 0) return SGB_OK;
+    cudaStream_t s = (cudaStream_t)stream;
+    DevBuf& cnt = g->scratch[9];
+    DevBuf& off = g->scratch[10];
+    SGB_TRY(cnt.ensure((size_t)npools * 4 + 16));
+    SGB_TRY(off.ensure((size_t)npools * 4 + 16));
+    k_clamp_counts<<<(unsigned)((npools + 255) / 256), 256, 0, s>>>(counts, npools, (int32_t)nslot, cnt.as<uint32_t>(),
+                                                                     g->err.as<unsigned>());
+    SGB_CUDA(cudaGetLastError());
+    uint32_t* total = off.as<uint32_t>() + npools;
+    SGB_TRY(scan_exclusive_u32(cnt.as<uint32_t>(), off.as<uint32_t>(), npools, total, &g->scratch[6], s));
+    SGB_TRY(g->hscratch.ensure(64));
+    SGB_CUDA(cudaMemcpyAsync(g->hscratch.p, total, 4, cudaMemcpyDeviceToHost, s));
+    SGB_CUDA(cudaStreamSynchronize(s));
+    const int64_t add = *(uint32_t*)g->hscratch.p;
+    if (add == 0) return SGB_OK;
+    SGB_TRY(g->pend_lin.reserve((size_t)(g->npend + add) * 8));
+    PoolCopy pc{};
+    pc.nprop = g->nprop;
+    for (int p = 0; p < g->nprop; ++p) {
+        const int es = elem_size(g->ptype[p]);
+        SGB_TRY(g->pend_val[p].reserve((size_t)(g->npend + add) * es));
+        pc.src[p] = values ? (const unsigned char*)values[p] : nullptr;
+        if (pc.src[p]) g->pend_has[p] = true;
+        pc.dst[p] = g->pend_val[p].as<unsigned char>() + (size_t)g->npend * es;
+        pc.es[p] = es;
+        pc.bck[p] = bck_pattern(g, p);
+    }
+    const int64_t maxlin = g->geo.bsz[0] * g->geo.bsz[1] * g->geo.bsz[2] * g->geo.bs;
+    k_pool_copy<<<(unsigned)npools, 128, 0, s>>>(cnt.as<uint32_t>(), off.as<uint32_t>(), nslot, lin, maxlin,
+                                                 g->pend_lin.as<int64_t>() + g->npend, pc, g->err.as<unsigned>());
+    SGB_CUDA(cudaGetLastError());
+    g->npend += add;
+    return SGB_OK;
+}
+
+int sgb_get_view(sgb_grid* g, int nn_kind, sgb_view* out, sgb_stream stream) {
+    if (!g || !out || (nn_kind != SGB_NN_STAR && nn_kind != SGB_NN_FULL)) return SGB_EINVAL;
+    cudaStream_t s = (cudaStream_t)stream;
+    SGB_TRY(ensure_neighbours(g, nn_kind, s));
+    for (int p = 0; p < g->nprop; ++p) SGB_TRY(ensure_clean(g, p, s));
+    std::memset(out, 0, sizeof(*out));
+    out->n = g->n;
+    out->edge = g->geo.edge;
+    out->bs = g->geo.bs;
+    out->nprop = g->nprop;
+    out->nn_kind = nn_kind;
+    for (int d = 0; d < 3; ++d) {
+        out->size[d] = g->geo.size[d];
+        out->bsz[d] = g->geo.bsz[d];
+    }
+    out->keys = g->keys.as<int64_t>();
+    for (int p = 0; p < g->nprop; ++p) out->data[p] = g->data[p].p;
+    out->mask = g->mask.as<uint8_t>();
+    out->nn = g->nn[nn_kind].as<int32_t>();
+    return SGB_OK;
+}
+
 int sgb_nchunks(const sgb_grid* g, int64_t* n) {
     if (!g || !n) return SGB_EINVAL;
     *n = g->n;
@@ -564,6 +672,10 @@ int sgb_check_device_errors(sgb_grid* g, sgb_stream stream) {
         set_error("an inserted point lies outside the grid domain");
         return SGB_ERANGE;
     }
+    if (e & kErrPoolOverflow) {
+        set_error("an insert pool counted more points than its slots (the excess was dropped)");
+        return SGB_ERANGE;
+    }
     return SGB_OK;
 }
 
@@ -578,7 +690,7 @@ int sgb_device_bytes(const sgb_grid* g, int64_t* bytes) {
 }
 
 int sgb_set_launch_config(sgb_grid* g, int ctas_per_sm, int stages) {
-    if (!g || ctas_per_sm < 0 || ctas_per_sm > 4 || stages < 0 || (stages > 0 && (stages < 3 || stages > 8)))
+    if (!g || ctas_per_sm < 0 || ctas_per_sm > 8 || stages < 0 || (stages > 0 && (stages < 3 || stages > 16)))
         return SGB_EINVAL;
     if (ctas_per_sm) g->ctas_per_sm = ctas_per_sm;
     if (stages) g->stages = stages;

@@ -17,6 +17,7 @@ constexpr int kMaxProps = 8;
 enum : unsigned {
     kErrWaitTimeout = 1u,   // a bounded mbarrier wait gave up
     kErrOutOfDomain = 2u,   // an inserted point lies outside the domain
+    kErrPoolOverflow = 4u,  // an insert pool reported more points than it has slots
 };
 
 inline int elem_size(int t) { return t == SGB_F64 ? 8 : (t == SGB_U8 ? 1 : 4); }
@@ -64,7 +65,8 @@ struct Geometry {
 // Launch parameters of the fixed-function stencils.
 struct StencilParams {
     float dt, Du, Dv, F, nFK;
-    float bck[2];
+    float bck[2];   // backgrounds of the source properties
+    float bckd[2];  // backgrounds of the destination properties
     float coeff[27];
     int64_t box_lo[3], box_hi[3];
     int has_box;
@@ -73,13 +75,13 @@ struct StencilParams {
 // Per-grid entry of a stencil launch.  A grid takes part in global step t
 // when start <= t < start + nsteps; it then reads ping-pong buffer
 // (t - start) & 1 and writes the other one.  A single-grid launch is the
-// entry {start 0, nsteps 1} at t = 0.
+// entry {start 0, nsteps 1} at t = 0.  bck[b][j] is the background of the
+// j-th field of ping-pong buffer b (buffer 0 = the src properties, 1 = dst).
 struct GridInfo {
     int64_t start;
     int64_t nsteps;
     float dt, Du, Dv, F, nFK;
-    float bck[2];
-    float pad_;
+    float bck[2][2];
 };
 
 // Field pointers of a launch: [ping-pong buffer][source property].
@@ -130,8 +132,8 @@ struct sgb_grid {
 
     sgb::DevBuf err;      // unsigned device error word
     int num_sms = 148;
-    int ctas_per_sm = 2;
-    int stages = 6;
+    int ctas_per_sm = 4;
+    int stages = 8;
 };
 
 namespace sgb {

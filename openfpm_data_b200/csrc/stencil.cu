@@ -17,8 +17,11 @@
 // Semantics kept from the reference: a halo or centre value whose mask byte
 // is 0 reads the background value; active = EXIST && !PADDING && inside the
 // inclusive box; HEAT7 writes every point of the destination chunk (active
-// points the update, the others the tile value, as storeBlock does), GS7 and
-// BOX27 write active points only.  Arithmetic follows the reference's FP32
+// points the update, the others the tile value, as storeBlock does; a point
+// whose mask byte is 0 gets the destination's background, which no read can
+// tell from the reference's copy of the source background), GS7 and BOX27
+// write active points only.  Ping-pong steps take each buffer's own
+// background (GridInfo::bck).  Arithmetic follows the reference's FP32
 // association with nvcc's FMA contraction and flush-to-zero (-use_fast_math,
 // src/CMakeLists.txt:158), written with explicit intrinsics so the compiler
 // cannot re-associate it.
@@ -50,7 +53,8 @@ __global__ void __launch_bounds__(256) k_stencil_tile(FieldSet fs, const uint8_t
         const GridInfo gi = grids ? grids[gid[chunk]] : g0;
         if (!(t >= gi.start && t < gi.start + gi.nsteps)) continue;  // uniform across the CTA
         const int par = (int)((t - gi.start) & 1);
-        const float* src[2] = {fs.in[par][0], fs.in[par][NP - 1]};
+        // selects, not a dynamic index into the parameter struct (which would copy it to local memory)
+        const float* src[2] = {par ? fs.in[1][0] : fs.in[0][0], par ? fs.in[1][NP - 1] : fs.in[0][NP - 1]};
         for (int cell = threadIdx.x; cell < TT; cell += blockDim.x) {
             const int tx = cell % T, ty = (cell / T) % T, tz = cell / (T * T);
             const int dx = tx == 0 ? -1 : (tx == T - 1 ? 1 : 0);
@@ -67,7 +71,7 @@ __global__ void __launch_bounds__(256) k_stencil_tile(FieldSet fs, const uint8_t
             const int64_t idx = sc * BS + lx + E * (ly + E * lz);
             const bool ex = sc >= 0 && mask[idx] != 0;
 #pragma unroll
-            for (int p = 0; p < NP; ++p) tile[p][cell] = ex ? src[p][idx] : gi.bck[p];
+            for (int p = 0; p < NP; ++p) tile[p][cell] = ex ? src[p][idx] : (par ? gi.bck[1][p] : gi.bck[0][p]);
         }
         __syncthreads();
         int64_t cx = 0, cy = 0, cz = 0;
@@ -77,8 +81,8 @@ __global__ void __launch_bounds__(256) k_stencil_tile(FieldSet fs, const uint8_t
             cy = ((key / geo.bsz[0]) % geo.bsz[1]) * E;
             cz = (key / (geo.bsz[0] * geo.bsz[1])) * E;
         }
-        float* d0 = fs.out[par][0];
-        float* d1 = fs.out[par][NP - 1];
+        float* d0 = par ? fs.out[1][0] : fs.out[0][0];
+        float* d1 = par ? fs.out[1][NP - 1] : fs.out[0][NP - 1];
         for (int pnt = threadIdx.x; pnt < BS; pnt += blockDim.x) {
             const int x = pnt % E, y = (pnt / E) % E, z = pnt / (E * E);
             const uint8_t m = mask[chunk * BS + pnt];
@@ -90,7 +94,7 @@ __global__ void __launch_bounds__(256) k_stencil_tile(FieldSet fs, const uint8_t
                 const float cur = tile[0][c];
                 d0[gidx] = act ? heat_update(cur, tile[0][c - 1], tile[0][c + 1], tile[0][c - T], tile[0][c + T],
                                              tile[0][c - T * T], tile[0][c + T * T], gi.dt)
-                               : cur;
+                               : (m ? cur : (par ? gi.bck[0][0] : gi.bck[1][0]));
             } else if (KIND == SGB_GS7) {
                 if (!act) continue;
                 const float u = tile[0][c], v = tile[1][c];
@@ -139,6 +143,7 @@ int make_params(sgb_grid* g, int kind, const int* src, const int* dst, const flo
                 return SGB_EINVAL;
             }
         std::memcpy(&prm.bck[j], g->bck[src[j]], 4);
+        std::memcpy(&prm.bckd[j], g->bck[dst[j]], 4);
     }
     if (np == 2 && (src[0] == src[1] || dst[0] == dst[1])) return SGB_EINVAL;
     if (kind == SGB_HEAT7) {
@@ -179,8 +184,10 @@ GridInfo grid_info_of(const StencilParams& prm) {
     gi.Dv = prm.Dv;
     gi.F = prm.F;
     gi.nFK = prm.nFK;
-    gi.bck[0] = prm.bck[0];
-    gi.bck[1] = prm.bck[1];
+    for (int j = 0; j < 2; ++j) {
+        gi.bck[0][j] = prm.bck[j];
+        gi.bck[1][j] = prm.bckd[j];
+    }
     return gi;
 }
 

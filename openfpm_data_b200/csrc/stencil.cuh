@@ -9,9 +9,6 @@
 
 namespace sgb {
 
-constexpr int kConsumerWarps = 8;
-constexpr int kThreads = (kConsumerWarps + 1) * 32;
-
 __device__ __forceinline__ bool in_box(const StencilParams& prm, int64_t cx, int64_t cy, int64_t cz) {
     return cx >= prm.box_lo[0] && cx <= prm.box_hi[0] && cy >= prm.box_lo[1] && cy <= prm.box_hi[1] &&
            cz >= prm.box_lo[2] && cz <= prm.box_hi[2];

@@ -6,15 +6,25 @@
 // tile point by point and substitutes the background where a mask byte is 0.
 //
 // Here: a persistent, warp-specialised kernel.  Each CTA owns a contiguous
-// range of chunk positions.  One producer warp streams every chunk into an
-// S-stage shared-memory ring with 1-D bulk copies (cp.async.bulk, the TMA
-// engine): the source tiles (2 KB per field), the mask tile (512 B), the two
-// z faces (256 B each) and the y=7 / y=0 rows of the y neighbours (8 x 32 B
-// each); completion is counted in bytes on the stage's mbarrier.  The x halo
-// is not fetched: an existing -x / +x neighbour is always the previous / next
-// position of the sorted index (ids differ by one), which is in the ring
-// already, so consumers keep a stage until the next chunk is done.  Eight
-// consumer warps compute from shared memory and store to HBM.
+// range [c0, c1) of chunk positions and streams [lo, hi), the range widened by
+// one chunk on each side, through an S-stage shared-memory ring.  One
+// producer warp issues, per chunk, 1-D bulk copies (cp.async.bulk) of the
+// source tiles (2 KB per field), the mask tile (512 B) and the two z faces
+// (256 B each), and 3-D TMA tensor copies of the two y faces (8 rows of
+// 32 B); completion is counted in bytes on the stage's `full` mbarrier.  The
+// x halo is not fetched: an existing -x / +x neighbour is always the previous
+// / next position of the sorted index, so it sits in the neighbouring stage.
+//
+// Consumers: warp w of kCW computes chunks c0 + w, c0 + w + kCW, ...; each
+// lane owns a pair of x-adjacent points of one y row and marches z = 0..7,
+// carrying the z-1 / z / z+1 values in registers, so a point pair costs five
+// shared loads per field.  A stage is read by the consumers of chunks q - 1,
+// q and q + 1 and is refilled once all three have arrived on its `empty`
+// mbarrier (the producer arrives for those outside [c0, c1)).  Warps run at
+// different speeds, so before waiting on a `full` phase parity a consumer
+// checks the stage's sequence number: the stage may still be completing the
+// copies of chunk q - S, whose phase parity is the opposite one, and parity
+// alone would then read as "done".
 //
 // Points with mask byte 0 hold the background value in HBM (grid.cu keeps
 // that invariant per property, see sgb_grid::clean), so a neighbour value is
@@ -32,6 +42,9 @@
 
 namespace sgb {
 
+constexpr int kCW = 4;                     // consumer warps per CTA
+constexpr int kThreads8 = (kCW + 1) * 32;  // + one producer warp
+
 template <int NP>
 struct alignas(128) Stage8 {
     float tile[NP][512];
@@ -39,10 +52,48 @@ struct alignas(128) Stage8 {
     float zm[NP][64], zp[NP][64];  // [y*8 + x]: z = 7 slice of the -z chunk / z = 0 slice of the +z chunk
     uint8_t mt[512];
     GridInfo gi;
+    float2 bk[NP];       // background of each source field, twice (read in place of absent faces)
     int32_t nn[8];
-    int64_t key;
+    int32_t cx, cy, cz;  // first point of the chunk (box tests)
     int32_t par, active;
+    int32_t seq;         // ring position of the chunk held; -1 before the first
 };
+
+__device__ __forceinline__ float2 lds_f2(uint32_t a) {
+    float2 v;
+    asm volatile("ld.shared.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "r"(a));
+    return v;
+}
+
+__device__ __forceinline__ float lds_f1(uint32_t a) {
+    float v;
+    asm volatile("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(a));
+    return v;
+}
+
+__device__ __forceinline__ uint32_t lds_u16(uint32_t a) {
+    unsigned short v;
+    asm volatile("ld.shared.u16 %0, [%1];" : "=h"(v) : "r"(a));
+    return v;
+}
+
+__device__ __forceinline__ int32_t ld_seq(const int32_t* p) { return *reinterpret_cast<const volatile int32_t*>(p); }
+
+// Wait until ring stage `st` holds chunk q (bounded) and its copies landed.
+template <int NP>
+__device__ __forceinline__ bool wait_chunk(const Stage8<NP>& st, uint64_t* full, int q, uint32_t parity,
+                                           unsigned* err) {
+    if (ld_seq(&st.seq) != q) {
+        const uint64_t t0 = global_timer_ns();
+        for (uint32_t it = 0; ld_seq(&st.seq) != q; ++it) {
+            if ((it & 63u) == 63u && global_timer_ns() - t0 > 2000000000ull) {
+                atomicOr(err, kErrWaitTimeout);
+                return false;
+            }
+        }
+    }
+    return mbar_wait_bounded(full, parity, err);
+}
 
 // The y faces of a chunk are 8 rows of 32 B, 256 B apart: one 3-D tensor
 // copy each.  A field is viewed as a tensor [chunks*8 (z)][8 (y)][8 (x)] of
@@ -91,8 +142,9 @@ static int encode_yface(CUtensorMap* map, const float* base, int64_t chunks) {
     return SGB_OK;
 }
 
+
 template <int KIND, int NP>
-__global__ void __launch_bounds__(kThreads, 2)
+__global__ void __launch_bounds__(kThreads8, 4)
     k_stencil7_e8(FieldSet fs, const __grid_constant__ TmapSet tm, const uint8_t* __restrict__ mask,
                   const int32_t* __restrict__ nn, const int64_t* __restrict__ keys, const int32_t* __restrict__ gid,
                   const GridInfo* __restrict__ grids, GridInfo g0, int64_t n, Geometry geo, StencilParams prm,
@@ -109,17 +161,20 @@ __global__ void __launch_bounds__(kThreads, 2)
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < S; ++s) {
-            mbar_init(&full[s], 1);                // the producer's expect_tx arrival
-            mbar_init(&empty[s], kConsumerWarps);  // one arrival per consumer warp
+            mbar_init(&full[s], 1);   // the producer's (expect_tx) arrival
+            mbar_init(&empty[s], 3);  // the consumers of chunks q - 1, q, q + 1
+            stage[s].seq = -1;
         }
         mbar_fence_init();
     }
     __syncthreads();
     if (c0 >= c1) return;
 
-    if (warp == kConsumerWarps) {
+    if (warp == kCW) {
         // ------------------------------------------------------------ producer
-        int64_t q = 0;
+        const int Q = (int)(hi - lo);
+        int q = 0, s = 0;
+        uint32_t ph = 0;  // phase parity of stage s for chunk q
         bool ok = true;
         // Neighbour rows (8 ints per chunk, contiguous) are fetched in windows
         // of 8 chunks, one window ahead: lane l holds entries l and l + 32 of a
@@ -137,10 +192,9 @@ __global__ void __launch_bounds__(kThreads, 2)
         int32_t gid_nxt = (grids && lo + 8 + lane < hi && lane < 8) ? gid[lo + 8 + lane] : 0;
         int32_t g_last = -1;
         GridInfo gi = g0;
-        for (; q < hi - lo; ++q) {
+        for (; q < Q; ++q) {
             const int64_t c = lo + q;
-            const int s = (int)(q % S);
-            const int j = (int)(q & 7);
+            const int j = q & 7;
             if (j == 0 && q > 0) {
                 w0 = x0v;
                 w1 = x1v;
@@ -157,7 +211,7 @@ __global__ void __launch_bounds__(kThreads, 2)
                     g_last = gc;
                 }
             }
-            if (q >= S && !mbar_wait_bounded(&empty[s], (uint32_t)(q / S - 1) & 1u, err)) {
+            if (q >= S && !mbar_wait_bounded(&empty[s], ph ^ 1u, err)) {
                 ok = false;
                 break;
             }
@@ -166,10 +220,21 @@ __global__ void __launch_bounds__(kThreads, 2)
             const int par = (int)((t - gi.start) & 1);
             if (lane < 8) st.nn[lane] = nb_cur;
             if (lane == 0) {
-                st.key = prm.has_box ? keys[c] : 0;
+                if (prm.has_box) {
+                    const int64_t key = keys[c];
+                    st.cx = (int32_t)((key % geo.bsz[0]) * 8);
+                    st.cy = (int32_t)(((key / geo.bsz[0]) % geo.bsz[1]) * 8);
+                    st.cz = (int32_t)((key / (geo.bsz[0] * geo.bsz[1])) * 8);
+                }
                 st.gi = gi;
+#pragma unroll
+                for (int p = 0; p < NP; ++p) {
+                    const float b = par ? gi.bck[1][p] : gi.bck[0][p];  // no dynamic index into a register struct
+                    st.bk[p] = make_float2(b, b);
+                }
                 st.par = par;
                 st.active = active;
+                *reinterpret_cast<volatile int32_t*>(&st.seq) = q;
             }
             const int32_t fzm = __shfl_sync(0xffffffffu, nb_cur, 4), fzp = __shfl_sync(0xffffffffu, nb_cur, 5);
             const int32_t fym = __shfl_sync(0xffffffffu, nb_cur, 2), fyp = __shfl_sync(0xffffffffu, nb_cur, 3);
@@ -178,7 +243,8 @@ __global__ void __launch_bounds__(kThreads, 2)
                 const uint32_t faces = (fym >= 0) + (fyp >= 0) + (fzm >= 0) + (fzp >= 0);
                 if (lane == 0) mbar_arrive_expect_tx(&full[s], NP * (2048 + 256 * faces) + 512);
                 __syncwarp();
-                const float* sp[2] = {fs.in[par][0], fs.in[par][NP - 1]};
+                const float* sp0 = par ? fs.in[1][0] : fs.in[0][0];
+                const float* sp1 = par ? fs.in[1][NP - 1] : fs.in[0][NP - 1];
                 // per field: own tile, two z faces (contiguous), two y faces (tensor boxes); then the mask tile
                 if (lane < NP * 5 + 1) {
                     const int tk = lane;
@@ -186,7 +252,7 @@ __global__ void __launch_bounds__(kThreads, 2)
                         bulk_g2s(st.mt, mask + c * 512, 512, &full[s]);
                     } else {
                         const int p = tk / 5, r = tk % 5;
-                        const float* src = p == 0 ? sp[0] : sp[1];
+                        const float* src = p == 0 ? sp0 : sp1;
                         if (r == 0) bulk_g2s(st.tile[p], src + c * 512, 2048, &full[s]);
                         else if (r == 1) { if (fzm >= 0) bulk_g2s(st.zm[p], src + (int64_t)fzm * 512 + 448, 256, &full[s]); }
                         else if (r == 2) { if (fzp >= 0) bulk_g2s(st.zp[p], src + (int64_t)fzp * 512, 256, &full[s]); }
@@ -197,118 +263,160 @@ __global__ void __launch_bounds__(kThreads, 2)
             } else if (lane == 0) {
                 mbar_arrive(&full[s]);
             }
+            if (lane == 0) {
+                // consumers of chunk c are c - 1, c, c + 1 inside [c0, c1); arrive for the others
+                const int k = (c - 1 >= c0 && c - 1 < c1) + (c >= c0 && c < c1) + (c + 1 >= c0 && c + 1 < c1);
+                if (k < 3) mbar_arrive_cnt(&empty[s], (uint32_t)(3 - k));
+            }
+            if (++s == S) {
+                s = 0;
+                ph ^= 1u;
+            }
         }
         if (!ok) {
             // let the copies already issued land before the CTA retires
-            for (int64_t r = q - 1; r >= 0 && r >= q - S; --r)
+            for (int r = q - 1; r >= 0 && r >= q - S; --r)
                 mbar_wait_bounded(&full[r % S], (uint32_t)(r / S) & 1u, err, 100000000ull);
         }
         return;
     }
 
     // ---------------------------------------------------------------- consumers
-    const int tid = threadIdx.x;
-    const int z = tid >> 5, y = (tid >> 2) & 7, x0 = (tid & 3) << 1;
-    const int o0 = z * 64 + y * 8 + x0;
-    for (int64_t i = c0; i < c1; ++i) {
-        const int64_t q = i - lo;
-        const int s = (int)(q % S);
-        if (!mbar_wait_bounded(&full[s], (uint32_t)(q / S) & 1u, err)) break;
-        const bool has_next = i + 1 < hi;
-        const int sn = (int)((q + 1) % S);
-        if (has_next && !mbar_wait_bounded(&full[sn], (uint32_t)((q + 1) / S) & 1u, err)) break;
+    const int y = lane >> 2, x0 = (lane & 3) << 1;
+    const int o0 = y * 8 + x0;  // the lane's first point in a z slice
+    int64_t i = c0 + warp;
+    if (i >= c1) return;
+    int q = (int)(i - lo);
+    int s = q % S;
+    uint32_t ph = (uint32_t)(q / S) & 1u;
+    for (; i < c1; i += kCW) {
+        const bool has_prev = i > lo, has_next = i + 1 < hi;
+        const int sm1 = s == 0 ? S - 1 : s - 1, sp1 = s + 1 == S ? 0 : s + 1;
+        const uint32_t phm1 = s == 0 ? ph ^ 1u : ph, php1 = s + 1 == S ? ph ^ 1u : ph;
+        if (has_prev && !wait_chunk(stage[sm1], &full[sm1], q - 1, phm1, err)) break;
+        if (!wait_chunk(stage[s], &full[s], q, ph, err)) break;
+        if (has_next && !wait_chunk(stage[sp1], &full[sp1], q + 1, php1, err)) break;
         const Stage8<NP>& st = stage[s];
         if (st.active) {
-            const Stage8<NP>& pv = stage[(s + S - 1) % S];
-            const Stage8<NP>& nx = stage[sn];
+            const Stage8<NP>& pv = stage[sm1];
+            const Stage8<NP>& nx = stage[sp1];
             const int32_t n0 = st.nn[0], n1 = st.nn[1], n2 = st.nn[2], n3 = st.nn[3], n4 = st.nn[4], n5 = st.nn[5];
             // an absent neighbour is -1, which must not match position i - 1 of chunk 0
             const bool xm_ok = n0 >= 0 && n0 == (int32_t)(i - 1), xp_ok = n1 >= 0 && n1 == (int32_t)(i + 1);
-            const uchar2 m2 = *reinterpret_cast<const uchar2*>(&st.mt[o0]);
-            bool act0 = (m2.x & 1) && !(m2.x & 2), act1 = (m2.y & 1) && !(m2.y & 2);
-            if (prm.has_box) {
-                const int64_t key = st.key;
-                const int64_t cx = (key % geo.bsz[0]) * 8 + x0, cy = ((key / geo.bsz[0]) % geo.bsz[1]) * 8 + y,
-                              cz = (key / (geo.bsz[0] * geo.bsz[1])) * 8 + z;
-                act0 = act0 && in_box(prm, cx, cy, cz);
-                act1 = act1 && in_box(prm, cx + 1, cy, cz);
+            // Shared addresses of the lane's operands at z = 0 and their steps per z.  Absent
+            // neighbour chunks read the stage's background pair with step 0.
+            uint32_t aC[NP], aYm[NP], aYp[NP], aXm[NP], aXp[NP], aZp[NP];
+            float2 zmv[NP], cv[NP];
+#pragma unroll
+            for (int p = 0; p < NP; ++p) {
+                const uint32_t bk = smem_u32(&st.bk[p]);
+                aC[p] = smem_u32(&st.tile[p][o0]);
+                aYm[p] = y > 0 ? aC[p] - 32 : (n2 >= 0 ? smem_u32(&st.ym[p][x0]) : bk);
+                aYp[p] = y < 7 ? aC[p] + 32 : (n3 >= 0 ? smem_u32(&st.yp[p][x0]) : bk);
+                aXm[p] = x0 > 0 ? aC[p] - 4 : (xm_ok ? smem_u32(&pv.tile[p][y * 8 + 7]) : bk);
+                aXp[p] = x0 < 6 ? aC[p] + 8 : (xp_ok ? smem_u32(&nx.tile[p][y * 8]) : bk);
+                aZp[p] = n5 >= 0 ? smem_u32(&st.zp[p][o0]) : bk;
+                zmv[p] = lds_f2(n4 >= 0 ? smem_u32(&st.zm[p][o0]) : bk);
+                cv[p] = lds_f2(aC[p]);
             }
-            const bool need = KIND == SGB_HEAT7 || act0 || act1;
-            if (need) {
-                float2 c2[NP], lap[NP];
+            const uint32_t sYm = y > 0 ? 256u : (n2 >= 0 ? 32u : 0u);
+            const uint32_t sYp = y < 7 ? 256u : (n3 >= 0 ? 32u : 0u);
+            const uint32_t sXm = (x0 > 0 || xm_ok) ? 256u : 0u;
+            const uint32_t sXp = (x0 < 6 || xp_ok) ? 256u : 0u;
+            const uint32_t aM = smem_u32(&st.mt[o0]);
+            const int par = st.par;
+            float* d0 = (par ? fs.out[1][0] : fs.out[0][0]) + i * 512 + o0;
+            float* d1 = (par ? fs.out[1][NP - 1] : fs.out[0][NP - 1]) + i * 512 + o0;
+            const GridInfo gi = st.gi;
+            const float bd = st.gi.bck[par ^ 1][0];  // HEAT7: background of the destination
+            const int32_t bx = st.cx + x0, by = st.cy + y, bz = st.cz;
+#pragma unroll
+            for (int z = 0; z < 8; ++z) {
+                const uint32_t m = lds_u16(aM + z * 64);
+                float2 lap[NP], cur[NP];
 #pragma unroll
                 for (int p = 0; p < NP; ++p) {
-                    const float b = st.gi.bck[p];
-                    const float2 c = *reinterpret_cast<const float2*>(&st.tile[p][o0]);
-                    const float2 ym = y > 0 ? *reinterpret_cast<const float2*>(&st.tile[p][o0 - 8])
-                                            : (n2 >= 0 ? *reinterpret_cast<const float2*>(&st.ym[p][z * 8 + x0]) : make_float2(b, b));
-                    const float2 yp = y < 7 ? *reinterpret_cast<const float2*>(&st.tile[p][o0 + 8])
-                                            : (n3 >= 0 ? *reinterpret_cast<const float2*>(&st.yp[p][z * 8 + x0]) : make_float2(b, b));
-                    const float2 zm = z > 0 ? *reinterpret_cast<const float2*>(&st.tile[p][o0 - 64])
-                                            : (n4 >= 0 ? *reinterpret_cast<const float2*>(&st.zm[p][y * 8 + x0]) : make_float2(b, b));
-                    const float2 zp = z < 7 ? *reinterpret_cast<const float2*>(&st.tile[p][o0 + 64])
-                                            : (n5 >= 0 ? *reinterpret_cast<const float2*>(&st.zp[p][y * 8 + x0]) : make_float2(b, b));
-                    const float xm0 = x0 > 0 ? st.tile[p][o0 - 1] : (xm_ok ? pv.tile[p][o0 + 7] : b);
-                    const float xp1 = x0 < 6 ? st.tile[p][o0 + 2] : (xp_ok ? nx.tile[p][o0 - 6] : b);
-                    c2[p] = c;
-                    lap[p].x = lap7(c.x, xm0, c.y, ym.x, yp.x, zm.x, zp.x);
-                    lap[p].y = lap7(c.y, c.x, xp1, ym.y, yp.y, zm.y, zp.y);
+                    const float2 zp = z < 7 ? lds_f2(aC[p] + (z + 1) * 256) : lds_f2(aZp[p]);
+                    const float2 ym = lds_f2(aYm[p] + z * sYm);
+                    const float2 yp = lds_f2(aYp[p] + z * sYp);
+                    const float xm = lds_f1(aXm[p] + z * sXm);
+                    const float xp = lds_f1(aXp[p] + z * sXp);
+                    const float2 c = cv[p];
+                    lap[p].x = lap7(c.x, xm, c.y, ym.x, yp.x, zmv[p].x, zp.x);
+                    lap[p].y = lap7(c.y, c.x, xp, ym.y, yp.y, zmv[p].y, zp.y);
+                    cur[p] = c;
+                    zmv[p] = c;
+                    cv[p] = zp;
                 }
-                const int64_t gidx = i * 512 + o0;
-                float* d0 = fs.out[st.par][0];
+                const uint32_t m0 = m & 0xffu, m1 = m >> 8;
+                bool act0 = (m0 & 3u) == 1u, act1 = (m1 & 3u) == 1u;  // EXIST and not PADDING
+                if (prm.has_box) {
+                    act0 = act0 && in_box(prm, bx, by, bz + z);
+                    act1 = act1 && in_box(prm, bx + 1, by, bz + z);
+                }
                 if (KIND == SGB_HEAT7) {
-                    const float dt = st.gi.dt;
                     float2 r;
-                    r.x = act0 ? __fmaf_rn(dt, lap[0].x, c2[0].x) : c2[0].x;
-                    r.y = act1 ? __fmaf_rn(dt, lap[0].y, c2[0].y) : c2[0].y;
-                    *reinterpret_cast<float2*>(d0 + gidx) = r;
+                    r.x = act0 ? __fmaf_rn(gi.dt, lap[0].x, cur[0].x) : (m0 ? cur[0].x : bd);
+                    r.y = act1 ? __fmaf_rn(gi.dt, lap[0].y, cur[0].y) : (m1 ? cur[0].y : bd);
+                    *reinterpret_cast<float2*>(d0 + z * 64) = r;
                 } else {
-                    float* d1 = fs.out[st.par][NP - 1];
                     float2 un, vn;
-                    gs_update(c2[0].x, c2[NP - 1].x, lap[0].x, lap[NP - 1].x, st.gi, un.x, vn.x);
-                    gs_update(c2[0].y, c2[NP - 1].y, lap[0].y, lap[NP - 1].y, st.gi, un.y, vn.y);
+                    gs_update(cur[0].x, cur[NP - 1].x, lap[0].x, lap[NP - 1].x, gi, un.x, vn.x);
+                    gs_update(cur[0].y, cur[NP - 1].y, lap[0].y, lap[NP - 1].y, gi, un.y, vn.y);
                     if (act0 && act1) {
-                        *reinterpret_cast<float2*>(d0 + gidx) = un;
-                        *reinterpret_cast<float2*>(d1 + gidx) = vn;
-                    } else if (act0) {
-                        d0[gidx] = un.x;
-                        d1[gidx] = vn.x;
-                    } else if (act1) {
-                        d0[gidx + 1] = un.y;
-                        d1[gidx + 1] = vn.y;
+                        *reinterpret_cast<float2*>(d0 + z * 64) = un;
+                        *reinterpret_cast<float2*>(d1 + z * 64) = vn;
+                    } else {
+                        if (act0) {
+                            d0[z * 64] = un.x;
+                            d1[z * 64] = vn.x;
+                        }
+                        if (act1) {
+                            d0[z * 64 + 1] = un.y;
+                            d1[z * 64 + 1] = vn.y;
+                        }
                     }
                 }
             }
         }
-        if (i - 1 >= lo) {
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&empty[(s + S - 1) % S]);
+        __syncwarp();
+        if (lane == 0) {
+            if (has_prev) mbar_arrive(&empty[sm1]);
+            mbar_arrive(&empty[s]);
+            if (has_next) mbar_arrive(&empty[sp1]);
+        }
+        q += kCW;
+        s += kCW;  // S >= kCW: at most one wrap
+        if (s >= S) {
+            s -= S;
+            ph ^= 1u;
         }
     }
 }
 
+template <int KIND, int NP>
+static int launch_kind(const LaunchDesc& L, const TmapSet& tm, cudaStream_t s) {
+    // ring depth: all kCW consumers busy plus the two halo chunks, within the shared memory of one CTA
+    const size_t per = sizeof(Stage8<NP>) + 16;
+    const int smax = (int)((227u * 1024u) / per);
+    const int S = std::min(std::max(L.stages, kCW + 2), smax);
+    const size_t smem = (size_t)S * per;
+    auto kern = k_stencil7_e8<KIND, NP>;
+    SGB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    kern<<<L.ctas, kThreads8, smem, s>>>(L.fs, tm, L.mask, L.nn, L.keys, L.gid, L.grids, L.g0, L.n, L.geo, L.prm, L.t,
+                                         S, L.err);
+    SGB_CUDA(cudaGetLastError());
+    return SGB_OK;
+}
+
 int launch_e8(const LaunchDesc& L, cudaStream_t s) {
-    const int S = L.stages;
     const int np = L.kind == SGB_GS7 ? 2 : 1;
     TmapSet tm;
     std::memset(&tm, 0, sizeof(tm));
     for (int b = 0; b < 2; ++b)
         for (int p = 0; p < np; ++p) SGB_TRY(encode_yface(&tm.yface[b][p], L.fs.in[b][p], L.arr_chunks));
-    if (L.kind == SGB_GS7) {
-        const size_t smem = (size_t)S * sizeof(Stage8<2>) + 2 * S * 8;
-        auto kern = k_stencil7_e8<SGB_GS7, 2>;
-        SGB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        kern<<<L.ctas, kThreads, smem, s>>>(L.fs, tm, L.mask, L.nn, L.keys, L.gid, L.grids, L.g0, L.n, L.geo, L.prm,
-                                            L.t, S, L.err);
-    } else {
-        const size_t smem = (size_t)S * sizeof(Stage8<1>) + 2 * S * 8;
-        auto kern = k_stencil7_e8<SGB_HEAT7, 1>;
-        SGB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        kern<<<L.ctas, kThreads, smem, s>>>(L.fs, tm, L.mask, L.nn, L.keys, L.gid, L.grids, L.g0, L.n, L.geo, L.prm,
-                                            L.t, S, L.err);
-    }
-    SGB_CUDA(cudaGetLastError());
-    return SGB_OK;
+    if (L.kind == SGB_GS7) return launch_kind<SGB_GS7, 2>(L, tm, s);
+    return launch_kind<SGB_HEAT7, 1>(L, tm, s);
 }
 
 }  // namespace sgb

@@ -25,6 +25,13 @@ OPS = {"sRight_": L.OP_RIGHT, "sLeft_": L.OP_LEFT, "sadd_": L.OP_ADD, "smax_": L
        "sBitwiseOr_": L.OP_OR, None: L.OP_NONE, "none": L.OP_NONE}
 
 
+class _View(C.Structure):
+    """sgb_view of include/sgb200.h."""
+    _fields_ = [("n", C.c_int64), ("edge", C.c_int), ("bs", C.c_int), ("nprop", C.c_int), ("nn_kind", C.c_int),
+                ("size", C.c_int64 * 3), ("bsz", C.c_int64 * 3), ("keys", C.c_void_p), ("data", C.c_void_p * 8),
+                ("mask", C.c_void_p), ("nn", C.c_void_p)]
+
+
 def _stream(stream=None) -> int:
     if stream is None:
         return torch.cuda.current_stream().cuda_stream
@@ -111,6 +118,26 @@ class SparseGridGpu:
         ptrs, keep = self._values(values)
         L.check(self._lib.sgb_insert_lin(self._h, l.shape[0], l.data_ptr(), ptrs, _stream(stream)), "sgb_insert_lin")
         self._keep = (l, keep)
+
+    def insert_pools(self, counts: torch.Tensor, lin: torch.Tensor, values, stream=None) -> None:
+        """Stage per-CTA insert pools (setGPUInsertBuffer + insert<p> + flush_block_insert):
+        counts int32 [npools], lin int64 [npools, nslot], values[p] [npools, nslot] or None."""
+        dev = f"cuda:{self.device}"
+        cnt = counts.to(device=dev, dtype=torch.int32).contiguous()
+        l = lin.to(device=dev, dtype=torch.int64).contiguous()
+        npools, nslot = l.shape
+        ptrs, keep = self._values(values)
+        L.check(self._lib.sgb_insert_pools(self._h, npools, nslot, cnt.data_ptr(), l.data_ptr(), ptrs,
+                                           _stream(stream)), "sgb_insert_pools")
+        self._keep = (cnt, l, keep)
+
+    def view(self, nn: int = L.NN_STAR, stream=None) -> dict:
+        """Device view for user kernels (toKernel): sizes and raw device pointers (sgb_get_view)."""
+        v = _View()
+        L.check(self._lib.sgb_get_view(self._h, nn, C.byref(v), _stream(stream)), "sgb_get_view")
+        return {"n": v.n, "edge": v.edge, "bs": v.bs, "nprop": v.nprop, "nn_kind": v.nn_kind,
+                "size": tuple(v.size), "bsz": tuple(v.bsz), "keys": v.keys or 0,
+                "data": [v.data[p] or 0 for p in range(v.nprop)], "mask": v.mask or 0, "nn": v.nn or 0}
 
     def flush(self, ops: Iterable, stream=None) -> None:
         """flush<ops...>: one reduction per property (sgb_op ids or reference names)."""

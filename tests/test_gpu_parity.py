@@ -187,16 +187,18 @@ def test_tag_boundaries_2d_golden_as_slab(sgb):
 
 
 # ------------------------------------------------------------------ stencils
-def _load_pointset(sgb, ps, edge, nprop_extra=1):
-    """Grid with the point set's fields followed by as many ping-pong copies."""
+def _load_pointset(sgb, ps, edge, nprop_extra=1, bcks=None):
+    """Grid with the point set's fields followed by as many ping-pong copies
+    (backgrounds `bcks` per property, default the point set's)."""
     nf = len(ps.values)
     keys, data, mask = W.build_block_map(ps.coords, ps.values, ps.size, edge, ps.bck)
     ptypes = [O.T_F32] * (nf * 2)
     g = sgb.SparseGridGpu(ps.size, ["f32"] * (nf * 2), edge=edge)
     o = O.OracleGrid(ps.size, edge=edge, ptypes=ptypes)
     for p in range(nf * 2):
-        g.setBackgroundValue(p, ps.bck[p % nf])
-        o.set_background(p, ps.bck[p % nf])
+        b = ps.bck[p % nf] if bcks is None else bcks[p]
+        g.setBackgroundValue(p, b)
+        o.set_background(p, b)
     full = data + [d.copy() for d in data]
     g.load_map(keys, full, mask)
     o.load_map(keys, full, mask)
@@ -251,11 +253,46 @@ def test_gray_scott_matches_oracle(sgb, edge):
     g.check_device_errors()
 
 
+@pytest.mark.parametrize("edge", [8, 4])
+@pytest.mark.parametrize("kind", ["heat", "gs"])
+def test_pingpong_with_distinct_backgrounds(sgb, edge, kind):
+    """Source and destination properties with different backgrounds: every
+    ping-pong step must substitute the background of the buffer it reads
+    (HeatStencil's storeBlock copies the source background into the
+    destination's non-existing points; reads there give the destination's)."""
+    if kind == "heat":
+        ps = W.heat_shell()
+        g, o = _load_pointset(sgb, ps, edge, bcks=[0.3, 0.9])
+        fin = g.run_steps(sgb.HEAT7, [0], [1], [W.HEAT_DT], 7, use_graph=True)
+        for k in range(7):
+            o.heat7(k % 2, 1 - k % 2, W.HEAT_DT)
+        assert fin is True
+        props = [0, 1]
+    else:
+        ps = _small_gs(size=64, nballs=4, seed=5)
+        g, o = _load_pointset(sgb, ps, edge, bcks=[1.0, 0.0, 0.75, 0.125])
+        prm = [W.GS_PARAMS[k] for k in ("Du", "Dv", "F", "k", "dt")]
+        g.run_steps(sgb.GS7, [0, 1], [2, 3], prm, 7, use_graph=True)
+        for k in range(7):
+            a, b = ([0, 1], [2, 3]) if k % 2 == 0 else ([2, 3], [0, 1])
+            o.gs7(a[0], a[1], b[0], b[1], *prm)
+        props = [0, 1, 2, 3]
+    _compare_maps(g, o, props=props, exact=False)
+    # reads of non-existing points see each property's own background
+    keys, data, mask = g.deviceToHost()
+    n = len(keys)
+    off = (mask[: n * g.bs] & 1) == 0
+    bcks = [0.3, 0.9] if kind == "heat" else [1.0, 0.0, 0.75, 0.125]
+    for p in props:
+        assert np.all(data[p][: n * g.bs][off] == np.float32(bcks[p]))
+    g.check_device_errors()
+
+
 def test_gray_scott_launch_configs_agree(sgb):
     ps = _small_gs(size=80, nballs=5, seed=4)
     prm = [W.GS_PARAMS[k] for k in ("Du", "Dv", "F", "k", "dt")]
     outs = []
-    for ctas, stages in [(1, 3), (2, 6), (3, 8), (4, 4)]:
+    for ctas, stages in [(1, 3), (2, 6), (3, 8), (4, 4), (2, 12), (8, 16)]:
         g, _ = _load_pointset(sgb, ps, 8)
         g.setLaunchConfig(ctas, stages)
         g.run_steps(sgb.GS7, [0, 1], [2, 3], prm, 9)
