@@ -42,8 +42,8 @@ L2_BYTES = 126 * 2 ** 20
 METRIC = "stencil Gpts/s (Gray-Scott 7-point, 512^3 sparse grid)"
 UNIT = "Gpts/s"
 ALG_BYTES_PER_PT = 17
-# the library's default launch configuration of the pipelined 8^3 kernel
-DEFAULT_CTAS_PER_SM, DEFAULT_STAGES = 4, 8
+# the library's default launch configuration of the pipelined 8^3 kernel (automatic ring depth)
+DEFAULT_CTAS_PER_SM, DEFAULT_STAGES = 4, "auto"
 WORKLOADS = ("gs512", "heat128", "insert1024", "batched256", "served")
 
 

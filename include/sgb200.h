@@ -233,9 +233,12 @@ int sgb_check_device_errors(sgb_grid* g, sgb_stream s);
 /* Bytes of device memory held by the grid. */
 int sgb_device_bytes(const sgb_grid* g, int64_t* bytes);
 
-/* Stencil launch configuration: CTAs per SM (1..8) and staging depth
- * (3..16 chunks in flight per CTA; the 8^3 kernel uses at least 6 and at
- * most what fits in one CTA's shared memory); 0 keeps the current value. */
+/* Stencil launch configuration of the 8^3 kernel: CTAs per SM (1..8, two
+ * warps each, every warp its own pipeline) and the staging ring depth per
+ * warp (3..16 chunks, at most what fits in one CTA's shared memory, or -1
+ * for the automatic depth: the deepest ring, up to 8, with which the
+ * requested CTAs per SM stay resident; the default); 0 keeps the current
+ * value. */
 int sgb_set_launch_config(sgb_grid* g, int ctas_per_sm, int stages);
 
 /* ---------------------------------------------------------------- batches

@@ -133,7 +133,7 @@ struct sgb_grid {
     sgb::DevBuf err;      // unsigned device error word
     int num_sms = 148;
     int ctas_per_sm = 4;
-    int stages = 8;
+    int stages = 0;  // 0: deepest staging ring that keeps ctas_per_sm CTAs resident
 };
 
 namespace sgb {

@@ -5,26 +5,22 @@
 // (src/SparseGridGpu/SparseGridGpu_ker_util.hpp:487-564) gathers the 10^3
 // tile point by point and substitutes the background where a mask byte is 0.
 //
-// Here: a persistent, warp-specialised kernel.  Each CTA owns a contiguous
-// range [c0, c1) of chunk positions and streams [lo, hi), the range widened by
-// one chunk on each side, through an S-stage shared-memory ring.  One
-// producer warp issues, per chunk, 1-D bulk copies (cp.async.bulk) of the
-// source tiles (2 KB per field), the mask tile (512 B) and the two z faces
-// (256 B each), and 3-D TMA tensor copies of the two y faces (8 rows of
-// 32 B); completion is counted in bytes on the stage's `full` mbarrier.  The
-// x halo is not fetched: an existing -x / +x neighbour is always the previous
-// / next position of the sorted index, so it sits in the neighbouring stage.
+// Here every warp is an independent pipeline over a contiguous range [a, b)
+// of chunk positions.  It streams [lo, hi), the range widened by one chunk on
+// each side, through its own R-stage shared-memory ring: per chunk, lanes
+// issue 1-D bulk copies (cp.async.bulk) of the source tiles (2 KB per field),
+// the mask tile (512 B) and the two z faces (256 B each), and 3-D TMA tensor
+// copies of the two y faces (8 rows of 32 B), counted in bytes on the stage's
+// mbarrier.  The x halo is not fetched: an existing -x / +x neighbour is
+// always the previous / next position of the sorted index, so it sits in the
+// neighbouring stage of the same ring.  While chunk q is computed, chunks up
+// to q - 2 + R are in flight; after it, the stage of chunk q - 1 is refilled
+// with chunk q - 1 + R.  A warp waits only on its own barriers, in order, so
+// phase parities are exact and no warp ever waits for another.
 //
-// Consumers: warp w of kCW computes chunks c0 + w, c0 + w + kCW, ...; each
-// lane owns a pair of x-adjacent points of one y row and marches z = 0..7,
-// carrying the z-1 / z / z+1 values in registers, so a point pair costs five
-// shared loads per field.  A stage is read by the consumers of chunks q - 1,
-// q and q + 1 and is refilled once all three have arrived on its `empty`
-// mbarrier (the producer arrives for those outside [c0, c1)).  Warps run at
-// different speeds, so before waiting on a `full` phase parity a consumer
-// checks the stage's sequence number: the stage may still be completing the
-// copies of chunk q - S, whose phase parity is the opposite one, and parity
-// alone would then read as "done".
+// Compute: each lane owns a pair of x-adjacent points of one y row and
+// marches z = 0..7, carrying the z-1 / z / z+1 values in registers, so a
+// point pair costs five shared loads per field.
 //
 // Points with mask byte 0 hold the background value in HBM (grid.cu keeps
 // that invariant per property, see sgb_grid::clean), so a neighbour value is
@@ -42,8 +38,8 @@
 
 namespace sgb {
 
-constexpr int kCW = 4;                     // consumer warps per CTA
-constexpr int kThreads8 = (kCW + 1) * 32;  // + one producer warp
+constexpr int kWarps = 2;                  // warps per CTA, each its own pipeline
+constexpr int kThreads8 = kWarps * 32;
 
 template <int NP>
 struct alignas(128) Stage8 {
@@ -56,7 +52,6 @@ struct alignas(128) Stage8 {
     int32_t nn[8];
     int32_t cx, cy, cz;  // first point of the chunk (box tests)
     int32_t par, active;
-    int32_t seq;         // ring position of the chunk held; -1 before the first
 };
 
 __device__ __forceinline__ float2 lds_f2(uint32_t a) {
@@ -75,24 +70,6 @@ __device__ __forceinline__ uint32_t lds_u16(uint32_t a) {
     unsigned short v;
     asm volatile("ld.shared.u16 %0, [%1];" : "=h"(v) : "r"(a));
     return v;
-}
-
-__device__ __forceinline__ int32_t ld_seq(const int32_t* p) { return *reinterpret_cast<const volatile int32_t*>(p); }
-
-// Wait until ring stage `st` holds chunk q (bounded) and its copies landed.
-template <int NP>
-__device__ __forceinline__ bool wait_chunk(const Stage8<NP>& st, uint64_t* full, int q, uint32_t parity,
-                                           unsigned* err) {
-    if (ld_seq(&st.seq) != q) {
-        const uint64_t t0 = global_timer_ns();
-        for (uint32_t it = 0; ld_seq(&st.seq) != q; ++it) {
-            if ((it & 63u) == 63u && global_timer_ns() - t0 > 2000000000ull) {
-                atomicOr(err, kErrWaitTimeout);
-                return false;
-            }
-        }
-    }
-    return mbar_wait_bounded(full, parity, err);
 }
 
 // The y faces of a chunk are 8 rows of 32 B, 256 B apart: one 3-D tensor
@@ -143,163 +120,150 @@ static int encode_yface(CUtensorMap* map, const float* base, int64_t chunks) {
 }
 
 
+
 template <int KIND, int NP>
-__global__ void __launch_bounds__(kThreads8, 4)
+__global__ void __launch_bounds__(kThreads8)
     k_stencil7_e8(FieldSet fs, const __grid_constant__ TmapSet tm, const uint8_t* __restrict__ mask,
                   const int32_t* __restrict__ nn, const int64_t* __restrict__ keys, const int32_t* __restrict__ gid,
                   const GridInfo* __restrict__ grids, GridInfo g0, int64_t n, Geometry geo, StencilParams prm,
-                  int64_t t, int S, unsigned* err) {
+                  int64_t t, int R, int64_t nwarps, unsigned* err) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    Stage8<NP>* stage = reinterpret_cast<Stage8<NP>*>(smem_raw);
-    uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + (size_t)S * sizeof(Stage8<NP>));
-    uint64_t* empty = full + S;
-
-    const int64_t nct = gridDim.x;
-    const int64_t c0 = n * blockIdx.x / nct, c1 = n * (blockIdx.x + 1) / nct;
-    const int64_t lo = c0 > 0 ? c0 - 1 : 0, hi = c1 + 1 < n ? c1 + 1 : n;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-
-    if (threadIdx.x == 0) {
-        for (int s = 0; s < S; ++s) {
-            mbar_init(&full[s], 1);   // the producer's (expect_tx) arrival
-            mbar_init(&empty[s], 3);  // the consumers of chunks q - 1, q, q + 1
-            stage[s].seq = -1;
-        }
+    Stage8<NP>* ring = reinterpret_cast<Stage8<NP>*>(smem_raw) + (size_t)warp * R;
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + (size_t)kWarps * R * sizeof(Stage8<NP>)) + warp * R;
+    const int64_t gw = (int64_t)blockIdx.x * kWarps + warp;
+    if (gw >= nwarps) return;
+    const int64_t a = n * gw / nwarps, b = n * (gw + 1) / nwarps;
+    if (a >= b) return;
+    const int64_t lo = a > 0 ? a - 1 : 0, hi = b < n ? b + 1 : n;
+    const int Q = (int)(hi - lo);
+    if (lane == 0) {
+        for (int r = 0; r < R; ++r) mbar_init(&full[r], 1);  // the issuing lane's expect_tx arrival
         mbar_fence_init();
     }
-    __syncthreads();
-    if (c0 >= c1) return;
+    __syncwarp();
 
-    if (warp == kCW) {
-        // ------------------------------------------------------------ producer
-        const int Q = (int)(hi - lo);
-        int q = 0, s = 0;
-        uint32_t ph = 0;  // phase parity of stage s for chunk q
-        bool ok = true;
-        // Neighbour rows (8 ints per chunk, contiguous) are fetched in windows
-        // of 8 chunks, one window ahead: lane l holds entries l and l + 32 of a
-        // window, so no chunk waits on a dependent global load.
-        const int64_t nnend = hi * 8;
-        auto load_win = [&](int64_t first, int32_t& a, int32_t& b) {
-            const int64_t e = first * 8 + lane;
-            a = e < nnend ? nn[e] : -1;
-            b = e + 32 < nnend ? nn[e + 32] : -1;
-        };
-        int32_t w0, w1, x0v, x1v;
-        load_win(lo, w0, w1);
-        load_win(lo + 8, x0v, x1v);
-        int32_t gid_win = (grids && lo + lane < hi && lane < 8) ? gid[lo + lane] : 0;
-        int32_t gid_nxt = (grids && lo + 8 + lane < hi && lane < 8) ? gid[lo + 8 + lane] : 0;
-        int32_t g_last = -1;
-        GridInfo gi = g0;
-        for (; q < Q; ++q) {
-            const int64_t c = lo + q;
-            const int j = q & 7;
-            if (j == 0 && q > 0) {
-                w0 = x0v;
-                w1 = x1v;
-                gid_win = gid_nxt;
-                load_win(c + 8, x0v, x1v);
-                gid_nxt = (grids && c + 8 + lane < hi && lane < 8) ? gid[c + 8 + lane] : 0;
+    // ------------------------------------------------------------ issue side
+    // Neighbour rows (8 ints per chunk, contiguous) are fetched in windows of
+    // 8 chunks, one window ahead: lane l holds entries l and l + 32 of a window.
+    const int64_t nnend = hi * 8;
+    auto load_win = [&](int64_t first, int32_t& wa, int32_t& wb) {
+        const int64_t e = first * 8 + lane;
+        wa = e < nnend ? nn[e] : -1;
+        wb = e + 32 < nnend ? nn[e + 32] : -1;
+    };
+    int32_t w0, w1, x0v, x1v;
+    load_win(lo, w0, w1);
+    load_win(lo + 8, x0v, x1v);
+    int32_t gid_win = (grids && lo + lane < hi && lane < 8) ? gid[lo + lane] : 0;
+    int32_t gid_nxt = (grids && lo + 8 + lane < hi && lane < 8) ? gid[lo + 8 + lane] : 0;
+    int32_t g_last = -1;
+    GridInfo gi = g0;
+    // Fill ring slot `slot` with chunk lo + q; q increases by one per call.
+    auto issue = [&](int q, int slot) {
+        const int64_t c = lo + q;
+        const int j = q & 7;
+        if (j == 0 && q > 0) {
+            w0 = x0v;
+            w1 = x1v;
+            gid_win = gid_nxt;
+            load_win(c + 8, x0v, x1v);
+            gid_nxt = (grids && c + 8 + lane < hi && lane < 8) ? gid[c + 8 + lane] : 0;
+        }
+        const int32_t wsel = j < 4 ? w0 : w1;  // entries j*8 .. j*8+7 of the window
+        const int32_t nb_cur = __shfl_sync(0xffffffffu, wsel, ((j & 3) << 3) + (lane & 7));
+        if (grids) {
+            const int32_t gc = __shfl_sync(0xffffffffu, gid_win, j);
+            if (gc != g_last) {  // chunks of one grid are contiguous: one load per grid
+                gi = grids[gc];
+                g_last = gc;
             }
-            const int32_t wsel = j < 4 ? w0 : w1;  // entries j*8 .. j*8+7 of the window
-            const int32_t nb_cur = __shfl_sync(0xffffffffu, wsel, ((j & 3) << 3) + (lane & 7));
-            if (grids) {
-                const int32_t gc = __shfl_sync(0xffffffffu, gid_win, j);
-                if (gc != g_last) {  // chunks of one grid are contiguous: one load per grid
-                    gi = grids[gc];
-                    g_last = gc;
+        }
+        Stage8<NP>& st = ring[slot];
+        uint64_t* bar = &full[slot];
+        const bool active = t >= gi.start && t < gi.start + gi.nsteps;
+        const int par = (int)((t - gi.start) & 1);
+        if (lane < 8) st.nn[lane] = nb_cur;
+        if (lane == 0) {
+            if (prm.has_box) {
+                const int64_t key = keys[c];
+                st.cx = (int32_t)((key % geo.bsz[0]) * 8);
+                st.cy = (int32_t)(((key / geo.bsz[0]) % geo.bsz[1]) * 8);
+                st.cz = (int32_t)((key / (geo.bsz[0] * geo.bsz[1])) * 8);
+            }
+            st.gi = gi;
+#pragma unroll
+            for (int p = 0; p < NP; ++p) {
+                const float bv = par ? gi.bck[1][p] : gi.bck[0][p];  // no dynamic index into a register struct
+                st.bk[p] = make_float2(bv, bv);
+            }
+            st.par = par;
+            st.active = active;
+        }
+        const int32_t fzm = __shfl_sync(0xffffffffu, nb_cur, 4), fzp = __shfl_sync(0xffffffffu, nb_cur, 5);
+        const int32_t fym = __shfl_sync(0xffffffffu, nb_cur, 2), fyp = __shfl_sync(0xffffffffu, nb_cur, 3);
+        __syncwarp();
+        if (active) {
+            const uint32_t faces = (fym >= 0) + (fyp >= 0) + (fzm >= 0) + (fzp >= 0);
+            if (lane == 0) mbar_arrive_expect_tx(bar, NP * (2048 + 256 * faces) + 512);
+            __syncwarp();
+            const float* sp0 = par ? fs.in[1][0] : fs.in[0][0];
+            const float* sp1 = par ? fs.in[1][NP - 1] : fs.in[0][NP - 1];
+            // per field: own tile, two z faces (contiguous), two y faces (tensor boxes); then the mask tile
+            if (lane < NP * 5 + 1) {
+                if (lane == NP * 5) {
+                    bulk_g2s(st.mt, mask + c * 512, 512, bar);
+                } else {
+                    const int p = lane / 5, r = lane % 5;
+                    const float* src = p == 0 ? sp0 : sp1;
+                    if (r == 0) bulk_g2s(st.tile[p], src + c * 512, 2048, bar);
+                    else if (r == 1) { if (fzm >= 0) bulk_g2s(st.zm[p], src + (int64_t)fzm * 512 + 448, 256, bar); }
+                    else if (r == 2) { if (fzp >= 0) bulk_g2s(st.zp[p], src + (int64_t)fzp * 512, 256, bar); }
+                    else if (r == 3) { if (fym >= 0) tma_yface(st.ym[p], &tm.yface[par][p], 7, fym * 8, bar); }
+                    else { if (fyp >= 0) tma_yface(st.yp[p], &tm.yface[par][p], 0, fyp * 8, bar); }
                 }
             }
-            if (q >= S && !mbar_wait_bounded(&empty[s], ph ^ 1u, err)) {
+        } else if (lane == 0) {
+            mbar_arrive(bar);
+        }
+    };
+
+    const int npro = Q < R ? Q : R;
+    for (int q = 0; q < npro; ++q) issue(q, q);
+    int issued = npro;
+
+    // ------------------------------------------------------------ compute side
+    const int y = lane >> 2, x0 = (lane & 3) << 1;
+    const int o0 = y * 8 + x0;  // the lane's first point in a z slice
+    int waited = 0, ws = 0;     // chunks [0, waited) have landed; ws = slot of chunk `waited`
+    uint32_t wph = 0;           // phase parity of slot ws for chunk `waited`
+    int q = (int)(a - lo);
+    int sq = q;                 // slot of chunk q (q < R)
+    for (int64_t i = a; i < b; ++i, ++q) {
+        const int need = i + 1 < hi ? q + 1 : q;
+        bool ok = true;
+        while (waited <= need) {
+            if (!mbar_wait_bounded(&full[ws], wph, err)) {
                 ok = false;
                 break;
             }
-            Stage8<NP>& st = stage[s];
-            const bool active = t >= gi.start && t < gi.start + gi.nsteps;
-            const int par = (int)((t - gi.start) & 1);
-            if (lane < 8) st.nn[lane] = nb_cur;
-            if (lane == 0) {
-                if (prm.has_box) {
-                    const int64_t key = keys[c];
-                    st.cx = (int32_t)((key % geo.bsz[0]) * 8);
-                    st.cy = (int32_t)(((key / geo.bsz[0]) % geo.bsz[1]) * 8);
-                    st.cz = (int32_t)((key / (geo.bsz[0] * geo.bsz[1])) * 8);
-                }
-                st.gi = gi;
-#pragma unroll
-                for (int p = 0; p < NP; ++p) {
-                    const float b = par ? gi.bck[1][p] : gi.bck[0][p];  // no dynamic index into a register struct
-                    st.bk[p] = make_float2(b, b);
-                }
-                st.par = par;
-                st.active = active;
-                *reinterpret_cast<volatile int32_t*>(&st.seq) = q;
+            if (++ws == R) {
+                ws = 0;
+                wph ^= 1u;
             }
-            const int32_t fzm = __shfl_sync(0xffffffffu, nb_cur, 4), fzp = __shfl_sync(0xffffffffu, nb_cur, 5);
-            const int32_t fym = __shfl_sync(0xffffffffu, nb_cur, 2), fyp = __shfl_sync(0xffffffffu, nb_cur, 3);
-            __syncwarp();
-            if (active) {
-                const uint32_t faces = (fym >= 0) + (fyp >= 0) + (fzm >= 0) + (fzp >= 0);
-                if (lane == 0) mbar_arrive_expect_tx(&full[s], NP * (2048 + 256 * faces) + 512);
-                __syncwarp();
-                const float* sp0 = par ? fs.in[1][0] : fs.in[0][0];
-                const float* sp1 = par ? fs.in[1][NP - 1] : fs.in[0][NP - 1];
-                // per field: own tile, two z faces (contiguous), two y faces (tensor boxes); then the mask tile
-                if (lane < NP * 5 + 1) {
-                    const int tk = lane;
-                    if (tk == NP * 5) {
-                        bulk_g2s(st.mt, mask + c * 512, 512, &full[s]);
-                    } else {
-                        const int p = tk / 5, r = tk % 5;
-                        const float* src = p == 0 ? sp0 : sp1;
-                        if (r == 0) bulk_g2s(st.tile[p], src + c * 512, 2048, &full[s]);
-                        else if (r == 1) { if (fzm >= 0) bulk_g2s(st.zm[p], src + (int64_t)fzm * 512 + 448, 256, &full[s]); }
-                        else if (r == 2) { if (fzp >= 0) bulk_g2s(st.zp[p], src + (int64_t)fzp * 512, 256, &full[s]); }
-                        else if (r == 3) { if (fym >= 0) tma_yface(st.ym[p], &tm.yface[par][p], 7, fym * 8, &full[s]); }
-                        else { if (fyp >= 0) tma_yface(st.yp[p], &tm.yface[par][p], 0, fyp * 8, &full[s]); }
-                    }
-                }
-            } else if (lane == 0) {
-                mbar_arrive(&full[s]);
-            }
-            if (lane == 0) {
-                // consumers of chunk c are c - 1, c, c + 1 inside [c0, c1); arrive for the others
-                const int k = (c - 1 >= c0 && c - 1 < c1) + (c >= c0 && c < c1) + (c + 1 >= c0 && c + 1 < c1);
-                if (k < 3) mbar_arrive_cnt(&empty[s], (uint32_t)(3 - k));
-            }
-            if (++s == S) {
-                s = 0;
-                ph ^= 1u;
-            }
+            ++waited;
         }
         if (!ok) {
-            // let the copies already issued land before the CTA retires
-            for (int r = q - 1; r >= 0 && r >= q - S; --r)
-                mbar_wait_bounded(&full[r % S], (uint32_t)(r / S) & 1u, err, 100000000ull);
+            // let the copies already issued land before the warp retires
+            for (int r = waited + 1; r < issued; ++r)
+                mbar_wait_bounded(&full[r % R], (uint32_t)(r / R) & 1u, err, 100000000ull);
+            return;
         }
-        return;
-    }
-
-    // ---------------------------------------------------------------- consumers
-    const int y = lane >> 2, x0 = (lane & 3) << 1;
-    const int o0 = y * 8 + x0;  // the lane's first point in a z slice
-    int64_t i = c0 + warp;
-    if (i >= c1) return;
-    int q = (int)(i - lo);
-    int s = q % S;
-    uint32_t ph = (uint32_t)(q / S) & 1u;
-    for (; i < c1; i += kCW) {
-        const bool has_prev = i > lo, has_next = i + 1 < hi;
-        const int sm1 = s == 0 ? S - 1 : s - 1, sp1 = s + 1 == S ? 0 : s + 1;
-        const uint32_t phm1 = s == 0 ? ph ^ 1u : ph, php1 = s + 1 == S ? ph ^ 1u : ph;
-        if (has_prev && !wait_chunk(stage[sm1], &full[sm1], q - 1, phm1, err)) break;
-        if (!wait_chunk(stage[s], &full[s], q, ph, err)) break;
-        if (has_next && !wait_chunk(stage[sp1], &full[sp1], q + 1, php1, err)) break;
-        const Stage8<NP>& st = stage[s];
+        const int sp = sq == 0 ? R - 1 : sq - 1, sn = sq + 1 == R ? 0 : sq + 1;
+        const Stage8<NP>& st = ring[sq];
         if (st.active) {
-            const Stage8<NP>& pv = stage[sm1];
-            const Stage8<NP>& nx = stage[sp1];
+            const Stage8<NP>& pv = ring[sp];
+            const Stage8<NP>& nx = ring[sn];
             const int32_t n0 = st.nn[0], n1 = st.nn[1], n2 = st.nn[2], n3 = st.nn[3], n4 = st.nn[4], n5 = st.nn[5];
             // an absent neighbour is -1, which must not match position i - 1 of chunk 0
             const bool xm_ok = n0 >= 0 && n0 == (int32_t)(i - 1), xp_ok = n1 >= 0 && n1 == (int32_t)(i + 1);
@@ -327,7 +291,7 @@ __global__ void __launch_bounds__(kThreads8, 4)
             const int par = st.par;
             float* d0 = (par ? fs.out[1][0] : fs.out[0][0]) + i * 512 + o0;
             float* d1 = (par ? fs.out[1][NP - 1] : fs.out[0][NP - 1]) + i * 512 + o0;
-            const GridInfo gi = st.gi;
+            const GridInfo cgi = st.gi;
             const float bd = st.gi.bck[par ^ 1][0];  // HEAT7: background of the destination
             const int32_t bx = st.cx + x0, by = st.cy + y, bz = st.cz;
 #pragma unroll
@@ -356,13 +320,13 @@ __global__ void __launch_bounds__(kThreads8, 4)
                 }
                 if (KIND == SGB_HEAT7) {
                     float2 r;
-                    r.x = act0 ? __fmaf_rn(gi.dt, lap[0].x, cur[0].x) : (m0 ? cur[0].x : bd);
-                    r.y = act1 ? __fmaf_rn(gi.dt, lap[0].y, cur[0].y) : (m1 ? cur[0].y : bd);
+                    r.x = act0 ? __fmaf_rn(cgi.dt, lap[0].x, cur[0].x) : (m0 ? cur[0].x : bd);
+                    r.y = act1 ? __fmaf_rn(cgi.dt, lap[0].y, cur[0].y) : (m1 ? cur[0].y : bd);
                     *reinterpret_cast<float2*>(d0 + z * 64) = r;
                 } else {
                     float2 un, vn;
-                    gs_update(cur[0].x, cur[NP - 1].x, lap[0].x, lap[NP - 1].x, gi, un.x, vn.x);
-                    gs_update(cur[0].y, cur[NP - 1].y, lap[0].y, lap[NP - 1].y, gi, un.y, vn.y);
+                    gs_update(cur[0].x, cur[NP - 1].x, lap[0].x, lap[NP - 1].x, cgi, un.x, vn.x);
+                    gs_update(cur[0].y, cur[NP - 1].y, lap[0].y, lap[NP - 1].y, cgi, un.y, vn.y);
                     if (act0 && act1) {
                         *reinterpret_cast<float2*>(d0 + z * 64) = un;
                         *reinterpret_cast<float2*>(d1 + z * 64) = vn;
@@ -380,31 +344,39 @@ __global__ void __launch_bounds__(kThreads8, 4)
             }
         }
         __syncwarp();
-        if (lane == 0) {
-            if (has_prev) mbar_arrive(&empty[sm1]);
-            mbar_arrive(&empty[s]);
-            if (has_next) mbar_arrive(&empty[sp1]);
+        if (i > lo && issued < Q) {
+            // chunk q - 1 is no longer read: its slot takes chunk q - 1 + R
+            fence_proxy_async_smem();
+            issue(issued, sp);
+            ++issued;
         }
-        q += kCW;
-        s += kCW;  // S >= kCW: at most one wrap
-        if (s >= S) {
-            s -= S;
-            ph ^= 1u;
-        }
+        sq = sn;
     }
 }
 
 template <int KIND, int NP>
 static int launch_kind(const LaunchDesc& L, const TmapSet& tm, cudaStream_t s) {
-    // ring depth: all kCW consumers busy plus the two halo chunks, within the shared memory of one CTA
-    const size_t per = sizeof(Stage8<NP>) + 16;
-    const int smax = (int)((227u * 1024u) / per);
-    const int S = std::min(std::max(L.stages, kCW + 2), smax);
-    const size_t smem = (size_t)S * per;
+    // ring depth per warp: at least 3 (chunks q - 1, q, q + 1), within one CTA's shared memory; 0 = the
+    // deepest ring (up to 8) with which the requested CTAs per SM stay resident
+    const size_t per = sizeof(Stage8<NP>) + 8;
+    const int rmax = (int)((227u * 1024u) / (per * kWarps));
+    int R = L.stages;
+    if (R <= 0) {
+        const int64_t per_sm = std::max<int64_t>(1, ((int64_t)L.ctas + L.num_sms - 1) / L.num_sms);
+        const int64_t budget = 228 * 1024 / per_sm - 1024;  // 1 KB of every CTA's shared memory is reserved
+        R = (int)std::max<int64_t>(3, std::min<int64_t>(8, budget / (int64_t)(per * kWarps)));
+    }
+    R = std::min(std::max(R, 3), rmax);
+    const size_t smem = (size_t)kWarps * R * per;
+    // warps: CTAs per SM x SMs x kWarps, but at least 4 chunks per warp (each warp also streams its two
+    // neighbour chunks)
+    const int64_t total = (int64_t)L.ctas * kWarps;
+    const int64_t nwarps = std::max<int64_t>(1, std::min<int64_t>(total, L.n / 4));
+    const unsigned blocks = (unsigned)((nwarps + kWarps - 1) / kWarps);
     auto kern = k_stencil7_e8<KIND, NP>;
     SGB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    kern<<<L.ctas, kThreads8, smem, s>>>(L.fs, tm, L.mask, L.nn, L.keys, L.gid, L.grids, L.g0, L.n, L.geo, L.prm, L.t,
-                                         S, L.err);
+    kern<<<blocks, kThreads8, smem, s>>>(L.fs, tm, L.mask, L.nn, L.keys, L.gid, L.grids, L.g0, L.n, L.geo, L.prm, L.t,
+                                         R, nwarps, L.err);
     SGB_CUDA(cudaGetLastError());
     return SGB_OK;
 }
