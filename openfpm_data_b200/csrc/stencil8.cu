@@ -54,24 +54,6 @@ struct alignas(128) Stage8 {
     int32_t par, active;
 };
 
-__device__ __forceinline__ float2 lds_f2(uint32_t a) {
-    float2 v;
-    asm volatile("ld.shared.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "r"(a));
-    return v;
-}
-
-__device__ __forceinline__ float lds_f1(uint32_t a) {
-    float v;
-    asm volatile("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(a));
-    return v;
-}
-
-__device__ __forceinline__ uint32_t lds_u16(uint32_t a) {
-    unsigned short v;
-    asm volatile("ld.shared.u16 %0, [%1];" : "=h"(v) : "r"(a));
-    return v;
-}
-
 // The y faces of a chunk are 8 rows of 32 B, 256 B apart: one 3-D tensor
 // copy each.  A field is viewed as a tensor [chunks*8 (z)][8 (y)][8 (x)] of
 // float, box {8, 1, 8}; the x coordinate is always 0 (16-byte aligned).
@@ -121,7 +103,7 @@ static int encode_yface(CUtensorMap* map, const float* base, int64_t chunks) {
 
 
 
-template <int KIND, int NP>
+template <int KIND, int NP, bool BOX>
 __global__ void __launch_bounds__(kThreads8)
     k_stencil7_e8(FieldSet fs, const __grid_constant__ TmapSet tm, const uint8_t* __restrict__ mask,
                   const int32_t* __restrict__ nn, const int64_t* __restrict__ keys, const int32_t* __restrict__ gid,
@@ -185,7 +167,7 @@ __global__ void __launch_bounds__(kThreads8)
         const int par = (int)((t - gi.start) & 1);
         if (lane < 8) st.nn[lane] = nb_cur;
         if (lane == 0) {
-            if (prm.has_box) {
+            if (BOX) {
                 const int64_t key = keys[c];
                 st.cx = (int32_t)((key % geo.bsz[0]) * 8);
                 st.cy = (int32_t)(((key / geo.bsz[0]) % geo.bsz[1]) * 8);
@@ -209,19 +191,23 @@ __global__ void __launch_bounds__(kThreads8)
             __syncwarp();
             const float* sp0 = par ? fs.in[1][0] : fs.in[0][0];
             const float* sp1 = par ? fs.in[1][NP - 1] : fs.in[0][NP - 1];
-            // per field: own tile, two z faces (contiguous), two y faces (tensor boxes); then the mask tile
+            // per field: own tile, two z faces (contiguous), two y faces (tensor boxes); then the mask tile.
+            // Each lane selects its copy, then one of two copy instructions is issued.
             if (lane < NP * 5 + 1) {
-                if (lane == NP * 5) {
-                    bulk_g2s(st.mt, mask + c * 512, 512, bar);
-                } else {
-                    const int p = lane / 5, r = lane % 5;
-                    const float* src = p == 0 ? sp0 : sp1;
-                    if (r == 0) bulk_g2s(st.tile[p], src + c * 512, 2048, bar);
-                    else if (r == 1) { if (fzm >= 0) bulk_g2s(st.zm[p], src + (int64_t)fzm * 512 + 448, 256, bar); }
-                    else if (r == 2) { if (fzp >= 0) bulk_g2s(st.zp[p], src + (int64_t)fzp * 512, 256, bar); }
-                    else if (r == 3) { if (fym >= 0) tma_yface(st.ym[p], &tm.yface[par][p], 7, fym * 8, bar); }
-                    else { if (fyp >= 0) tma_yface(st.yp[p], &tm.yface[par][p], 0, fyp * 8, bar); }
-                }
+                const int p = lane / 5 < NP ? lane / 5 : NP - 1, r = lane == NP * 5 ? 5 : lane % 5;
+                const float* src = p == 0 ? sp0 : sp1;
+                const int32_t fn = r == 1 ? fzm : r == 2 ? fzp : r == 3 ? fym : r == 4 ? fyp : 0;
+                void* dst = r == 0 ? (void*)st.tile[p] : r == 1 ? (void*)st.zm[p] : r == 2 ? (void*)st.zp[p]
+                          : r == 3 ? (void*)st.ym[p] : r == 4 ? (void*)st.yp[p] : (void*)st.mt;
+                const void* gsrc = r == 0 ? (const void*)(src + c * 512)
+                                 : r == 1 ? (const void*)(src + (int64_t)fzm * 512 + 448)
+                                 : r == 2 ? (const void*)(src + (int64_t)fzp * 512)
+                                          : (const void*)(mask + c * 512);
+                const uint32_t bytes = r == 0 ? 2048u : r == 5 ? 512u : 256u;
+                const bool valid = fn >= 0;
+                const bool tensor = r == 3 || r == 4;
+                if (valid && !tensor) bulk_g2s(dst, gsrc, bytes, bar);
+                if (valid && tensor) tma_yface(dst, &tm.yface[par][p], r == 3 ? 7 : 0, fn * 8, bar);
             }
         } else if (lane == 0) {
             mbar_arrive(bar);
@@ -269,25 +255,30 @@ __global__ void __launch_bounds__(kThreads8)
             const bool xm_ok = n0 >= 0 && n0 == (int32_t)(i - 1), xp_ok = n1 >= 0 && n1 == (int32_t)(i + 1);
             // Shared addresses of the lane's operands at z = 0 and their steps per z.  Absent
             // neighbour chunks read the stage's background pair with step 0.
+            // (byte offsets into the dynamic shared array: plain loads through it stay shared-memory loads
+            // and leave the scheduler free to batch them)
+            auto off = [&](const void* ptr) { return (uint32_t)((const unsigned char*)ptr - smem_raw); };
+            auto ld2 = [&](uint32_t o) { return *reinterpret_cast<const float2*>(smem_raw + o); };
+            auto ld1 = [&](uint32_t o) { return *reinterpret_cast<const float*>(smem_raw + o); };
             uint32_t aC[NP], aYm[NP], aYp[NP], aXm[NP], aXp[NP], aZp[NP];
             float2 zmv[NP], cv[NP];
 #pragma unroll
             for (int p = 0; p < NP; ++p) {
-                const uint32_t bk = smem_u32(&st.bk[p]);
-                aC[p] = smem_u32(&st.tile[p][o0]);
-                aYm[p] = y > 0 ? aC[p] - 32 : (n2 >= 0 ? smem_u32(&st.ym[p][x0]) : bk);
-                aYp[p] = y < 7 ? aC[p] + 32 : (n3 >= 0 ? smem_u32(&st.yp[p][x0]) : bk);
-                aXm[p] = x0 > 0 ? aC[p] - 4 : (xm_ok ? smem_u32(&pv.tile[p][y * 8 + 7]) : bk);
-                aXp[p] = x0 < 6 ? aC[p] + 8 : (xp_ok ? smem_u32(&nx.tile[p][y * 8]) : bk);
-                aZp[p] = n5 >= 0 ? smem_u32(&st.zp[p][o0]) : bk;
-                zmv[p] = lds_f2(n4 >= 0 ? smem_u32(&st.zm[p][o0]) : bk);
-                cv[p] = lds_f2(aC[p]);
+                const uint32_t bk = off(&st.bk[p]);
+                aC[p] = off(&st.tile[p][o0]);
+                aYm[p] = y > 0 ? aC[p] - 32 : (n2 >= 0 ? off(&st.ym[p][x0]) : bk);
+                aYp[p] = y < 7 ? aC[p] + 32 : (n3 >= 0 ? off(&st.yp[p][x0]) : bk);
+                aXm[p] = x0 > 0 ? aC[p] - 4 : (xm_ok ? off(&pv.tile[p][y * 8 + 7]) : bk);
+                aXp[p] = x0 < 6 ? aC[p] + 8 : (xp_ok ? off(&nx.tile[p][y * 8]) : bk);
+                aZp[p] = n5 >= 0 ? off(&st.zp[p][o0]) : bk;
+                zmv[p] = ld2(n4 >= 0 ? off(&st.zm[p][o0]) : bk);
+                cv[p] = ld2(aC[p]);
             }
             const uint32_t sYm = y > 0 ? 256u : (n2 >= 0 ? 32u : 0u);
             const uint32_t sYp = y < 7 ? 256u : (n3 >= 0 ? 32u : 0u);
             const uint32_t sXm = (x0 > 0 || xm_ok) ? 256u : 0u;
             const uint32_t sXp = (x0 < 6 || xp_ok) ? 256u : 0u;
-            const uint32_t aM = smem_u32(&st.mt[o0]);
+            const uint32_t aM = off(&st.mt[o0]);
             const int par = st.par;
             float* d0 = (par ? fs.out[1][0] : fs.out[0][0]) + i * 512 + o0;
             float* d1 = (par ? fs.out[1][NP - 1] : fs.out[0][NP - 1]) + i * 512 + o0;
@@ -296,15 +287,15 @@ __global__ void __launch_bounds__(kThreads8)
             const int32_t bx = st.cx + x0, by = st.cy + y, bz = st.cz;
 #pragma unroll
             for (int z = 0; z < 8; ++z) {
-                const uint32_t m = lds_u16(aM + z * 64);
+                const uint32_t m = *reinterpret_cast<const unsigned short*>(smem_raw + aM + z * 64);
                 float2 lap[NP], cur[NP];
 #pragma unroll
                 for (int p = 0; p < NP; ++p) {
-                    const float2 zp = z < 7 ? lds_f2(aC[p] + (z + 1) * 256) : lds_f2(aZp[p]);
-                    const float2 ym = lds_f2(aYm[p] + z * sYm);
-                    const float2 yp = lds_f2(aYp[p] + z * sYp);
-                    const float xm = lds_f1(aXm[p] + z * sXm);
-                    const float xp = lds_f1(aXp[p] + z * sXp);
+                    const float2 zp = z < 7 ? ld2(aC[p] + (z + 1) * 256) : ld2(aZp[p]);
+                    const float2 ym = ld2(aYm[p] + z * sYm);
+                    const float2 yp = ld2(aYp[p] + z * sYp);
+                    const float xm = ld1(aXm[p] + z * sXm);
+                    const float xp = ld1(aXp[p] + z * sXp);
                     const float2 c = cv[p];
                     lap[p].x = lap7(c.x, xm, c.y, ym.x, yp.x, zmv[p].x, zp.x);
                     lap[p].y = lap7(c.y, c.x, xp, ym.y, yp.y, zmv[p].y, zp.y);
@@ -314,7 +305,7 @@ __global__ void __launch_bounds__(kThreads8)
                 }
                 const uint32_t m0 = m & 0xffu, m1 = m >> 8;
                 bool act0 = (m0 & 3u) == 1u, act1 = (m1 & 3u) == 1u;  // EXIST and not PADDING
-                if (prm.has_box) {
+                if (BOX) {
                     act0 = act0 && in_box(prm, bx, by, bz + z);
                     act1 = act1 && in_box(prm, bx + 1, by, bz + z);
                 }
@@ -327,19 +318,14 @@ __global__ void __launch_bounds__(kThreads8)
                     float2 un, vn;
                     gs_update(cur[0].x, cur[NP - 1].x, lap[0].x, lap[NP - 1].x, cgi, un.x, vn.x);
                     gs_update(cur[0].y, cur[NP - 1].y, lap[0].y, lap[NP - 1].y, cgi, un.y, vn.y);
-                    if (act0 && act1) {
-                        *reinterpret_cast<float2*>(d0 + z * 64) = un;
-                        *reinterpret_cast<float2*>(d1 + z * 64) = vn;
-                    } else {
-                        if (act0) {
-                            d0[z * 64] = un.x;
-                            d1[z * 64] = vn.x;
-                        }
-                        if (act1) {
-                            d0[z * 64 + 1] = un.y;
-                            d1[z * 64 + 1] = vn.y;
-                        }
-                    }
+                    // three independent predicated stores, no branches
+                    const bool both = act0 && act1;
+                    if (both) *reinterpret_cast<float2*>(d0 + z * 64) = un;
+                    if (both) *reinterpret_cast<float2*>(d1 + z * 64) = vn;
+                    if (act0 && !both) d0[z * 64] = un.x;
+                    if (act0 && !both) d1[z * 64] = vn.x;
+                    if (act1 && !both) d0[z * 64 + 1] = un.y;
+                    if (act1 && !both) d1[z * 64 + 1] = vn.y;
                 }
             }
         }
@@ -354,7 +340,7 @@ __global__ void __launch_bounds__(kThreads8)
     }
 }
 
-template <int KIND, int NP>
+template <int KIND, int NP, bool BOX>
 static int launch_kind(const LaunchDesc& L, const TmapSet& tm, cudaStream_t s) {
     // ring depth per warp: at least 3 (chunks q - 1, q, q + 1), within one CTA's shared memory; 0 = the
     // deepest ring (up to 8) with which the requested CTAs per SM stay resident
@@ -373,7 +359,7 @@ static int launch_kind(const LaunchDesc& L, const TmapSet& tm, cudaStream_t s) {
     const int64_t total = (int64_t)L.ctas * kWarps;
     const int64_t nwarps = std::max<int64_t>(1, std::min<int64_t>(total, L.n / 4));
     const unsigned blocks = (unsigned)((nwarps + kWarps - 1) / kWarps);
-    auto kern = k_stencil7_e8<KIND, NP>;
+    auto kern = k_stencil7_e8<KIND, NP, BOX>;
     SGB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     kern<<<blocks, kThreads8, smem, s>>>(L.fs, tm, L.mask, L.nn, L.keys, L.gid, L.grids, L.g0, L.n, L.geo, L.prm, L.t,
                                          R, nwarps, L.err);
@@ -387,8 +373,9 @@ int launch_e8(const LaunchDesc& L, cudaStream_t s) {
     std::memset(&tm, 0, sizeof(tm));
     for (int b = 0; b < 2; ++b)
         for (int p = 0; p < np; ++p) SGB_TRY(encode_yface(&tm.yface[b][p], L.fs.in[b][p], L.arr_chunks));
-    if (L.kind == SGB_GS7) return launch_kind<SGB_GS7, 2>(L, tm, s);
-    return launch_kind<SGB_HEAT7, 1>(L, tm, s);
+    const bool box = L.prm.has_box != 0;
+    if (L.kind == SGB_GS7) return box ? launch_kind<SGB_GS7, 2, true>(L, tm, s) : launch_kind<SGB_GS7, 2, false>(L, tm, s);
+    return box ? launch_kind<SGB_HEAT7, 1, true>(L, tm, s) : launch_kind<SGB_HEAT7, 1, false>(L, tm, s);
 }
 
 }  // namespace sgb
