@@ -233,7 +233,7 @@ int sgb_check_device_errors(sgb_grid* g, sgb_stream s);
 /* Bytes of device memory held by the grid. */
 int sgb_device_bytes(const sgb_grid* g, int64_t* bytes);
 
-/* Stencil launch configuration of the 8^3 kernel: CTAs per SM (1..8, two
+/* Stencil launch configuration of the 8^3 kernel: CTAs per SM (1..16, two
  * warps each, every warp its own pipeline) and the staging ring depth per
  * warp (3..16 chunks, at most what fits in one CTA's shared memory, or -1
  * for the automatic depth: the deepest ring, up to 8, with which the

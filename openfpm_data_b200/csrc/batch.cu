@@ -195,7 +195,7 @@ int sgb_batch_destroy(sgb_batch* b) {
 }
 
 int sgb_batch_set_launch_config(sgb_batch* b, int ctas_per_sm, int stages) {
-    if (!b || ctas_per_sm < 0 || ctas_per_sm > 8 || stages < -1 || (stages > 0 && (stages < 3 || stages > 16)))
+    if (!b || ctas_per_sm < 0 || ctas_per_sm > 16 || stages < -1 || (stages > 0 && (stages < 3 || stages > 16)))
         return SGB_EINVAL;
     if (ctas_per_sm) b->ctas_per_sm = ctas_per_sm;
     if (stages) b->stages = stages < 0 ? 0 : stages;  // -1: automatic depth

@@ -8,27 +8,28 @@
 // Here every warp is an independent pipeline over a contiguous range [a, b)
 // of chunk positions.  It streams [lo, hi), the range widened by one chunk on
 // each side, through its own R-stage shared-memory ring: per chunk, lanes
-// issue 1-D bulk copies (cp.async.bulk) of the source tiles (2 KB per field),
-// the mask tile (512 B) and the two z faces (256 B each), and 3-D TMA tensor
-// copies of the two y faces (8 rows of 32 B), counted in bytes on the stage's
+// issue 1-D bulk copies (cp.async.bulk, the TMA engine) of the source tiles
+// (2 KB per field) and the mask tile (512 B), counted in bytes on the stage's
 // mbarrier.  The x halo is not fetched: an existing -x / +x neighbour is
 // always the previous / next position of the sorted index, so it sits in the
-// neighbouring stage of the same ring.  While chunk q is computed, chunks up
-// to q - 2 + R are in flight; after it, the stage of chunk q - 1 is refilled
-// with chunk q - 1 + R.  A warp waits only on its own barriers, in order, so
-// phase parities are exact and no warp ever waits for another.
+// neighbouring stage of the same ring.  The y and z faces (256 B each per
+// field) go to registers instead of shared memory, loaded one chunk ahead:
+// a z face is one 8-byte load per lane (the lane's own x pair), a y face one
+// 8-byte load per lane spread over the lanes ([z][x pair]) and handed to the
+// y = 0 / y = 7 lanes by a shuffle at each z.  Keeping faces out of the ring
+// makes a stage 2.6 KB (heat) / 4.6 KB (Gray-Scott), so more warps fit on an
+// SM.  While chunk q is computed, chunks up to q - 2 + R are in flight; after
+// it, the stage of chunk q - 1 is refilled with chunk q - 1 + R.  A warp
+// waits only on its own barriers, in order, so phase parities are exact and
+// no warp ever waits for another.
 //
 // Compute: each lane owns a pair of x-adjacent points of one y row and
-// marches z = 0..7, carrying the z-1 / z / z+1 values in registers, so a
-// point pair costs five shared loads per field.
+// marches z = 0..7, carrying the z-1 / z / z+1 values in registers.
 //
 // Points with mask byte 0 hold the background value in HBM (grid.cu keeps
 // that invariant per property, see sgb_grid::clean), so a neighbour value is
 // read as stored; the background is substituted only for neighbour chunks
 // that do not exist.  Arithmetic is that of stencil.cuh.
-#include <cuda.h>
-#include <cudaTypedefs.h>
-
 #include <algorithm>
 #include <cstring>
 
@@ -44,69 +45,86 @@ constexpr int kThreads8 = kWarps * 32;
 template <int NP>
 struct alignas(128) Stage8 {
     float tile[NP][512];
-    float ym[NP][64], yp[NP][64];  // [z*8 + x]: y = 7 row of the -y chunk / y = 0 row of the +y chunk
-    float zm[NP][64], zp[NP][64];  // [y*8 + x]: z = 7 slice of the -z chunk / z = 0 slice of the +z chunk
     uint8_t mt[512];
     GridInfo gi;
-    float2 bk[NP];       // background of each source field, twice (read in place of absent faces)
+    float2 bk[NP];       // background of each source field, twice (read for absent x neighbours)
     int32_t nn[8];
     int32_t cx, cy, cz;  // first point of the chunk (box tests)
     int32_t par, active;
 };
 
-// The y faces of a chunk are 8 rows of 32 B, 256 B apart: one 3-D tensor
-// copy each.  A field is viewed as a tensor [chunks*8 (z)][8 (y)][8 (x)] of
-// float, box {8, 1, 8}; the x coordinate is always 0 (16-byte aligned).
-struct TmapSet {
-    CUtensorMap yface[2][2];  // [ping-pong buffer][field]
+// y and z faces of one chunk in registers (see the file comment)
+template <int NP>
+struct Faces {
+    float2 zm[NP], zp[NP];  // the lane's own x pair in the z = 7 / z = 0 slices of the -z / +z chunks
+    float2 ym[NP], yp[NP];  // [z = lane / 4][x pair = lane % 4] of the y = 7 / y = 0 rows of the -y / +y chunks
 };
 
-__device__ __forceinline__ void tma_yface(void* dst, const CUtensorMap* map, int y, int z, uint64_t* bar) {
-    asm volatile(
-        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
-        "[%5];" ::"r"(smem_u32(dst)),
-        "l"(reinterpret_cast<uint64_t>(map)), "r"(0), "r"(y), "r"(z), "r"(smem_u32(bar))
-        : "memory");
+__device__ __forceinline__ float2 ldg_f2(const float* p) {
+    return __ldg(reinterpret_cast<const float2*>(p));
 }
 
-static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
-    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-    if (!fn) {
-        void* p = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
-            q == cudaDriverEntryPointSuccess)
-            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
-    }
-    return fn;
+// Packed FP32 pair arithmetic (sm_100: one instruction per x pair).  Each
+// element is rounded exactly like the scalar add.rn.ftz / mul.rn.ftz /
+// fma.rn.ftz it replaces.  Unlike the scalar forms, a packed mul.rn followed
+// by a packed add.rn is contracted into one fma by the assembler (measured:
+// 27% of Laplacians off by one ulp), so no packed product may feed a packed
+// sum: the Laplacian below builds -6c from exact doublings instead.
+__device__ __forceinline__ float2 add2(float2 a, float2 b) {
+    float2 r;
+    asm("{\n\t.reg .b64 ra, rb, rd;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+        "add.rn.ftz.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;\n\t}"
+        : "=f"(r.x), "=f"(r.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return r;
 }
 
-static int encode_yface(CUtensorMap* map, const float* base, int64_t chunks) {
-    auto enc = tensor_map_encoder();
-    if (!enc) {
-        set_error("cuTensorMapEncodeTiled is not available from the driver");
-        return SGB_ECUDA;
-    }
-    const cuuint64_t dims[3] = {8, 8, (cuuint64_t)std::max<int64_t>(chunks, 1) * 8};
-    const cuuint64_t strides[2] = {8 * sizeof(float), 64 * sizeof(float)};
-    const cuuint32_t box[3] = {8, 1, 8};
-    const cuuint32_t estr[3] = {1, 1, 1};
-    CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(base), dims, strides, box, estr,
-                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    if (r != CUDA_SUCCESS) {
-        set_error("cuTensorMapEncodeTiled failed");
-        return SGB_ECUDA;
-    }
-    return SGB_OK;
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) {
+    float2 r;
+    asm("{\n\t.reg .b64 ra, rb, rd;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+        "mul.rn.ftz.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;\n\t}"
+        : "=f"(r.x), "=f"(r.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return r;
 }
 
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) {
+    float2 r;
+    asm("{\n\t.reg .b64 ra, rb, rc, rd;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\tmov.b64 rc, {%6, %7};\n\t"
+        "fma.rn.ftz.f32x2 rd, ra, rb, rc;\n\tmov.b64 {%0, %1}, rd;\n\t}"
+        : "=f"(r.x), "=f"(r.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(c.x), "f"(c.y));
+    return r;
+}
 
+__device__ __forceinline__ float2 dup2(float v) { return make_float2(v, v); }
+
+// lap7 of stencil.cuh for the lane's x pair (c.x at x0, c.y at x0 + 1):
+// (((-6 c) + (xm + xp)) + (ym + yp)) + (zm + zp), with xm/xp of c.x being
+// (xm, c.y) and of c.y being (c.x, xp).
+__device__ __forceinline__ float2 lap7_pair(float2 c, float xm, float xp, float2 ym, float2 yp, float2 zm,
+                                           float2 zp) {
+    // -6c rounded once, as __fmul_rn(-6, c): 2c and 4c are exact, 4c + 2c = 6c rounds once
+    const float2 c2 = add2(c, c), c4 = add2(c2, c2), c6 = add2(c4, c2);
+    float2 l = make_float2(-c6.x, -c6.y);
+    l = add2(l, add2(make_float2(xm, c.x), make_float2(c.y, xp)));
+    l = add2(l, add2(ym, yp));
+    return add2(l, add2(zm, zp));
+}
+
+// gs_update of stencil.cuh for an x pair
+__device__ __forceinline__ void gs_update_pair(float2 u, float2 v, float2 lu, float2 lv, const GridInfo& p,
+                                               float2& un, float2& vn) {
+    const float2 uvv = mul2(mul2(u, v), v);
+    float2 du = fma2(dup2(p.Du), lu, make_float2(-uvv.x, -uvv.y));
+    du = fma2(dup2(p.F), add2(dup2(1.0f), make_float2(-u.x, -u.y)), du);  // 1 - u == 1 + (-u) exactly
+    float2 dv = fma2(dup2(p.Dv), lv, uvv);
+    dv = fma2(dup2(p.nFK), v, dv);
+    un = fma2(dup2(p.dt), du, u);
+    vn = fma2(dup2(p.dt), dv, v);
+}
 
 template <int KIND, int NP, bool BOX>
-__global__ void __launch_bounds__(kThreads8)
-    k_stencil7_e8(FieldSet fs, const __grid_constant__ TmapSet tm, const uint8_t* __restrict__ mask,
-                  const int32_t* __restrict__ nn, const int64_t* __restrict__ keys, const int32_t* __restrict__ gid,
+__global__ void __launch_bounds__(kThreads8, 8)
+    k_stencil7_e8(FieldSet fs, const uint8_t* __restrict__ mask, const int32_t* __restrict__ nn,
+                  const int64_t* __restrict__ keys, const int32_t* __restrict__ gid,
                   const GridInfo* __restrict__ grids, GridInfo g0, int64_t n, Geometry geo, StencilParams prm,
                   int64_t t, int R, int64_t nwarps, unsigned* err) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -182,32 +200,16 @@ __global__ void __launch_bounds__(kThreads8)
             st.par = par;
             st.active = active;
         }
-        const int32_t fzm = __shfl_sync(0xffffffffu, nb_cur, 4), fzp = __shfl_sync(0xffffffffu, nb_cur, 5);
-        const int32_t fym = __shfl_sync(0xffffffffu, nb_cur, 2), fyp = __shfl_sync(0xffffffffu, nb_cur, 3);
         __syncwarp();
         if (active) {
-            const uint32_t faces = (fym >= 0) + (fyp >= 0) + (fzm >= 0) + (fzp >= 0);
-            if (lane == 0) mbar_arrive_expect_tx(bar, NP * (2048 + 256 * faces) + 512);
+            if (lane == 0) mbar_arrive_expect_tx(bar, NP * 2048 + 512);
             __syncwarp();
-            const float* sp0 = par ? fs.in[1][0] : fs.in[0][0];
-            const float* sp1 = par ? fs.in[1][NP - 1] : fs.in[0][NP - 1];
-            // per field: own tile, two z faces (contiguous), two y faces (tensor boxes); then the mask tile.
-            // Each lane selects its copy, then one of two copy instructions is issued.
-            if (lane < NP * 5 + 1) {
-                const int p = lane / 5 < NP ? lane / 5 : NP - 1, r = lane == NP * 5 ? 5 : lane % 5;
-                const float* src = p == 0 ? sp0 : sp1;
-                const int32_t fn = r == 1 ? fzm : r == 2 ? fzp : r == 3 ? fym : r == 4 ? fyp : 0;
-                void* dst = r == 0 ? (void*)st.tile[p] : r == 1 ? (void*)st.zm[p] : r == 2 ? (void*)st.zp[p]
-                          : r == 3 ? (void*)st.ym[p] : r == 4 ? (void*)st.yp[p] : (void*)st.mt;
-                const void* gsrc = r == 0 ? (const void*)(src + c * 512)
-                                 : r == 1 ? (const void*)(src + (int64_t)fzm * 512 + 448)
-                                 : r == 2 ? (const void*)(src + (int64_t)fzp * 512)
-                                          : (const void*)(mask + c * 512);
-                const uint32_t bytes = r == 0 ? 2048u : r == 5 ? 512u : 256u;
-                const bool valid = fn >= 0;
-                const bool tensor = r == 3 || r == 4;
-                if (valid && !tensor) bulk_g2s(dst, gsrc, bytes, bar);
-                if (valid && tensor) tma_yface(dst, &tm.yface[par][p], r == 3 ? 7 : 0, fn * 8, bar);
+            // lanes 0..NP-1: the field tiles; lane NP: the mask tile
+            if (lane <= NP) {
+                const float* src = (lane == 0) ? (par ? fs.in[1][0] : fs.in[0][0])
+                                               : (par ? fs.in[1][NP - 1] : fs.in[0][NP - 1]);
+                if (lane < NP) bulk_g2s(st.tile[lane], src + c * 512, 2048, bar);
+                else bulk_g2s(st.mt, mask + c * 512, 512, bar);
             }
         } else if (lane == 0) {
             mbar_arrive(bar);
@@ -221,11 +223,31 @@ __global__ void __launch_bounds__(kThreads8)
     // ------------------------------------------------------------ compute side
     const int y = lane >> 2, x0 = (lane & 3) << 1;
     const int o0 = y * 8 + x0;  // the lane's first point in a z slice
+    const int yo = (lane >> 2) * 64 + ((lane & 3) << 1);  // this lane's element of a y face: z = lane / 4
+    // faces of the chunk held in ring slot `slot` (its metadata are written at issue time)
+    auto load_faces = [&](const Stage8<NP>& st, Faces<NP>& f) {
+        const int par = st.par;
+        const int32_t fym = st.nn[2], fyp = st.nn[3], fzm = st.nn[4], fzp = st.nn[5];
+#pragma unroll
+        for (int p = 0; p < NP; ++p) {
+            const float* src = p == 0 ? (par ? fs.in[1][0] : fs.in[0][0]) : (par ? fs.in[1][NP - 1] : fs.in[0][NP - 1]);
+            const float2 bk = st.bk[p];
+            f.zm[p] = fzm >= 0 ? ldg_f2(src + (int64_t)fzm * 512 + 448 + o0) : bk;
+            f.zp[p] = fzp >= 0 ? ldg_f2(src + (int64_t)fzp * 512 + o0) : bk;
+            f.ym[p] = fym >= 0 ? ldg_f2(src + (int64_t)fym * 512 + 56 + yo) : bk;
+            f.yp[p] = fyp >= 0 ? ldg_f2(src + (int64_t)fyp * 512 + yo) : bk;
+        }
+    };
     int waited = 0, ws = 0;     // chunks [0, waited) have landed; ws = slot of chunk `waited`
     uint32_t wph = 0;           // phase parity of slot ws for chunk `waited`
     int q = (int)(a - lo);
     int sq = q;                 // slot of chunk q (q < R)
+    Faces<NP> fc, fn;           // faces of the chunk being computed / of the next one
+    load_faces(ring[sq], fn);
     for (int64_t i = a; i < b; ++i, ++q) {
+        const int sp = sq == 0 ? R - 1 : sq - 1, sn = sq + 1 == R ? 0 : sq + 1;
+        fc = fn;
+        if (i + 1 < b) load_faces(ring[sn], fn);  // one chunk ahead; chunk q + 1's metadata are in slot sn
         const int need = i + 1 < hi ? q + 1 : q;
         bool ok = true;
         while (waited <= need) {
@@ -245,37 +267,29 @@ __global__ void __launch_bounds__(kThreads8)
                 mbar_wait_bounded(&full[r % R], (uint32_t)(r / R) & 1u, err, 100000000ull);
             return;
         }
-        const int sp = sq == 0 ? R - 1 : sq - 1, sn = sq + 1 == R ? 0 : sq + 1;
         const Stage8<NP>& st = ring[sq];
         if (st.active) {
             const Stage8<NP>& pv = ring[sp];
             const Stage8<NP>& nx = ring[sn];
-            const int32_t n0 = st.nn[0], n1 = st.nn[1], n2 = st.nn[2], n3 = st.nn[3], n4 = st.nn[4], n5 = st.nn[5];
+            const int32_t n0 = st.nn[0], n1 = st.nn[1];
             // an absent neighbour is -1, which must not match position i - 1 of chunk 0
             const bool xm_ok = n0 >= 0 && n0 == (int32_t)(i - 1), xp_ok = n1 >= 0 && n1 == (int32_t)(i + 1);
-            // Shared addresses of the lane's operands at z = 0 and their steps per z.  Absent
-            // neighbour chunks read the stage's background pair with step 0.
             // (byte offsets into the dynamic shared array: plain loads through it stay shared-memory loads
             // and leave the scheduler free to batch them)
             auto off = [&](const void* ptr) { return (uint32_t)((const unsigned char*)ptr - smem_raw); };
             auto ld2 = [&](uint32_t o) { return *reinterpret_cast<const float2*>(smem_raw + o); };
             auto ld1 = [&](uint32_t o) { return *reinterpret_cast<const float*>(smem_raw + o); };
-            uint32_t aC[NP], aYm[NP], aYp[NP], aXm[NP], aXp[NP], aZp[NP];
+            uint32_t aC[NP], aXm[NP], aXp[NP];
             float2 zmv[NP], cv[NP];
 #pragma unroll
             for (int p = 0; p < NP; ++p) {
                 const uint32_t bk = off(&st.bk[p]);
                 aC[p] = off(&st.tile[p][o0]);
-                aYm[p] = y > 0 ? aC[p] - 32 : (n2 >= 0 ? off(&st.ym[p][x0]) : bk);
-                aYp[p] = y < 7 ? aC[p] + 32 : (n3 >= 0 ? off(&st.yp[p][x0]) : bk);
                 aXm[p] = x0 > 0 ? aC[p] - 4 : (xm_ok ? off(&pv.tile[p][y * 8 + 7]) : bk);
                 aXp[p] = x0 < 6 ? aC[p] + 8 : (xp_ok ? off(&nx.tile[p][y * 8]) : bk);
-                aZp[p] = n5 >= 0 ? off(&st.zp[p][o0]) : bk;
-                zmv[p] = ld2(n4 >= 0 ? off(&st.zm[p][o0]) : bk);
+                zmv[p] = fc.zm[p];
                 cv[p] = ld2(aC[p]);
             }
-            const uint32_t sYm = y > 0 ? 256u : (n2 >= 0 ? 32u : 0u);
-            const uint32_t sYp = y < 7 ? 256u : (n3 >= 0 ? 32u : 0u);
             const uint32_t sXm = (x0 > 0 || xm_ok) ? 256u : 0u;
             const uint32_t sXp = (x0 < 6 || xp_ok) ? 256u : 0u;
             const uint32_t aM = off(&st.mt[o0]);
@@ -283,7 +297,8 @@ __global__ void __launch_bounds__(kThreads8)
             float* d0 = (par ? fs.out[1][0] : fs.out[0][0]) + i * 512 + o0;
             float* d1 = (par ? fs.out[1][NP - 1] : fs.out[0][NP - 1]) + i * 512 + o0;
             const GridInfo cgi = st.gi;
-            const float bd = st.gi.bck[par ^ 1][0];  // HEAT7: background of the destination
+            const float bd = st.gi.bck[par ^ 1][0];  // backgrounds of the destination fields
+            const float bd0 = bd, bd1 = st.gi.bck[par ^ 1][NP - 1];
             const int32_t bx = st.cx + x0, by = st.cy + y, bz = st.cz;
 #pragma unroll
             for (int z = 0; z < 8; ++z) {
@@ -291,14 +306,19 @@ __global__ void __launch_bounds__(kThreads8)
                 float2 lap[NP], cur[NP];
 #pragma unroll
                 for (int p = 0; p < NP; ++p) {
-                    const float2 zp = z < 7 ? ld2(aC[p] + (z + 1) * 256) : ld2(aZp[p]);
-                    const float2 ym = ld2(aYm[p] + z * sYm);
-                    const float2 yp = ld2(aYp[p] + z * sYp);
+                    // y faces: row z of the face sits in lanes 4z .. 4z+3, one x pair each
+                    const int srcl = z * 4 + (lane & 3);
+                    const float2 fym = make_float2(__shfl_sync(0xffffffffu, fc.ym[p].x, srcl),
+                                                   __shfl_sync(0xffffffffu, fc.ym[p].y, srcl));
+                    const float2 fyp = make_float2(__shfl_sync(0xffffffffu, fc.yp[p].x, srcl),
+                                                   __shfl_sync(0xffffffffu, fc.yp[p].y, srcl));
+                    const float2 zp = z < 7 ? ld2(aC[p] + (z + 1) * 256) : fc.zp[p];
+                    const float2 ym = y > 0 ? ld2(aC[p] + z * 256 - 32) : fym;
+                    const float2 yp = y < 7 ? ld2(aC[p] + z * 256 + 32) : fyp;
                     const float xm = ld1(aXm[p] + z * sXm);
                     const float xp = ld1(aXp[p] + z * sXp);
                     const float2 c = cv[p];
-                    lap[p].x = lap7(c.x, xm, c.y, ym.x, yp.x, zmv[p].x, zp.x);
-                    lap[p].y = lap7(c.y, c.x, xp, ym.y, yp.y, zmv[p].y, zp.y);
+                    lap[p] = lap7_pair(c, xm, xp, ym, yp, zmv[p], zp);
                     cur[p] = c;
                     zmv[p] = c;
                     cv[p] = zp;
@@ -310,16 +330,24 @@ __global__ void __launch_bounds__(kThreads8)
                     act1 = act1 && in_box(prm, bx + 1, by, bz + z);
                 }
                 if (KIND == SGB_HEAT7) {
+                    const float2 h = fma2(dup2(cgi.dt), lap[0], cur[0]);
                     float2 r;
-                    r.x = act0 ? __fmaf_rn(cgi.dt, lap[0].x, cur[0].x) : (m0 ? cur[0].x : bd);
-                    r.y = act1 ? __fmaf_rn(cgi.dt, lap[0].y, cur[0].y) : (m1 ? cur[0].y : bd);
+                    r.x = act0 ? h.x : (m0 ? cur[0].x : bd);
+                    r.y = act1 ? h.y : (m1 ? cur[0].y : bd);
                     *reinterpret_cast<float2*>(d0 + z * 64) = r;
                 } else {
                     float2 un, vn;
-                    gs_update(cur[0].x, cur[NP - 1].x, lap[0].x, lap[NP - 1].x, cgi, un.x, vn.x);
-                    gs_update(cur[0].y, cur[NP - 1].y, lap[0].y, lap[NP - 1].y, cgi, un.y, vn.y);
-                    // three independent predicated stores, no branches
-                    const bool both = act0 && act1;
+                    gs_update_pair(cur[0], cur[NP - 1], lap[0], lap[NP - 1], cgi, un, vn);
+                    // Active points take the update.  Points that do not exist take the destination's
+                    // background, which they hold already (the background invariant), so the pair is
+                    // written whole with one vector store; only existing inactive points (padding,
+                    // outside the box) keep their value, with scalar stores.
+                    const bool w0 = act0 || m0 == 0, w1 = act1 || m1 == 0;
+                    un.x = act0 ? un.x : bd0;
+                    vn.x = act0 ? vn.x : bd1;
+                    un.y = act1 ? un.y : bd0;
+                    vn.y = act1 ? vn.y : bd1;
+                    const bool both = w0 && w1;
                     if (both) *reinterpret_cast<float2*>(d0 + z * 64) = un;
                     if (both) *reinterpret_cast<float2*>(d1 + z * 64) = vn;
                     if (act0 && !both) d0[z * 64] = un.x;
@@ -341,7 +369,7 @@ __global__ void __launch_bounds__(kThreads8)
 }
 
 template <int KIND, int NP, bool BOX>
-static int launch_kind(const LaunchDesc& L, const TmapSet& tm, cudaStream_t s) {
+static int launch_kind(const LaunchDesc& L, cudaStream_t s) {
     // ring depth per warp: at least 3 (chunks q - 1, q, q + 1), within one CTA's shared memory; 0 = the
     // deepest ring (up to 8) with which the requested CTAs per SM stay resident
     const size_t per = sizeof(Stage8<NP>) + 8;
@@ -361,21 +389,16 @@ static int launch_kind(const LaunchDesc& L, const TmapSet& tm, cudaStream_t s) {
     const unsigned blocks = (unsigned)((nwarps + kWarps - 1) / kWarps);
     auto kern = k_stencil7_e8<KIND, NP, BOX>;
     SGB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    kern<<<blocks, kThreads8, smem, s>>>(L.fs, tm, L.mask, L.nn, L.keys, L.gid, L.grids, L.g0, L.n, L.geo, L.prm, L.t,
-                                         R, nwarps, L.err);
+    kern<<<blocks, kThreads8, smem, s>>>(L.fs, L.mask, L.nn, L.keys, L.gid, L.grids, L.g0, L.n, L.geo, L.prm, L.t, R,
+                                         nwarps, L.err);
     SGB_CUDA(cudaGetLastError());
     return SGB_OK;
 }
 
 int launch_e8(const LaunchDesc& L, cudaStream_t s) {
-    const int np = L.kind == SGB_GS7 ? 2 : 1;
-    TmapSet tm;
-    std::memset(&tm, 0, sizeof(tm));
-    for (int b = 0; b < 2; ++b)
-        for (int p = 0; p < np; ++p) SGB_TRY(encode_yface(&tm.yface[b][p], L.fs.in[b][p], L.arr_chunks));
     const bool box = L.prm.has_box != 0;
-    if (L.kind == SGB_GS7) return box ? launch_kind<SGB_GS7, 2, true>(L, tm, s) : launch_kind<SGB_GS7, 2, false>(L, tm, s);
-    return box ? launch_kind<SGB_HEAT7, 1, true>(L, tm, s) : launch_kind<SGB_HEAT7, 1, false>(L, tm, s);
+    if (L.kind == SGB_GS7) return box ? launch_kind<SGB_GS7, 2, true>(L, s) : launch_kind<SGB_GS7, 2, false>(L, s);
+    return box ? launch_kind<SGB_HEAT7, 1, true>(L, s) : launch_kind<SGB_HEAT7, 1, false>(L, s);
 }
 
 }  // namespace sgb

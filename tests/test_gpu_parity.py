@@ -234,6 +234,35 @@ def test_heat_pipelined_equals_tiled(sgb):
     assert np.array_equal(a[1][0], b[1][0]) and np.array_equal(a[1][1], b[1][1])
 
 
+@pytest.mark.parametrize("box", [None, ((5, 9, 13), (60, 70, 50))])
+def test_gray_scott_pipelined_equals_tiled(sgb, box):
+    """The pipelined 8^3 kernel and the one-chunk-per-CTA kernel give the same
+    bits everywhere, existing points and the background-filled rest alike,
+    with padding points (tagBoundaries) and a box leaving existing points
+    untouched."""
+    rng = np.random.default_rng(5)
+    g1, _, _ = _sparse_grid(sgb, rng, (96, 80, 72), 8, 60000, ptypes=(O.T_F32,) * 4)
+    keys, data, mask = g1.deviceToHost()
+    g2 = sgb.SparseGridGpu((96, 80, 72), ["f32"] * 4, edge=8)
+    for g in (g1, g2):
+        for p, b in enumerate([1.0, 0.0, 0.5, 0.25]):
+            g.setBackgroundValue(p, b)
+    n = len(keys)
+    g1.load_map(keys, [d[: n * 512] for d in data], mask[: n * 512])
+    g2.load_map(keys, [d[: n * 512] for d in data], mask[: n * 512])
+    g1.tagBoundaries()
+    g2.tagBoundaries()
+    prm = [W.GS_PARAMS[k] for k in ("Du", "Dv", "F", "k", "dt")]
+    for k in range(5):
+        a, b = ([0, 1], [2, 3]) if k % 2 == 0 else ([2, 3], [0, 1])
+        g1.applyStencils(sgb.GS7, a, b, prm, box=box)
+        g2.applyStencils(sgb.GS7, a, b, prm, box=box, tiled=True)
+    x, y = g1.deviceToHost(), g2.deviceToHost()
+    for p in range(4):
+        assert np.array_equal(x[1][p].view(np.uint32), y[1][p].view(np.uint32)), f"property {p}"
+    g1.check_device_errors()
+
+
 def _small_gs(size=96, nballs=6, seed=9):
     return W.gray_scott(size=size, nballs=nballs, rmin=8.0, rmax=20.0, seed=seed)
 
