@@ -43,7 +43,7 @@ METRIC = "stencil Gpts/s (Gray-Scott 7-point, 512^3 sparse grid)"
 UNIT = "Gpts/s"
 ALG_BYTES_PER_PT = 17
 # the library's default launch configuration of the pipelined 8^3 kernel (automatic ring depth)
-DEFAULT_CTAS_PER_SM, DEFAULT_STAGES = 4, "auto"
+DEFAULT_CTAS_PER_SM, DEFAULT_STAGES = "auto", "auto"
 WORKLOADS = ("gs512", "heat128", "insert1024", "batched256", "served")
 
 
@@ -55,7 +55,7 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--e2e-solves", type=int, default=3)
     ap.add_argument("--solve-steps", type=int, default=1000)
-    ap.add_argument("--cpu-steps", type=int, default=10)
+    ap.add_argument("--cpu-steps", type=int, default=400, help="cap of the CPU baseline sample (about 25 s)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ctas-per-sm", type=int, default=0)
     ap.add_argument("--stages", type=int, default=0)

@@ -234,11 +234,11 @@ int sgb_check_device_errors(sgb_grid* g, sgb_stream s);
 int sgb_device_bytes(const sgb_grid* g, int64_t* bytes);
 
 /* Stencil launch configuration of the 8^3 kernel: CTAs per SM (1..16, two
- * warps each, every warp its own pipeline) and the staging ring depth per
- * warp (3..16 chunks, at most what fits in one CTA's shared memory, or -1
- * for the automatic depth: the deepest ring, up to 8, with which the
- * requested CTAs per SM stay resident; the default); 0 keeps the current
- * value. */
+ * warps each, every warp its own pipeline; -1 for the automatic choice per
+ * stencil kind, the default) and the staging ring depth per warp (3..16
+ * chunks, at most what fits in one CTA's shared memory, or -1 for the
+ * automatic depth: the deepest ring, up to 8, with which the CTAs per SM stay
+ * resident; the default); 0 keeps the current value. */
 int sgb_set_launch_config(sgb_grid* g, int ctas_per_sm, int stages);
 
 /* ---------------------------------------------------------------- batches

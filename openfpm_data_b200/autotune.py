@@ -2,7 +2,8 @@
 
 Candidates: chunk edge 8 (pipelined kernel: one 32-thread warp per
 512-point chunk, each warp with its own staging ring, 2-6 CTAs of two warps
-per SM, ring depth 3, 5 or the automatic depth -1) and chunk edge 4
+per SM or the automatic choice -1, ring depth 3, 4 or the automatic depth
+-1) and chunk edge 4
 (one-chunk-per-CTA tile kernel: 256 threads per 64-point chunk).  Each
 candidate runs a few timed batch steps (CUDA events) on a sample of the
 grids, rebuilt with its chunk edge; the fastest per active point wins.
@@ -72,7 +73,7 @@ def _time_steps(b: Batch, steps: int) -> float:
 
 
 def autotune(specs: Sequence[Spec], kind: int, params, steps: int = 10, device: int = 0,
-             ctas=(2, 4, 6), stages=(-1, 3, 5), edges=(8, 4)) -> TuneResult:
+             ctas=(-1, 4, 6, 8), stages=(-1, 3, 4), edges=(8, 4)) -> TuneResult:
     table = []
     best = None
     for ce in edges:
@@ -90,5 +91,5 @@ def autotune(specs: Sequence[Spec], kind: int, params, steps: int = 10, device: 
             if best is None or nsps < best["ns_per_point_step"]:
                 best = row
         b.close()
-    return TuneResult(best["chunk_edge"], best["ctas_per_sm"] or 4, best["stages"], best["threads_per_chunk"],
+    return TuneResult(best["chunk_edge"], best["ctas_per_sm"], best["stages"], best["threads_per_chunk"],
                       best["ns_per_point_step"], table)

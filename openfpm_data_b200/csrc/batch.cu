@@ -36,7 +36,7 @@ struct sgb_batch {
     int64_t T = 0;
     bool dirty = true;     // grids table must be uploaded
     bool holes = false;    // removed slots to compact
-    int num_sms = 148, ctas_per_sm = 4, stages = 0;
+    int num_sms = 148, ctas_per_sm = 0, stages = 0;  // 0: automatic
     sgb::DevBuf err;
 };
 
@@ -139,7 +139,8 @@ static int batch_launch(sgb_batch* b, int64_t t, cudaStream_t s) {
     L.use_tile = 0;
     L.stages = b->stages;
     L.num_sms = b->num_sms;
-    L.ctas = (unsigned)std::max<int64_t>(1, std::min<int64_t>(b->n, (int64_t)b->num_sms * b->ctas_per_sm));
+    const int cps = b->ctas_per_sm > 0 ? b->ctas_per_sm : auto_ctas_per_sm(b->kind);
+    L.ctas = (unsigned)std::max<int64_t>(1, std::min<int64_t>(b->n, (int64_t)b->num_sms * cps));
     for (int k = 0; k < 2; ++k)
         for (int j = 0; j < 2; ++j) {
             const int p = j < b->np ? j : 0;
@@ -195,9 +196,9 @@ int sgb_batch_destroy(sgb_batch* b) {
 }
 
 int sgb_batch_set_launch_config(sgb_batch* b, int ctas_per_sm, int stages) {
-    if (!b || ctas_per_sm < 0 || ctas_per_sm > 16 || stages < -1 || (stages > 0 && (stages < 3 || stages > 16)))
+    if (!b || ctas_per_sm < -1 || ctas_per_sm > 16 || stages < -1 || (stages > 0 && (stages < 3 || stages > 16)))
         return SGB_EINVAL;
-    if (ctas_per_sm) b->ctas_per_sm = ctas_per_sm;
+    if (ctas_per_sm) b->ctas_per_sm = ctas_per_sm < 0 ? 0 : ctas_per_sm;  // -1: automatic
     if (stages) b->stages = stages < 0 ? 0 : stages;  // -1: automatic depth
     return SGB_OK;
 }

@@ -690,9 +690,9 @@ int sgb_device_bytes(const sgb_grid* g, int64_t* bytes) {
 }
 
 int sgb_set_launch_config(sgb_grid* g, int ctas_per_sm, int stages) {
-    if (!g || ctas_per_sm < 0 || ctas_per_sm > 16 || stages < -1 || (stages > 0 && (stages < 3 || stages > 16)))
+    if (!g || ctas_per_sm < -1 || ctas_per_sm > 16 || stages < -1 || (stages > 0 && (stages < 3 || stages > 16)))
         return SGB_EINVAL;
-    if (ctas_per_sm) g->ctas_per_sm = ctas_per_sm;
+    if (ctas_per_sm) g->ctas_per_sm = ctas_per_sm < 0 ? 0 : ctas_per_sm;  // -1: automatic
     if (stages) g->stages = stages < 0 ? 0 : stages;  // -1: automatic depth
     return SGB_OK;
 }

@@ -132,8 +132,8 @@ struct sgb_grid {
 
     sgb::DevBuf err;      // unsigned device error word
     int num_sms = 148;
-    int ctas_per_sm = 4;
-    int stages = 0;  // 0: deepest staging ring that keeps ctas_per_sm CTAs resident
+    int ctas_per_sm = 0;  // 0: automatic per stencil kind (auto_ctas_per_sm)
+    int stages = 0;       // 0: deepest staging ring that keeps ctas_per_sm CTAs resident
 };
 
 namespace sgb {

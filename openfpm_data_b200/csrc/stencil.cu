@@ -226,7 +226,8 @@ int launch_stencil_impl(sgb_grid* g, int kind, const int* src, const int* dst, c
     L.use_tile = use_tile;
     L.stages = g->stages;
     L.num_sms = g->num_sms;
-    L.ctas = (unsigned)std::max<int64_t>(1, std::min<int64_t>(g->n, (int64_t)g->num_sms * g->ctas_per_sm));
+    const int cps = g->ctas_per_sm > 0 ? g->ctas_per_sm : auto_ctas_per_sm(kind);
+    L.ctas = (unsigned)std::max<int64_t>(1, std::min<int64_t>(g->n, (int64_t)g->num_sms * cps));
     for (int b = 0; b < 2; ++b)
         for (int j = 0; j < 2; ++j) {
             L.fs.in[b][j] = g->data[src[j < np ? j : 0]].as<float>();

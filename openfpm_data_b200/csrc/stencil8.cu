@@ -64,63 +64,6 @@ __device__ __forceinline__ float2 ldg_f2(const float* p) {
     return __ldg(reinterpret_cast<const float2*>(p));
 }
 
-// Packed FP32 pair arithmetic (sm_100: one instruction per x pair).  Each
-// element is rounded exactly like the scalar add.rn.ftz / mul.rn.ftz /
-// fma.rn.ftz it replaces.  Unlike the scalar forms, a packed mul.rn followed
-// by a packed add.rn is contracted into one fma by the assembler (measured:
-// 27% of Laplacians off by one ulp), so no packed product may feed a packed
-// sum: the Laplacian below builds -6c from exact doublings instead.
-__device__ __forceinline__ float2 add2(float2 a, float2 b) {
-    float2 r;
-    asm("{\n\t.reg .b64 ra, rb, rd;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
-        "add.rn.ftz.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;\n\t}"
-        : "=f"(r.x), "=f"(r.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
-    return r;
-}
-
-__device__ __forceinline__ float2 mul2(float2 a, float2 b) {
-    float2 r;
-    asm("{\n\t.reg .b64 ra, rb, rd;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
-        "mul.rn.ftz.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;\n\t}"
-        : "=f"(r.x), "=f"(r.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
-    return r;
-}
-
-__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) {
-    float2 r;
-    asm("{\n\t.reg .b64 ra, rb, rc, rd;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\tmov.b64 rc, {%6, %7};\n\t"
-        "fma.rn.ftz.f32x2 rd, ra, rb, rc;\n\tmov.b64 {%0, %1}, rd;\n\t}"
-        : "=f"(r.x), "=f"(r.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(c.x), "f"(c.y));
-    return r;
-}
-
-__device__ __forceinline__ float2 dup2(float v) { return make_float2(v, v); }
-
-// lap7 of stencil.cuh for the lane's x pair (c.x at x0, c.y at x0 + 1):
-// (((-6 c) + (xm + xp)) + (ym + yp)) + (zm + zp), with xm/xp of c.x being
-// (xm, c.y) and of c.y being (c.x, xp).
-__device__ __forceinline__ float2 lap7_pair(float2 c, float xm, float xp, float2 ym, float2 yp, float2 zm,
-                                           float2 zp) {
-    // -6c rounded once, as __fmul_rn(-6, c): 2c and 4c are exact, 4c + 2c = 6c rounds once
-    const float2 c2 = add2(c, c), c4 = add2(c2, c2), c6 = add2(c4, c2);
-    float2 l = make_float2(-c6.x, -c6.y);
-    l = add2(l, add2(make_float2(xm, c.x), make_float2(c.y, xp)));
-    l = add2(l, add2(ym, yp));
-    return add2(l, add2(zm, zp));
-}
-
-// gs_update of stencil.cuh for an x pair
-__device__ __forceinline__ void gs_update_pair(float2 u, float2 v, float2 lu, float2 lv, const GridInfo& p,
-                                               float2& un, float2& vn) {
-    const float2 uvv = mul2(mul2(u, v), v);
-    float2 du = fma2(dup2(p.Du), lu, make_float2(-uvv.x, -uvv.y));
-    du = fma2(dup2(p.F), add2(dup2(1.0f), make_float2(-u.x, -u.y)), du);  // 1 - u == 1 + (-u) exactly
-    float2 dv = fma2(dup2(p.Dv), lv, uvv);
-    dv = fma2(dup2(p.nFK), v, dv);
-    un = fma2(dup2(p.dt), du, u);
-    vn = fma2(dup2(p.dt), dv, v);
-}
-
 template <int KIND, int NP, bool BOX>
 __global__ void __launch_bounds__(kThreads8, 8)
     k_stencil7_e8(FieldSet fs, const uint8_t* __restrict__ mask, const int32_t* __restrict__ nn,
@@ -318,7 +261,8 @@ __global__ void __launch_bounds__(kThreads8, 8)
                     const float xm = ld1(aXm[p] + z * sXm);
                     const float xp = ld1(aXp[p] + z * sXp);
                     const float2 c = cv[p];
-                    lap[p] = lap7_pair(c, xm, xp, ym, yp, zmv[p], zp);
+                    lap[p].x = lap7(c.x, xm, c.y, ym.x, yp.x, zmv[p].x, zp.x);
+                    lap[p].y = lap7(c.y, c.x, xp, ym.y, yp.y, zmv[p].y, zp.y);
                     cur[p] = c;
                     zmv[p] = c;
                     cv[p] = zp;
@@ -330,14 +274,15 @@ __global__ void __launch_bounds__(kThreads8, 8)
                     act1 = act1 && in_box(prm, bx + 1, by, bz + z);
                 }
                 if (KIND == SGB_HEAT7) {
-                    const float2 h = fma2(dup2(cgi.dt), lap[0], cur[0]);
+                    const float2 h = make_float2(__fmaf_rn(cgi.dt, lap[0].x, cur[0].x), __fmaf_rn(cgi.dt, lap[0].y, cur[0].y));
                     float2 r;
                     r.x = act0 ? h.x : (m0 ? cur[0].x : bd);
                     r.y = act1 ? h.y : (m1 ? cur[0].y : bd);
                     *reinterpret_cast<float2*>(d0 + z * 64) = r;
                 } else {
                     float2 un, vn;
-                    gs_update_pair(cur[0], cur[NP - 1], lap[0], lap[NP - 1], cgi, un, vn);
+                    gs_update(cur[0].x, cur[NP - 1].x, lap[0].x, lap[NP - 1].x, cgi, un.x, vn.x);
+                    gs_update(cur[0].y, cur[NP - 1].y, lap[0].y, lap[NP - 1].y, cgi, un.y, vn.y);
                     // Active points take the update.  Points that do not exist take the destination's
                     // background, which they hold already (the background invariant), so the pair is
                     // written whole with one vector store; only existing inactive points (padding,
