@@ -525,9 +525,20 @@ def run_batched256(args, dist: Dist):
     p1.record()
     torch.cuda.synchronize()
     tp = dist.max(p0.elapsed_time(p1) / 1e3)
+    # the reference's execution model: one applyStencils launch per grid per step, one CTA per chunk
+    # (the generic tile kernel, which gathers the halo per cell as loadGhostBlock does)
+    r0, r1 = _events()
+    r0.record()
+    for g in grids:
+        for k in range(steps_per_solve):
+            g.applyStencils(sgb.HEAT7, [k % 2], [1 - k % 2], [W.HEAT_DT], tiled=True)
+    r1.record()
+    torch.cuda.synchronize()
+    tr = dist.max(r0.elapsed_time(r1) / 1e3)
     for g in grids:
         g.close()
     plain = dist.world * len(specs) / tp
+    plain_ref = dist.world * len(specs) / tr
     peak, pk = _peak_hbm()
     ach = 9 * pts * steps_per_solve * nsolves / (t / dist.world) / 1e9 if dist.world == 1 else None
     roof = {"bound": "hbm", "achieved": round(ach, 1) if ach else None, "peak": peak, "unit": "GB/s",
@@ -540,6 +551,8 @@ def run_batched256(args, dist: Dist):
                                            "stages": tune.stages, "threads_per_chunk": tune.threads_per_chunk,
                                            "table": tune.table},
                               "plain_solves_per_s": round(plain, 3), "batched_over_plain": round(batched / plain, 2),
+                              "plain_one_cta_per_chunk_solves_per_s": round(plain_ref, 3),
+                              "batched_over_plain_one_cta_per_chunk": round(batched / plain_ref, 2),
                               "l2": "resident fields >> L2"},
                  roofline=roof, cpu_baseline=None, e2e=None, gpu_launches=steps_per_solve * nsolves, clocks=clk)
 

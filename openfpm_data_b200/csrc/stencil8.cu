@@ -327,10 +327,10 @@ static int launch_kind(const LaunchDesc& L, cudaStream_t s) {
     }
     R = std::min(std::max(R, 3), rmax);
     const size_t smem = (size_t)kWarps * R * per;
-    // warps: CTAs per SM x SMs x kWarps, but at least 4 chunks per warp (each warp also streams its two
-    // neighbour chunks)
+    // warps: CTAs per SM x SMs x kWarps, at most one per chunk (a small grid is latency-bound: one chunk per
+    // warp, whose two neighbour chunks are L2 hits, beats a few warps walking several chunks each)
     const int64_t total = (int64_t)L.ctas * kWarps;
-    const int64_t nwarps = std::max<int64_t>(1, std::min<int64_t>(total, L.n / 4));
+    const int64_t nwarps = std::max<int64_t>(1, std::min<int64_t>(total, L.n));
     const unsigned blocks = (unsigned)((nwarps + kWarps - 1) / kWarps);
     auto kern = k_stencil7_e8<KIND, NP, BOX>;
     SGB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));

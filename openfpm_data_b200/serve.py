@@ -31,10 +31,18 @@ KIND = {"heat": L.HEAT7, "gs": L.GS7}
 NFIELDS = {"heat": 1, "gs": 2}
 
 
+# Device bytes the batches may hold per byte of live solve state: the live
+# buffers grow by half their capacity at a time (old and new both held while
+# the contents are copied), and removals are compacted into a second buffer
+# set, so the peak is about 3.5 times the live state.
+BATCH_OVERHEAD = 3.5
+
+
 def bytes_per_chunk(kind: str, bs: int = 512) -> int:
-    """Resident bytes of one chunk in a batch: two ping-pong copies of each
-    field, the mask, the neighbour row, the key and the slot id."""
-    return bs * (2 * 4 * NFIELDS[kind] + 1) + 8 * 4 + 8 + 4
+    """Device bytes charged to the budget per chunk of a request: two
+    ping-pong copies of each field, the mask, the neighbour row, the key and
+    the slot id, times the batches' buffer overhead."""
+    return int((bs * (2 * 4 * NFIELDS[kind] + 1) + 8 * 4 + 8 + 4) * BATCH_OVERHEAD)
 
 
 def balls_of(req: W.Request) -> np.ndarray:
@@ -128,7 +136,12 @@ class Server:
         src, dst = list(range(nf)), list(range(nf, 2 * nf))
         prm = HEAT_PARAMS if req.kind == "heat" else GS_PARAMS
         b = self.batches[req.kind]
-        slot = b.add(g, KIND[req.kind], src, dst, prm, req.steps)
+        try:
+            slot = b.add(g, KIND[req.kind], src, dst, prm, req.steps)
+        except L.SgbError as e:
+            if e.status != L.ENOMEM:
+                raise
+            return False  # the device is fuller than the budget says: retry once memory is returned
         n = g.nchunks
         used = n * bytes_per_chunk(req.kind)
         self.used += used
