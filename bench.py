@@ -62,6 +62,7 @@ def parse():
     ap.add_argument("--workload", choices=list(WORKLOADS), default="gs512",
                     help="gs512 (the headline line) or one of the other workloads")
     ap.add_argument("--serve-seconds", type=float, default=60.0, help="served: arrival window")
+    ap.add_argument("--serve-rate", type=float, default=2000.0, help="served: Poisson arrival rate (requests/s)")
     ap.add_argument("--plain-sample", type=int, default=64, help="served: requests solved alone for the baseline")
     return ap.parse_args()
 
@@ -569,7 +570,7 @@ def run_served(args, dist: Dist):
     from openfpm_data_b200 import serve as S
     from openfpm_data_b200 import workloads as W
     torch.cuda.set_device(dist.local)
-    reqs = W.requests(duration=args.serve_seconds, seed=4 + 1000 * dist.rank)
+    reqs = W.requests(rate=args.serve_rate, duration=args.serve_seconds, seed=4 + 1000 * dist.rank)
     warm = W.requests(duration=0.05, seed=99)
     srv = S.Server(budget_bytes=150e9, device=dist.local)
     srv.run(warm, realtime=False)
@@ -590,9 +591,11 @@ def run_served(args, dist: Dist):
     tp = time.perf_counter() - t0
     plain = len(sample) / tp
     served = dist.world * summ["completed"] / st.wall
-    return _line("served solves/s (heat + Gray-Scott requests, Poisson 2000/s)", round(served, 2), "solves/s",
+    return _line(f"served solves/s (heat + Gray-Scott requests, Poisson {args.serve_rate:g}/s)", round(served, 2),
+                 "solves/s",
                  dist, args, summ["completed"], st.wall,
-                 {"workload": f"served_poisson2000_{args.serve_seconds:g}s_edge32-256_seed4", "requests": len(reqs),
+                 {"workload": f"served_poisson{args.serve_rate:g}_{args.serve_seconds:g}s_edge32-256_seed4",
+                  "requests": len(reqs),
                   "serve": summ, "plain_sample": len(sample), "plain_solves_per_s": round(plain, 3),
                   "served_over_plain": round(served / plain, 2), "budget_bytes": 150e9},
                  roofline=None, cpu_baseline=None,

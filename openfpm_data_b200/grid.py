@@ -323,12 +323,28 @@ class Batch:
         L.check(self._lib.sgb_batch_read(self._h, slot, None, None, None, C.byref(n), None), "sgb_batch_read")
         return n.value
 
-    def read(self, slot: int, nfields: int, bs: int = 512, stream=None):
-        """(keys, mask, [fields]) of a slot's current state as numpy arrays."""
+    def read(self, slot: int, nfields: int, bs: int = 512, stream=None, staged: bool = False):
+        """(keys, mask, [fields]) of a slot's current state as numpy arrays.
+
+        staged=True reads into a grow-only pinned host buffer owned by the
+        batch (fast device-to-host copies) and returns views of it, valid
+        until the next staged read."""
         n = self.nchunks(slot)
-        keys = np.empty(n, np.int64)
-        mask = np.empty(n * bs, np.uint8)
-        fields = [np.empty(n * bs, np.float32) for _ in range(nfields)]
+        if staged:
+            need = n * 8 + n * bs + nfields * n * bs * 4
+            buf = getattr(self, "_pinned", None)
+            if buf is None or buf.numel() < need:
+                buf = torch.empty(max(need, 1 << 20), dtype=torch.uint8).pin_memory()
+                self._pinned = buf
+            raw = buf.numpy()
+            keys = raw[: n * 8].view(np.int64)
+            mask = raw[n * 8: n * 8 + n * bs]
+            o = n * 8 + n * bs
+            fields = [raw[o + j * n * bs * 4: o + (j + 1) * n * bs * 4].view(np.float32) for j in range(nfields)]
+        else:
+            keys = np.empty(n, np.int64)
+            mask = np.empty(n * bs, np.uint8)
+            fields = [np.empty(n * bs, np.float32) for _ in range(nfields)]
         ptrs = (C.c_void_p * nfields)(*[f.ctypes.data for f in fields])
         L.check(self._lib.sgb_batch_read(self._h, slot, keys.ctypes.data_as(C.c_void_p),
                                          mask.ctypes.data_as(C.c_void_p), ptrs, None, _stream(stream)),

@@ -58,7 +58,6 @@ class Done:
     t_done: float
     points: int
     steps: int
-    checksum: float
 
     @property
     def latency(self) -> float:
@@ -145,25 +144,24 @@ class Server:
         n = g.nchunks
         used = n * bytes_per_chunk(req.kind)
         self.used += used
-        self.active[(req.kind, slot)] = (req, now, used, n)
+        self.active[(req.kind, slot)] = (req, now, used, n, g.countExistingElements())
         return True
 
     def retire(self, now_fn, stats: ServeStats) -> None:
         for key in list(self.active):
             kind, slot = key
-            req, t_admit, used, n = self.active[key]
+            req, t_admit, used, n, points = self.active[key]
             b = self.batches[kind]
             if b.slot_steps(slot) < req.steps:
                 continue
-            keys, mask, fields = b.read(slot, NFIELDS[kind])
-            ex = mask.astype(bool)
-            chk = float(np.sum(fields[0][ex], dtype=np.float64))
+            # the response: the request's block map and final fields, read into pinned host memory
+            keys, mask, fields = b.read(slot, NFIELDS[kind], staged=not self.keep_results)
             if self.keep_results:
                 self.results[req.rid] = [keys, mask, fields]
             b.remove(slot)
             self.used -= used
             del self.active[key]
-            stats.done.append(Done(req.rid, kind, req.t_arrival, t_admit, now_fn(), int(ex.sum()), req.steps, chk))
+            stats.done.append(Done(req.rid, kind, req.t_arrival, t_admit, now_fn(), points, req.steps))
 
     def run(self, reqs: List[W.Request], realtime: bool = True, time_limit: Optional[float] = None) -> ServeStats:
         """Serve a request list.  realtime=True releases requests at their
