@@ -204,28 +204,39 @@ __global__ void k_new_pos(const int64_t* newkeys, int64_t nnew, const int64_t* k
     keys_out[pos] = k;
 }
 
-// Move whole chunks (chunk_words 16-byte words each) to their new position.
-__global__ void k_move_chunks(const uint4* src, uint4* dst, int64_t nchunks, int chunk_words, const int64_t* newpos) {
-    const int64_t total = nchunks * chunk_words;
-    for (int64_t w = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; w < total; w += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t c = w / chunk_words;
-        const int64_t o = w - c * chunk_words;
-        dst[newpos[c] * chunk_words + o] = src[w];
+// Move whole chunks (chunk_words 16-byte words each) to their new position:
+// one warp per chunk (no per-word index division), 16-byte loads and stores.
+__global__ void k_move_chunks(const uint4* __restrict__ src, uint4* __restrict__ dst, int64_t nchunks, int chunk_words,
+                              const int64_t* __restrict__ newpos) {
+    const int lane = threadIdx.x & 31;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t c = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; c < nchunks; c += nw) {
+        const uint4* sp = src + c * chunk_words;
+        uint4* dp = dst + newpos[c] * chunk_words;
+#pragma unroll 4
+        for (int o = lane; o < chunk_words; o += 32) dp[o] = sp[o];
     }
 }
 
-// Fill new chunks with one element pattern (background) / zero mask.
-__global__ void k_fill_chunks(unsigned char* dst, int64_t nnew, int chunk_elems, int es, uint64_t pattern,
-                              const int64_t* newpos) {
-    const int64_t total = nnew * chunk_elems;
-    for (int64_t w = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; w < total; w += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t c = w / chunk_elems;
-        const int64_t o = w - c * chunk_elems;
-        unsigned char* q = dst + ((size_t)newpos[c] * chunk_elems + o) * es;
-        if (es == 4) *(uint32_t*)q = (uint32_t)pattern;
-        else if (es == 8) *(uint64_t*)q = pattern;
-        else *q = (unsigned char)pattern;
+// Fill new chunks with one element pattern (background) / zero mask: one
+// warp per chunk, the pattern replicated into 16-byte words.
+__global__ void k_fill_chunks(uint4* __restrict__ dst, int64_t nnew, int chunk_words, uint4 word,
+                              const int64_t* __restrict__ newpos) {
+    const int lane = threadIdx.x & 31;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t c = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; c < nnew; c += nw) {
+        uint4* dp = dst + newpos[c] * chunk_words;
+        for (int o = lane; o < chunk_words; o += 32) dp[o] = word;
     }
+}
+
+// The element pattern of es bytes repeated over a 16-byte word.
+static uint4 replicate16(uint64_t pattern, int es) {
+    unsigned char b[16];
+    for (int i = 0; i < 16; ++i) b[i] = (unsigned char)(pattern >> (8 * (i % es)));
+    uint4 w;
+    std::memcpy(&w, b, 16);
+    return w;
 }
 
 // Per unique point: reduce with the existing value, write, set EXIST.
@@ -382,26 +393,29 @@ static int flush_impl(sgb_grid* g, const int* ops, int bits, cudaStream_t s) {
         }
         k_new_pos<<<nblk(NB), 256, 0, s>>>(newkeys, NB, g->keys.as<int64_t>(), nold, g->keys2.as<int64_t>(), npos);
         SGB_CUDA(cudaGetLastError());
-        const unsigned grid = (unsigned)std::min<int64_t>(4096, std::max<int64_t>(1, (nold * bs / 16 + 255) / 256));
+        // one warp per chunk: at most 8 CTAs of 8 warps per SM, no more warps than chunks
+        auto warp_grid = [&](int64_t chunks) {
+            return (unsigned)std::max<int64_t>(1, std::min<int64_t>((int64_t)g->num_sms * 8, (chunks + 7) / 8));
+        };
         for (int p = 0; p < g->nprop; ++p) {
             const int es = elem_size(g->ptype[p]);
             if (nold > 0) {
-                k_move_chunks<<<grid, 256, 0, s>>>(g->data[p].as<uint4>(), g->data2[p].as<uint4>(), nold, bs * es / 16,
-                                                   oldpos);
+                k_move_chunks<<<warp_grid(nold), 256, 0, s>>>(g->data[p].as<uint4>(), g->data2[p].as<uint4>(), nold,
+                                                              bs * es / 16, oldpos);
                 SGB_CUDA(cudaGetLastError());
             }
             uint64_t pat = 0;
             std::memcpy(&pat, g->bck[p], es);
-            k_fill_chunks<<<(unsigned)std::min<int64_t>(4096, nblk(NB * bs)), 256, 0, s>>>(
-                g->data2[p].as<unsigned char>(), NB, bs, es, pat, npos);
+            k_fill_chunks<<<warp_grid(NB), 256, 0, s>>>(g->data2[p].as<uint4>(), NB, bs * es / 16,
+                                                        replicate16(pat, es), npos);
             SGB_CUDA(cudaGetLastError());
         }
         if (nold > 0) {
-            k_move_chunks<<<grid, 256, 0, s>>>(g->mask.as<uint4>(), g->mask2.as<uint4>(), nold, bs / 16, oldpos);
+            k_move_chunks<<<warp_grid(nold), 256, 0, s>>>(g->mask.as<uint4>(), g->mask2.as<uint4>(), nold, bs / 16,
+                                                          oldpos);
             SGB_CUDA(cudaGetLastError());
         }
-        k_fill_chunks<<<(unsigned)std::min<int64_t>(4096, nblk(NB * bs)), 256, 0, s>>>(g->mask2.as<unsigned char>(),
-                                                                                       NB, bs, 1, 0, npos);
+        k_fill_chunks<<<warp_grid(NB), 256, 0, s>>>(g->mask2.as<uint4>(), NB, bs / 16, make_uint4(0, 0, 0, 0), npos);
         SGB_CUDA(cudaGetLastError());
         // swap buffer sets
         std::swap(g->keys, g->keys2);
