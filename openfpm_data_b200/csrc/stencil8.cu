@@ -65,7 +65,7 @@ __device__ __forceinline__ float2 ldg_f2(const float* p) {
 }
 
 template <int KIND, int NP, bool BOX>
-__global__ void __launch_bounds__(kThreads8, 8)
+__global__ void __launch_bounds__(kThreads8, KIND == SGB_GS7 ? 5 : 8)
     k_stencil7_e8(FieldSet fs, const uint8_t* __restrict__ mask, const int32_t* __restrict__ nn,
                   const int64_t* __restrict__ keys, const int32_t* __restrict__ gid,
                   const GridInfo* __restrict__ grids, GridInfo g0, int64_t n, Geometry geo, StencilParams prm,
