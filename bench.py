@@ -55,7 +55,7 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--e2e-solves", type=int, default=3)
     ap.add_argument("--solve-steps", type=int, default=1000)
-    ap.add_argument("--cpu-steps", type=int, default=400, help="cap of the CPU baseline sample (about 25 s)")
+    ap.add_argument("--cpu-steps", type=int, default=150, help="cap of the CPU baseline sample (10-30 s)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ctas-per-sm", type=int, default=0)
     ap.add_argument("--stages", type=int, default=0)

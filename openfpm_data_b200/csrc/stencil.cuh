@@ -50,9 +50,9 @@ __device__ __forceinline__ void gs_update(float u, float v, float lu, float lv, 
 }
 
 // CTAs per SM of the pipelined 8^3 kernel when the caller leaves it automatic
-// (measured on the 512^3 grids: Gray-Scott keeps 5 two-warp CTAs with 4-deep
-// rings resident, heat 8 with 3-deep rings).
-inline int auto_ctas_per_sm(int kind) { return kind == SGB_GS7 ? 5 : 8; }
+// (measured on the 512^3 grids: Gray-Scott runs best with 6 two-warp CTAs
+// and 3-deep rings resident, heat with 8).
+inline int auto_ctas_per_sm(int kind) { return kind == SGB_GS7 ? 6 : 8; }
 
 // Everything one stencil launch needs.
 struct LaunchDesc {

@@ -13,18 +13,20 @@
 // mbarrier.  The x halo is not fetched: an existing -x / +x neighbour is
 // always the previous / next position of the sorted index, so it sits in the
 // neighbouring stage of the same ring.  The y and z faces (256 B each per
-// field) go to registers instead of shared memory, loaded one chunk ahead:
-// a z face is one 8-byte load per lane (the lane's own x pair), a y face one
-// 8-byte load per lane spread over the lanes ([z][x pair]) and handed to the
-// y = 0 / y = 7 lanes by a shuffle at each z.  Keeping faces out of the ring
-// makes a stage 2.6 KB (heat) / 4.6 KB (Gray-Scott), so more warps fit on an
-// SM.  While chunk q is computed, chunks up to q - 2 + R are in flight; after
+// field) are not staged by the ring: each lane loads, one chunk ahead, one
+// 16-byte quad of the z face its half of the warp needs and one of a y face
+// (lanes 0-15 the -y face, 16-31 the +y face, [z][x quad]); the y faces are
+// written once per chunk to a 0.5 / 1 KB per-warp buffer that the y = 0 /
+// y = 7 lanes read.  Keeping faces out of the ring makes a stage 2.6 KB
+// (heat) / 4.6 KB (Gray-Scott), so more warps fit on an SM.  While chunk q
+// is computed, chunks up to q - 2 + R are in flight; after
 // it, the stage of chunk q - 1 is refilled with chunk q - 1 + R.  A warp
 // waits only on its own barriers, in order, so phase parities are exact and
 // no warp ever waits for another.
 //
-// Compute: each lane owns a pair of x-adjacent points of one y row and
-// marches z = 0..7, carrying the z-1 / z / z+1 values in registers.
+// Compute: lanes 0-15 take z = 0..3 and lanes 16-31 z = 4..7; in each z
+// slice a lane owns four x-adjacent points (16-byte loads and stores) of one
+// y row and marches its four slices carrying z-1 / z / z+1 in registers.
 //
 // Points with mask byte 0 hold the background value in HBM (grid.cu keeps
 // that invariant per property, see sgb_grid::clean), so a neighbour value is
@@ -56,16 +58,20 @@ struct alignas(128) Stage8 {
 // y and z faces of one chunk in registers (see the file comment)
 template <int NP>
 struct Faces {
-    float2 zm[NP], zp[NP];  // the lane's own x pair in the z = 7 / z = 0 slices of the -z / +z chunks
-    float2 ym[NP], yp[NP];  // [z = lane / 4][x pair = lane % 4] of the y = 7 / y = 0 rows of the -y / +y chunks
+    // z face of the lane's half: the lane's own x quad in the z = 7 slice of the -z chunk (lanes 0-15) or
+    // the z = 0 slice of the +z chunk (lanes 16-31)
+    float4 zf[NP];
+    // y face element [z = (lane & 15) / 2][x quad = lane & 1] of the y = 7 row of the -y chunk (lanes 0-15)
+    // or the y = 0 row of the +y chunk (lanes 16-31)
+    float4 yf[NP];
 };
 
-__device__ __forceinline__ float2 ldg_f2(const float* p) {
-    return __ldg(reinterpret_cast<const float2*>(p));
+__device__ __forceinline__ float4 ldg_f4(const float* p) {
+    return __ldg(reinterpret_cast<const float4*>(p));
 }
 
 template <int KIND, int NP, bool BOX>
-__global__ void __launch_bounds__(kThreads8, KIND == SGB_GS7 ? 5 : 8)
+__global__ void __launch_bounds__(kThreads8, KIND == SGB_GS7 ? 6 : 8)
     k_stencil7_e8(FieldSet fs, const uint8_t* __restrict__ mask, const int32_t* __restrict__ nn,
                   const int64_t* __restrict__ keys, const int32_t* __restrict__ gid,
                   const GridInfo* __restrict__ grids, GridInfo g0, int64_t n, Geometry geo, StencilParams prm,
@@ -164,21 +170,25 @@ __global__ void __launch_bounds__(kThreads8, KIND == SGB_GS7 ? 5 : 8)
     int issued = npro;
 
     // ------------------------------------------------------------ compute side
-    const int y = lane >> 2, x0 = (lane & 3) << 1;
+    // Lane l takes z = 4h .. 4h + 3 with h = l / 16 and, in each z slice, the x quad xq = l % 2 of row
+    // y = (l % 16) / 2: four points, the z-1 / z / z+1 values carried in registers.
+    const int h = lane >> 4, r16 = lane & 15, y = r16 >> 1, xq = r16 & 1, x0 = xq << 2;
+    const int zb = h << 2;
     const int o0 = y * 8 + x0;  // the lane's first point in a z slice
-    const int yo = (lane >> 2) * 64 + ((lane & 3) << 1);  // this lane's element of a y face: z = lane / 4
-    // faces of the chunk held in ring slot `slot` (its metadata are written at issue time)
+    const int fo = (r16 >> 1) * 64 + (xq << 2);  // the lane's element of a y face (z = r16 / 2)
+    float* ybuf = reinterpret_cast<float*>(smem_raw + (size_t)kWarps * R * (sizeof(Stage8<NP>) + 8)) +
+                  warp * (NP * 2 * 64);  // y faces of the chunk being computed, [field][-y / +y][z * 8 + x]
+    // faces of the chunk held in ring slot `st` (its metadata are written at issue time)
     auto load_faces = [&](const Stage8<NP>& st, Faces<NP>& f) {
         const int par = st.par;
-        const int32_t fym = st.nn[2], fyp = st.nn[3], fzm = st.nn[4], fzp = st.nn[5];
+        const int32_t fy = h == 0 ? st.nn[2] : st.nn[3], fz = h == 0 ? st.nn[4] : st.nn[5];
 #pragma unroll
         for (int p = 0; p < NP; ++p) {
             const float* src = p == 0 ? (par ? fs.in[1][0] : fs.in[0][0]) : (par ? fs.in[1][NP - 1] : fs.in[0][NP - 1]);
-            const float2 bk = st.bk[p];
-            f.zm[p] = fzm >= 0 ? ldg_f2(src + (int64_t)fzm * 512 + 448 + o0) : bk;
-            f.zp[p] = fzp >= 0 ? ldg_f2(src + (int64_t)fzp * 512 + o0) : bk;
-            f.ym[p] = fym >= 0 ? ldg_f2(src + (int64_t)fym * 512 + 56 + yo) : bk;
-            f.yp[p] = fyp >= 0 ? ldg_f2(src + (int64_t)fyp * 512 + yo) : bk;
+            const float b = st.bk[p].x;
+            const float4 bk = make_float4(b, b, b, b);
+            f.zf[p] = fz >= 0 ? ldg_f4(src + (int64_t)fz * 512 + (h == 0 ? 448 : 0) + o0) : bk;
+            f.yf[p] = fy >= 0 ? ldg_f4(src + (int64_t)fy * 512 + (h == 0 ? 56 : 0) + fo) : bk;
         }
     };
     int waited = 0, ws = 0;     // chunks [0, waited) have landed; ws = slot of chunk `waited`
@@ -212,6 +222,11 @@ __global__ void __launch_bounds__(kThreads8, KIND == SGB_GS7 ? 5 : 8)
         }
         const Stage8<NP>& st = ring[sq];
         if (st.active) {
+            // the y faces of this chunk to the warp's buffer, read below by the y = 0 / y = 7 lanes
+#pragma unroll
+            for (int p = 0; p < NP; ++p)
+                *reinterpret_cast<float4*>(&ybuf[(p * 2 + h) * 64 + (r16 >> 1) * 8 + x0]) = fc.yf[p];
+            __syncwarp();
             const Stage8<NP>& pv = ring[sp];
             const Stage8<NP>& nx = ring[sn];
             const int32_t n0 = st.nn[0], n1 = st.nn[1];
@@ -220,85 +235,106 @@ __global__ void __launch_bounds__(kThreads8, KIND == SGB_GS7 ? 5 : 8)
             // (byte offsets into the dynamic shared array: plain loads through it stay shared-memory loads
             // and leave the scheduler free to batch them)
             auto off = [&](const void* ptr) { return (uint32_t)((const unsigned char*)ptr - smem_raw); };
-            auto ld2 = [&](uint32_t o) { return *reinterpret_cast<const float2*>(smem_raw + o); };
+            auto ld4 = [&](uint32_t o) { return *reinterpret_cast<const float4*>(smem_raw + o); };
             auto ld1 = [&](uint32_t o) { return *reinterpret_cast<const float*>(smem_raw + o); };
-            uint32_t aC[NP], aXm[NP], aXp[NP];
-            float2 zmv[NP], cv[NP];
+            // addresses at the lane's first z (zb) and their steps per z
+            uint32_t aC[NP], aXm[NP], aXp[NP], aYm[NP], aYp[NP];
+            float4 zmv[NP], cv[NP];
+            const uint32_t sYm = y > 0 ? 256u : 32u, sYp = y < 7 ? 256u : 32u;
+            const uint32_t sXm = (xq == 1 || xm_ok) ? 256u : 0u, sXp = (xq == 0 || xp_ok) ? 256u : 0u;
 #pragma unroll
             for (int p = 0; p < NP; ++p) {
                 const uint32_t bk = off(&st.bk[p]);
-                aC[p] = off(&st.tile[p][o0]);
-                aXm[p] = x0 > 0 ? aC[p] - 4 : (xm_ok ? off(&pv.tile[p][y * 8 + 7]) : bk);
-                aXp[p] = x0 < 6 ? aC[p] + 8 : (xp_ok ? off(&nx.tile[p][y * 8]) : bk);
-                zmv[p] = fc.zm[p];
-                cv[p] = ld2(aC[p]);
+                aC[p] = off(&st.tile[p][zb * 64 + o0]);
+                aYm[p] = y > 0 ? aC[p] - 32 : off(&ybuf[(p * 2 + 0) * 64 + zb * 8 + x0]);
+                aYp[p] = y < 7 ? aC[p] + 32 : off(&ybuf[(p * 2 + 1) * 64 + zb * 8 + x0]);
+                aXm[p] = xq == 1 ? aC[p] - 4 : (xm_ok ? off(&pv.tile[p][zb * 64 + y * 8 + 7]) : bk);
+                aXp[p] = xq == 0 ? aC[p] + 16 : (xp_ok ? off(&nx.tile[p][zb * 64 + y * 8]) : bk);
+                if (!(xq == 1 || xm_ok)) aXm[p] = bk;  // step 0 on the background
+                if (!(xq == 0 || xp_ok)) aXp[p] = bk;
+                // z - 1 of the first slice: the -z face for the lower half, slice 3 for the upper half
+                zmv[p] = h == 0 ? fc.zf[p] : ld4(aC[p] - 256);
+                cv[p] = ld4(aC[p]);
             }
-            const uint32_t sXm = (x0 > 0 || xm_ok) ? 256u : 0u;
-            const uint32_t sXp = (x0 < 6 || xp_ok) ? 256u : 0u;
-            const uint32_t aM = off(&st.mt[o0]);
+            const uint32_t aM = off(&st.mt[zb * 64 + o0]);
             const int par = st.par;
-            float* d0 = (par ? fs.out[1][0] : fs.out[0][0]) + i * 512 + o0;
-            float* d1 = (par ? fs.out[1][NP - 1] : fs.out[0][NP - 1]) + i * 512 + o0;
+            float* d0 = (par ? fs.out[1][0] : fs.out[0][0]) + i * 512 + zb * 64 + o0;
+            float* d1 = (par ? fs.out[1][NP - 1] : fs.out[0][NP - 1]) + i * 512 + zb * 64 + o0;
             const GridInfo cgi = st.gi;
-            const float bd = st.gi.bck[par ^ 1][0];  // backgrounds of the destination fields
-            const float bd0 = bd, bd1 = st.gi.bck[par ^ 1][NP - 1];
-            const int32_t bx = st.cx + x0, by = st.cy + y, bz = st.cz;
+            const float bd0 = st.gi.bck[par ^ 1][0], bd1 = st.gi.bck[par ^ 1][NP - 1];  // destination backgrounds
+            const int32_t bx = st.cx + x0, by = st.cy + y, bz = st.cz + zb;
 #pragma unroll
-            for (int z = 0; z < 8; ++z) {
-                const uint32_t m = *reinterpret_cast<const unsigned short*>(smem_raw + aM + z * 64);
-                float2 lap[NP], cur[NP];
+            for (int zz = 0; zz < 4; ++zz) {
+                const uint32_t m4 = *reinterpret_cast<const uint32_t*>(smem_raw + aM + zz * 64);
+                float4 lap[NP], cur[NP];
 #pragma unroll
                 for (int p = 0; p < NP; ++p) {
-                    // y faces: row z of the face sits in lanes 4z .. 4z+3, one x pair each
-                    const int srcl = z * 4 + (lane & 3);
-                    const float2 fym = make_float2(__shfl_sync(0xffffffffu, fc.ym[p].x, srcl),
-                                                   __shfl_sync(0xffffffffu, fc.ym[p].y, srcl));
-                    const float2 fyp = make_float2(__shfl_sync(0xffffffffu, fc.yp[p].x, srcl),
-                                                   __shfl_sync(0xffffffffu, fc.yp[p].y, srcl));
-                    const float2 zp = z < 7 ? ld2(aC[p] + (z + 1) * 256) : fc.zp[p];
-                    const float2 ym = y > 0 ? ld2(aC[p] + z * 256 - 32) : fym;
-                    const float2 yp = y < 7 ? ld2(aC[p] + z * 256 + 32) : fyp;
-                    const float xm = ld1(aXm[p] + z * sXm);
-                    const float xp = ld1(aXp[p] + z * sXp);
-                    const float2 c = cv[p];
-                    lap[p].x = lap7(c.x, xm, c.y, ym.x, yp.x, zmv[p].x, zp.x);
-                    lap[p].y = lap7(c.y, c.x, xp, ym.y, yp.y, zmv[p].y, zp.y);
+                    // z + 1: the next slice, or for the upper half's last slice the +z face
+                    float4 zp;
+                    if (zz < 3) {
+                        zp = ld4(aC[p] + (zz + 1) * 256);
+                    } else {
+                        const float4 t4 = ld4(h == 0 ? aC[p] + 4 * 256 : aC[p]);  // in-stage address for both halves
+                        zp = h == 0 ? t4 : fc.zf[p];
+                    }
+                    const float4 ym = ld4(aYm[p] + zz * sYm);
+                    const float4 yp = ld4(aYp[p] + zz * sYp);
+                    const float xm = ld1(aXm[p] + zz * sXm);
+                    const float xp = ld1(aXp[p] + zz * sXp);
+                    const float4 c = cv[p], zm = zmv[p];
+                    lap[p].x = lap7(c.x, xm, c.y, ym.x, yp.x, zm.x, zp.x);
+                    lap[p].y = lap7(c.y, c.x, c.z, ym.y, yp.y, zm.y, zp.y);
+                    lap[p].z = lap7(c.z, c.y, c.w, ym.z, yp.z, zm.z, zp.z);
+                    lap[p].w = lap7(c.w, c.z, xp, ym.w, yp.w, zm.w, zp.w);
                     cur[p] = c;
                     zmv[p] = c;
                     cv[p] = zp;
                 }
-                const uint32_t m0 = m & 0xffu, m1 = m >> 8;
-                bool act0 = (m0 & 3u) == 1u, act1 = (m1 & 3u) == 1u;  // EXIST and not PADDING
-                if (BOX) {
-                    act0 = act0 && in_box(prm, bx, by, bz + z);
-                    act1 = act1 && in_box(prm, bx + 1, by, bz + z);
+                const uint32_t mb[4] = {m4 & 0xffu, (m4 >> 8) & 0xffu, (m4 >> 16) & 0xffu, m4 >> 24};
+                bool act[4];
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    act[k] = (mb[k] & 3u) == 1u;  // EXIST and not PADDING
+                    if (BOX) act[k] = act[k] && in_box(prm, bx + k, by, bz + zz);
                 }
                 if (KIND == SGB_HEAT7) {
-                    const float2 h = make_float2(__fmaf_rn(cgi.dt, lap[0].x, cur[0].x), __fmaf_rn(cgi.dt, lap[0].y, cur[0].y));
-                    float2 r;
-                    r.x = act0 ? h.x : (m0 ? cur[0].x : bd);
-                    r.y = act1 ? h.y : (m1 ? cur[0].y : bd);
-                    *reinterpret_cast<float2*>(d0 + z * 64) = r;
+                    float4 o;
+                    o.x = act[0] ? __fmaf_rn(cgi.dt, lap[0].x, cur[0].x) : (mb[0] ? cur[0].x : bd0);
+                    o.y = act[1] ? __fmaf_rn(cgi.dt, lap[0].y, cur[0].y) : (mb[1] ? cur[0].y : bd0);
+                    o.z = act[2] ? __fmaf_rn(cgi.dt, lap[0].z, cur[0].z) : (mb[2] ? cur[0].z : bd0);
+                    o.w = act[3] ? __fmaf_rn(cgi.dt, lap[0].w, cur[0].w) : (mb[3] ? cur[0].w : bd0);
+                    *reinterpret_cast<float4*>(d0 + zz * 64) = o;
                 } else {
-                    float2 un, vn;
+                    float4 un, vn;
                     gs_update(cur[0].x, cur[NP - 1].x, lap[0].x, lap[NP - 1].x, cgi, un.x, vn.x);
                     gs_update(cur[0].y, cur[NP - 1].y, lap[0].y, lap[NP - 1].y, cgi, un.y, vn.y);
+                    gs_update(cur[0].z, cur[NP - 1].z, lap[0].z, lap[NP - 1].z, cgi, un.z, vn.z);
+                    gs_update(cur[0].w, cur[NP - 1].w, lap[0].w, lap[NP - 1].w, cgi, un.w, vn.w);
                     // Active points take the update.  Points that do not exist take the destination's
-                    // background, which they hold already (the background invariant), so the pair is
+                    // background, which they hold already (the background invariant), so the quad is
                     // written whole with one vector store; only existing inactive points (padding,
                     // outside the box) keep their value, with scalar stores.
-                    const bool w0 = act0 || m0 == 0, w1 = act1 || m1 == 0;
-                    un.x = act0 ? un.x : bd0;
-                    vn.x = act0 ? vn.x : bd1;
-                    un.y = act1 ? un.y : bd0;
-                    vn.y = act1 ? vn.y : bd1;
-                    const bool both = w0 && w1;
-                    if (both) *reinterpret_cast<float2*>(d0 + z * 64) = un;
-                    if (both) *reinterpret_cast<float2*>(d1 + z * 64) = vn;
-                    if (act0 && !both) d0[z * 64] = un.x;
-                    if (act0 && !both) d1[z * 64] = vn.x;
-                    if (act1 && !both) d0[z * 64 + 1] = un.y;
-                    if (act1 && !both) d1[z * 64 + 1] = vn.y;
+                    un.x = act[0] ? un.x : bd0;
+                    un.y = act[1] ? un.y : bd0;
+                    un.z = act[2] ? un.z : bd0;
+                    un.w = act[3] ? un.w : bd0;
+                    vn.x = act[0] ? vn.x : bd1;
+                    vn.y = act[1] ? vn.y : bd1;
+                    vn.z = act[2] ? vn.z : bd1;
+                    vn.w = act[3] ? vn.w : bd1;
+                    bool all = true;
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) all = all && (act[k] || mb[k] == 0);
+                    if (all) *reinterpret_cast<float4*>(d0 + zz * 64) = un;
+                    if (all) *reinterpret_cast<float4*>(d1 + zz * 64) = vn;
+                    if (__any_sync(0xffffffffu, !all)) {  // rare: padding or box edges in the quad
+                        const float u4[4] = {un.x, un.y, un.z, un.w}, v4[4] = {vn.x, vn.y, vn.z, vn.w};
+#pragma unroll
+                        for (int k = 0; k < 4; ++k) {
+                            if (!all && act[k]) d0[zz * 64 + k] = u4[k];
+                            if (!all && act[k]) d1[zz * 64 + k] = v4[k];
+                        }
+                    }
                 }
             }
         }
@@ -318,15 +354,17 @@ static int launch_kind(const LaunchDesc& L, cudaStream_t s) {
     // ring depth per warp: at least 3 (chunks q - 1, q, q + 1), within one CTA's shared memory; 0 = the
     // deepest ring (up to 8) with which the requested CTAs per SM stay resident
     const size_t per = sizeof(Stage8<NP>) + 8;
-    const int rmax = (int)((227u * 1024u) / (per * kWarps));
+    const size_t yface_bytes = NP * 2 * 64 * sizeof(float);  // per warp
+    const int rmax = (int)((227u * 1024u - kWarps * yface_bytes) / (per * kWarps));
     int R = L.stages;
     if (R <= 0) {
         const int64_t per_sm = std::max<int64_t>(1, ((int64_t)L.ctas + L.num_sms - 1) / L.num_sms);
         const int64_t budget = 228 * 1024 / per_sm - 1024;  // 1 KB of every CTA's shared memory is reserved
-        R = (int)std::max<int64_t>(3, std::min<int64_t>(8, budget / (int64_t)(per * kWarps)));
+        R = (int)std::max<int64_t>(3, std::min<int64_t>(8, (budget - (int64_t)(kWarps * yface_bytes)) /
+                                                               (int64_t)(per * kWarps)));
     }
     R = std::min(std::max(R, 3), rmax);
-    const size_t smem = (size_t)kWarps * R * per;
+    const size_t smem = (size_t)kWarps * (R * per + yface_bytes);
     // warps: CTAs per SM x SMs x kWarps, at most one per chunk (a small grid is latency-bound: one chunk per
     // warp, whose two neighbour chunks are L2 hits, beats a few warps walking several chunks each)
     const int64_t total = (int64_t)L.ctas * kWarps;
