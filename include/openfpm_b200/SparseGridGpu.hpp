@@ -527,6 +527,29 @@ class SparseGridGpu {
         return 0;
     }
 
+    // remove(box): queue a section whose points removePoints deletes (SparseGridGpu.hpp:3528-3531)
+    void remove(const Box<dim, int>& section_to_delete) { rem_sects_.push_back(section_to_delete); }
+
+    // removePoints(ctx) (SparseGridGpu.hpp:3417-3489): the chunks stay, their points in the boxes go
+    void removePoints(gpu::ofp_context_t&) {
+        if (rem_sects_.empty()) return;
+        std::vector<int64_t> b;
+        for (const auto& bx : rem_sects_)
+            for (int k = 0; k < 2; ++k)
+                for (unsigned d = 0; d < dim; ++d) b.push_back(k == 0 ? bx.getLow(d) : bx.getHigh(d));
+        check(sgb_remove_boxes(g_, (int64_t)rem_sects_.size(), b.data(), nullptr), "removePoints");
+        rem_sects_.clear();
+    }
+
+    // The existing points in the order getIterator() visits them (chunk order, then offset order);
+    // with start / stop only those inside that inclusive box (the sub-iterator).
+    std::vector<grid_key_dx<dim, int>> existingPoints() const { return existing_points_impl(nullptr); }
+    std::vector<grid_key_dx<dim, int>> existingPoints(const grid_key_dx<dim>& start, const grid_key_dx<dim>& stop) const {
+        int64_t b[6];
+        for (unsigned d = 0; d < 3; ++d) b[d] = start.get(d), b[3 + d] = stop.get(d);
+        return existing_points_impl(b);
+    }
+
     size_t countExistingElements() const {
         int64_t e = 0;
         check(sgb_count_existing(g_, &e, nullptr, nullptr), "countExistingElements");
@@ -558,6 +581,25 @@ class SparseGridGpu {
     }
 
    private:
+    std::vector<Box<dim, int>> rem_sects_;
+
+    std::vector<grid_key_dx<dim, int>> existing_points_impl(const int64_t* box) const {
+        int64_t cnt = 0;
+        check(sgb_existing_points(g_, box, nullptr, 0, &cnt, nullptr), "existingPoints");
+        std::vector<grid_key_dx<dim, int>> out(cnt);
+        if (cnt == 0) return out;
+        int32_t* d = nullptr;
+        if (cudaMalloc(&d, (size_t)cnt * 12) != cudaSuccess) throw sgb_error(SGB_ENOMEM, "existingPoints");
+        int st = sgb_existing_points(g_, box, d, cnt, &cnt, nullptr);
+        std::vector<int32_t> h((size_t)cnt * 3);
+        if (st == SGB_OK) cudaMemcpy(h.data(), d, h.size() * 4, cudaMemcpyDeviceToHost);
+        cudaFree(d);
+        check(st, "existingPoints");
+        for (int64_t i = 0; i < cnt; ++i)
+            for (unsigned k = 0; k < dim; ++k) out[i].set_d(k, h[i * 3 + k]);
+        return out;
+    }
+
     void run_fixed(int kind, unsigned s, unsigned d, const float* prm, int nprm, const Box<dim, int>& box) {
         int src[2] = {(int)s, 0}, dst[2] = {(int)d, 0};
         int64_t b[6];

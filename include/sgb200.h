@@ -188,6 +188,23 @@ int sgb_load_map_dev(sgb_grid* g, int64_t n, const int64_t* keys_dev, const void
  * (any pointer may be NULL to skip it). */
 int sgb_download_map(sgb_grid* g, int64_t* keys_host, void* const* data_host, uint8_t* mask_host, sgb_stream s);
 
+/* remove(box) for each box, then removePoints (SparseGridGpu.hpp:3417-3489,
+ * 3528-3531): every existing point inside one of the boxes loses its mask
+ * byte (EXIST and PADDING); chunks are kept.  boxes_host: nboxes x {lo[3],
+ * hi[3]}, inclusive, tested as unsigned int like the reference's
+ * Box<dim, unsigned int> (a negative lower corner matches nothing).  3-D
+ * grids; synchronises the stream. */
+int sgb_remove_boxes(sgb_grid* g, int64_t nboxes, const int64_t* boxes_host, sgb_stream s);
+
+/* The coordinates of the existing points, in (chunk position, offset in the
+ * chunk) order: the points the reference's getIterator() / sub-iterator
+ * (src/SparseGridGpu/Iterators/SparseGridGpu_iterator.hpp:17-304) visit.
+ * box_host: NULL or {lo[3], hi[3]} inclusive.  *count receives the number of
+ * points; coords_dev (int32 [3 * capacity]) is written when capacity >=
+ * *count, so a first call with capacity 0 sizes the buffer.  3-D grids. */
+int sgb_existing_points(sgb_grid* g, const int64_t* box_host, int32_t* coords_dev, int64_t capacity,
+                        int64_t* count, sgb_stream s);
+
 /* countExistingElements / countBoundaryElements (SparseGridGpu.hpp:2422-2474). */
 int sgb_count_existing(sgb_grid* g, int64_t* existing, int64_t* padding, sgb_stream s);
 

@@ -101,7 +101,7 @@ static int fill(void* dst, int64_t count, int esize, uint64_t pattern, cudaStrea
     return SGB_OK;
 }
 
-static uint64_t bck_pattern(const sgb_grid* g, int p) {
+uint64_t bck_pattern(const sgb_grid* g, int p) {
     uint64_t v = 0;
     std::memcpy(&v, g->bck[p], elem_size(g->ptype[p]));
     return v;

@@ -236,6 +236,45 @@ class SparseGridGpu:
                                            mask.ctypes.data_as(C.c_void_p), _stream(stream)), "sgb_download_map")
         return keys, data, mask
 
+    # ---------------------------------------------------------------- remove / iterate
+    def remove(self, box) -> None:
+        """remove(box): queue an inclusive box ((lo), (hi)) of points to remove at removePoints()."""
+        lo, hi = box
+        self._rem = getattr(self, "_rem", []) + [list(lo) + list(hi)]
+
+    def removePoints(self, stream=None) -> None:
+        """Remove the existing points inside the queued boxes (chunks stay) and clear the queue."""
+        rem = getattr(self, "_rem", [])
+        self._rem = []
+        if not rem:
+            return
+        b = np.ascontiguousarray(np.asarray(rem, dtype=np.int64).reshape(-1, 6))
+        L.check(self._lib.sgb_remove_boxes(self._h, len(b), b.ctypes.data_as(C.c_void_p), _stream(stream)),
+                "sgb_remove_boxes")
+
+    def existing_points(self, box=None, stream=None) -> torch.Tensor:
+        """int32 [k, 3] device tensor of the existing points (inside the inclusive box
+        ((lo), (hi)) if given), in chunk order then offset order."""
+        bx = None
+        if box is not None:
+            bx = np.ascontiguousarray(np.asarray(list(box[0]) + list(box[1]), dtype=np.int64))
+        bptr = None if bx is None else bx.ctypes.data_as(C.c_void_p)
+        cnt = C.c_int64()
+        L.check(self._lib.sgb_existing_points(self._h, bptr, None, 0, C.byref(cnt), _stream(stream)),
+                "sgb_existing_points")
+        out = torch.empty((cnt.value, 3), dtype=torch.int32, device=f"cuda:{self.device}")
+        if cnt.value:
+            L.check(self._lib.sgb_existing_points(self._h, bptr, out.data_ptr(), cnt.value, C.byref(cnt),
+                                                  _stream(stream)), "sgb_existing_points")
+        return out
+
+    def getIterator(self, start=None, stop=None):
+        """Host iteration over the existing points (inside [start, stop] when given), as
+        (x, y, z) tuples in the reference iterator's order."""
+        box = None if start is None else (start, stop)
+        for p in self.existing_points(box).cpu().numpy():
+            yield tuple(int(v) for v in p)
+
     def countExistingElements(self, stream=None) -> int:
         e = C.c_int64()
         L.check(self._lib.sgb_count_existing(self._h, C.byref(e), None, _stream(stream)), "sgb_count_existing")

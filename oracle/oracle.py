@@ -62,6 +62,7 @@ def _load():
         _lib.sgo_find_neighbours.restype = i32
         _lib.sgo_find_neighbours.argtypes = [vp, i32, vp]
         _lib.sgo_tag_boundaries.argtypes = [vp, i32]
+        _lib.sgo_remove_boxes.argtypes = [vp, i64, vp]
         f = C.c_float
         _lib.sgo_heat7.argtypes = [vp, i32, i32, f, vp]
         _lib.sgo_gs7.argtypes = [vp, i32, i32, i32, i32, f, f, f, f, f, vp]
@@ -174,6 +175,25 @@ class OracleGrid:
 
     def tag_boundaries(self, kind=NN_STAR):
         _lib.sgo_tag_boundaries(self._h, kind)
+
+    def remove_boxes(self, boxes):
+        """remove(box) for each box + removePoints; boxes [k, 6] = lo[3], hi[3] inclusive."""
+        b = np.ascontiguousarray(np.asarray(boxes, dtype=np.int64).reshape(-1, 6))
+        _lib.sgo_remove_boxes(self._h, len(b), _ptr(b))
+
+    def existing_points(self, box=None):
+        """Coordinates [k, 3] of the existing points in (chunk position, offset in the chunk)
+        order, optionally only those inside an inclusive box (lo, hi): the order of the
+        reference's SparseGridGpu iterators after deviceToHost."""
+        keys, _, mask = self.export()
+        n = len(keys)
+        idx = np.nonzero(mask[: n * self.bs] & 1)[0]
+        lin = keys[idx // self.bs] * self.bs + idx % self.bs
+        c = self.inv_lin(lin)
+        if box is not None:
+            lo, hi = np.asarray(box[0]), np.asarray(box[1])
+            c = c[np.all((c >= lo) & (c <= hi), axis=1)]
+        return c
 
     # -- stencils ----------------------------------------------------------
     @staticmethod

@@ -754,4 +754,31 @@ void sgo_gs7_f64(void* h, double* u, double* v, double* u2, double* v2, double D
     if (ua != u) { std::memcpy(u, ua, tot); std::memcpy(v, va, tot); }
 }
 
+// remove(box) + removePoints (src/SparseGridGpu/SparseGridGpu.hpp:3417-3489, 3528-3531;
+// SparseGridGpu_kernels.cuh:1235-1340): every existing point inside any of the
+// boxes gets mask byte 0; chunks stay.  The boxes are converted to unsigned int
+// as the reference's Box<dim, unsigned int> kernels do, so a negative lower
+// corner matches nothing and a negative upper corner matches everything above
+// the lower one.  boxes: nb x {lo[3], hi[3]}, inclusive.
+void sgo_remove_boxes(void* h, int64_t nb, const int64_t* boxes) {
+    Grid* g = (Grid*)h;
+    for (int64_t i = 0; i < g->n(); ++i) {
+        for (int o = 0; o < g->bs; ++o) {
+            uint8_t& m = g->mask[(size_t)i * g->bs + o];
+            if (!(m & 1)) continue;
+            int64_t c[3] = {0, 0, 0};
+            inv_lin(*g, g->keys[i] * g->bs + o, c);
+            for (int64_t k = 0; k < nb; ++k) {
+                bool in = true;
+                for (int d = 0; d < g->dim; ++d) {
+                    const uint32_t lo = (uint32_t)boxes[k * 6 + d], hi = (uint32_t)boxes[k * 6 + 3 + d];
+                    const uint32_t p = (uint32_t)c[d];
+                    in = in && p >= lo && p <= hi;
+                }
+                if (in) m = 0;
+            }
+        }
+    }
+}
+
 }  // extern "C"

@@ -297,6 +297,28 @@ int main() {
     HostMap Q = download(grid.handle(), 6);
     CHECK(same(Q, 2, Q, 3, active), "conv3x3x3_vs_conv_nnfull");
 
+    // ---------------------------------------------------------------- removePoints + iterator
+    {
+        const auto before = grid.existingPoints();
+        Box<3, int> rb;
+        for (int d = 0; d < 3; ++d) rb.setLow(d, 20), rb.setHigh(d, 35);
+        grid.remove(rb);
+        grid.removePoints(ctx);
+        const auto after = grid.existingPoints();
+        size_t inside = 0;
+        for (const auto& k : before) {
+            bool in = true;
+            for (int d = 0; d < 3; ++d) in = in && k.get(d) >= 20 && k.get(d) <= 35;
+            inside += in;
+        }
+        const auto sub = grid.existingPoints(grid_key_dx<3>({0, 0, 0}), grid_key_dx<3>({15, 63, 63}));
+        bool sub_ok = true;
+        for (const auto& k : sub) sub_ok = sub_ok && k.get(0) <= 15;
+        CHECK(before.size() == npts && inside > 0 && after.size() == npts - inside &&
+                  grid.countExistingElements() == after.size() && sub_ok && !sub.empty(),
+              "removePoints_and_iterator");
+    }
+
     int st = sgb_check_device_errors(grid.handle(), nullptr);
     CHECK(st == SGB_OK, "device_error_word_clear");
     std::printf("%s: %d failure(s)\n", g_fail ? "FAILED" : "PASSED", g_fail);
