@@ -22,6 +22,7 @@
 
 #include <cuda_runtime.h>
 
+#include <array>
 #include <cstdint>
 #include <cstring>
 #include <stdexcept>
@@ -76,6 +77,51 @@ struct Box {
 namespace gpu {
 struct ofp_context_t {};
 }  // namespace gpu
+
+// The sub-grid iterator's box (SparseGridGpu_iterator_sub): inclusive start / stop.
+template <unsigned dim>
+struct SparseGridGpu_iterator_sub {
+    grid_key_dx<dim> start, stop;
+    const grid_key_dx<dim>& getStart() const { return start; }
+    const grid_key_dx<dim>& getStop() const { return stop; }
+};
+
+// Byte offsets into a pack buffer (the reference's Pack_stat / Unpack_stat).
+struct Pack_stat {
+    size_t off = 0;
+    size_t getOffset() const { return off; }
+};
+struct Unpack_stat {
+    size_t off = 0;
+    size_t getOffset() const { return off; }
+    void addOffset(size_t b) { off += b; }
+};
+
+// A device byte buffer standing in for ExtPreAlloc<CudaMemory>.
+class CudaMemory {
+   public:
+    CudaMemory() = default;
+    CudaMemory(const CudaMemory&) = delete;
+    CudaMemory& operator=(const CudaMemory&) = delete;
+    ~CudaMemory() {
+        if (p_) cudaFree(p_);
+    }
+    bool resize(size_t n) {
+        if (n <= sz_) return true;
+        void* q = nullptr;
+        if (cudaMalloc(&q, n) != cudaSuccess) return false;
+        if (p_) cudaFree(p_);
+        p_ = q;
+        sz_ = n;
+        return true;
+    }
+    void* getDevicePointer() const { return p_; }
+    size_t size() const { return sz_; }
+
+   private:
+    void* p_ = nullptr;
+    size_t sz_ = 0;
+};
 
 enum flush_type { FLUSH_ON_HOST = 0, FLUSH_ON_DEVICE = 1 };
 enum StencilMode { STENCIL_MODE_INPLACE = 1, STENCIL_MODE_INPLACE_NO_SHARED = 3 };
@@ -550,6 +596,78 @@ class SparseGridGpu {
         return existing_points_impl(b);
     }
 
+    // getIterator(start, stop): the sub-grid iterator of the inclusive box
+    SparseGridGpu_iterator_sub<dim> getIterator(const grid_key_dx<dim>& start, const grid_key_dx<dim>& stop) const {
+        return SparseGridGpu_iterator_sub<dim>{start, stop};
+    }
+
+    // ---- ghost-exchange packing (SparseGridGpu.hpp:3041-3370 pack side, 1420-1615 and 3665-3750 unpack)
+    void packReset() { pack_subs_.clear(); }
+
+    // packRequest(sub_it, req): queue the box; the size comes with packCalculate
+    template <int... prp>
+    void packRequest(const SparseGridGpu_iterator_sub<dim>& sub_it, size_t&) {
+        pack_subs_.push_back(sub_it);
+    }
+
+    // packCalculate<prp...>(req, ctx): req += bytes to pack the queued boxes with prp...
+    template <int... prp>
+    void packCalculate(size_t& req, gpu::ofp_context_t&) {
+        const int props[] = {prp..., 0};
+        const std::vector<int64_t> b = pack_rows();
+        std::vector<int64_t> sizes(pack_subs_.size());
+        if (!sizes.empty())
+            check(sgb_pack_request(g_, (int64_t)sizes.size(), b.data(), (int)sizeof...(prp), props, sizes.data(),
+                                   nullptr),
+                  "packCalculate");
+        for (int64_t v : sizes) req += (size_t)v;
+    }
+
+    // pack<prp...>(mem, sub_it, sts): in the reference this only queues; the
+    // bytes are written by packFinalize, here too
+    template <int... prp>
+    void pack(CudaMemory&, const SparseGridGpu_iterator_sub<dim>&, Pack_stat&) {}
+
+    // packFinalize<prp...>(mem, sts): pack every queued box, back to back from sts's offset
+    template <int... prp>
+    void packFinalize(CudaMemory& mem, Pack_stat& sts, int = 0, bool = false) {
+        const int props[] = {prp..., 0};
+        const std::vector<int64_t> b = pack_rows();
+        int64_t written = 0;
+        check(sgb_pack(g_, (int64_t)pack_subs_.size(), b.data(), (int)sizeof...(prp), props,
+                       (unsigned char*)mem.getDevicePointer() + sts.off, (int64_t)(mem.size() - sts.off), &written,
+                       nullptr),
+              "packFinalize");
+        sts.off += (size_t)written;
+    }
+
+    // removeAddUnpackReset / unpack / removeAddUnpackFinalize: remove(box)
+    // sections, unpack one packed box per call into the box of sub_it, then
+    // apply the removals and merge the unpacked points
+    void removeAddUnpackReset() { rem_sects_.clear(); }
+
+    template <unsigned... prp>
+    void unpack(CudaMemory& mem, const SparseGridGpu_iterator_sub<dim>& sub_it, Unpack_stat& ps,
+                gpu::ofp_context_t&) {
+        const int props[] = {(int)prp..., 0};
+        int64_t start[3] = {0, 0, 0};
+        for (unsigned d = 0; d < dim; ++d) start[d] = sub_it.getStart().get(d);
+        int64_t used = 0;
+        check(sgb_unpack(g_, (const unsigned char*)mem.getDevicePointer() + ps.off, (int64_t)(mem.size() - ps.off),
+                         (int)sizeof...(prp), props, start, &used, nullptr),
+              "unpack");
+        ps.addOffset((size_t)used);
+    }
+
+    template <unsigned... prp>
+    void removeAddUnpackFinalize(gpu::ofp_context_t& ctx, int) {
+        removePoints(ctx);
+        std::array<int, 8> ops{};
+        const int listed[] = {(int)prp..., -1};
+        for (int k = 0; k < (int)sizeof...(prp); ++k) ops[listed[k]] = SGB_OP_RIGHT;
+        check(sgb_flush(g_, ops.data(), nullptr), "removeAddUnpackFinalize");
+    }
+
     size_t countExistingElements() const {
         int64_t e = 0;
         check(sgb_count_existing(g_, &e, nullptr, nullptr), "countExistingElements");
@@ -582,6 +700,16 @@ class SparseGridGpu {
 
    private:
     std::vector<Box<dim, int>> rem_sects_;
+    std::vector<SparseGridGpu_iterator_sub<dim>> pack_subs_;
+
+    std::vector<int64_t> pack_rows() const {
+        std::vector<int64_t> b;
+        for (const auto& it : pack_subs_) {
+            for (unsigned d = 0; d < 3; ++d) b.push_back(d < dim ? (int64_t)it.getStart().get(d) : 0);
+            for (unsigned d = 0; d < 3; ++d) b.push_back(d < dim ? (int64_t)it.getStop().get(d) : 0);
+        }
+        return b;
+    }
 
     std::vector<grid_key_dx<dim, int>> existing_points_impl(const int64_t* box) const {
         int64_t cnt = 0;

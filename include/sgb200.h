@@ -205,6 +205,43 @@ int sgb_remove_boxes(sgb_grid* g, int64_t nboxes, const int64_t* boxes_host, sgb
 int sgb_existing_points(sgb_grid* g, const int64_t* box_host, int32_t* coords_dev, int64_t capacity,
                         int64_t* count, sgb_stream s);
 
+/* Packing of sub-boxes for ghost exchange, in the reference's packed-box
+ * format (packRequest + packCalculate, pack + packFinalize, unpack:
+ * SparseGridGpu.hpp:3041-3210, 3244-3370, 1420-1615, 3665-3750).  One packed
+ * box, every section padded to 8 bytes:
+ *   uint64 n_cnk; int32 start[3] (box lower corner); int32 size[3] (grid size);
+ *   int64 chunk_id[n_cnk]; uint32 scan[n_cnk + 1] (scan[n_cnk] = n_pnt);
+ *   per packed property in the given order: n_pnt elements of its type;
+ *   int16 offset[n_pnt] (offset in the chunk); uint8 mask[n_pnt].
+ * A reference property of array type T[N] is N consecutive properties here,
+ * whose blocks sit back to back like the reference's component-major block.
+ * Packed points are the existing points inside the inclusive box, chunks in
+ * index order; inside a chunk the points are in offset order (the reference
+ * writes them in atomic-counter order, any order).  3-D grids; each call
+ * synchronises the stream.
+ *
+ * sgb_pack_request: bytes_host[k] = size of box k packed with props. */
+int sgb_pack_request(sgb_grid* g, int64_t nboxes, const int64_t* boxes_host, int nprops, const int* props,
+                     int64_t* bytes_host, sgb_stream s);
+
+/* Pack the boxes back to back into out_dev (8-byte aligned, capacity bytes;
+ * SGB_ERANGE if smaller than the summed request).  Padding bytes are zero. */
+int sgb_pack(sgb_grid* g, int64_t nboxes, const int64_t* boxes_host, int nprops, const int* props, void* out_dev,
+             int64_t capacity, int64_t* bytes_written, sgb_stream s);
+
+/* unpack of ONE packed box at buf_dev (8-byte aligned, nbytes readable):
+ * stages its points as inserts at packed coordinate - packed start +
+ * start_host (start_host NULL: at the packed coordinate), with the packed
+ * values for props (the properties the box was packed with, same order) and
+ * the background for the others.  *consumed = the box's size, the offset of
+ * the next box.  The packing grid must have this grid's chunk edge.  Points
+ * that land outside the domain fail the next flush like out-of-domain
+ * inserts.  removeAddUnpackFinalize<prp...> is sgb_flush with SGB_OP_RIGHT
+ * for the unpacked properties and SGB_OP_NONE for the others; sgb_remove_boxes
+ * before the unpacks plays the queued remove(box). */
+int sgb_unpack(sgb_grid* g, const void* buf_dev, int64_t nbytes, int nprops, const int* props,
+               const int64_t* start_host, int64_t* consumed, sgb_stream s);
+
 /* countExistingElements / countBoundaryElements (SparseGridGpu.hpp:2422-2474). */
 int sgb_count_existing(sgb_grid* g, int64_t* existing, int64_t* padding, sgb_stream s);
 

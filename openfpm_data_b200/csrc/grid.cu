@@ -92,7 +92,7 @@ __global__ void k_fill(unsigned char* dst, int64_t count, int esize, uint64_t pa
     }
 }
 
-static int fill(void* dst, int64_t count, int esize, uint64_t pattern, cudaStream_t s) {
+int fill(void* dst, int64_t count, int esize, uint64_t pattern, cudaStream_t s) {
     if (count <= 0) return SGB_OK;
     int64_t blocks = (count + 255) / 256;
     if (blocks > 4096) blocks = 4096;

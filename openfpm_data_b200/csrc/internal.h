@@ -159,6 +159,8 @@ int sanitize_prop(sgb_grid* g, int p, cudaStream_t s);
 // fill every point (n + 1 chunks) of property p with its background
 int fill_background_all(sgb_grid* g, int p, cudaStream_t s);
 int ensure_clean(sgb_grid* g, int p, cudaStream_t s);
+// fill count elements of esize bytes with the low esize bytes of pattern
+int fill(void* dst, int64_t count, int esize, uint64_t pattern, cudaStream_t s);
 // the background of property p as an element_size-byte pattern
 uint64_t bck_pattern(const sgb_grid* g, int p);
 int write_background(sgb_grid* g, int64_t pos, cudaStream_t s, DevBuf* data, DevBuf& mask);

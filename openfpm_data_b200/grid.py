@@ -275,6 +275,70 @@ class SparseGridGpu:
         for p in self.existing_points(box).cpu().numpy():
             yield tuple(int(v) for v in p)
 
+    # ---------------------------------------------------------------- pack / unpack
+    def packReset(self) -> None:
+        """Forget the queued pack boxes."""
+        self._pack = []
+
+    def packRequest(self, box) -> None:
+        """Queue an inclusive box ((lo), (hi)) to pack (packRequest(sub_it, req))."""
+        lo, hi = box
+        self._pack = getattr(self, "_pack", []) + [list(lo) + list(hi)]
+
+    def packCalculate(self, props: Sequence[int], stream=None) -> int:
+        """Bytes needed to pack the queued boxes with the listed properties."""
+        return int(sum(self.pack_sizes(getattr(self, "_pack", []), props, stream)))
+
+    def pack_sizes(self, boxes, props: Sequence[int], stream=None) -> list:
+        b = np.ascontiguousarray(np.asarray(boxes, dtype=np.int64).reshape(-1, 6))
+        out = np.zeros(len(b), dtype=np.int64)
+        if len(b):
+            L.check(self._lib.sgb_pack_request(self._h, len(b), b.ctypes.data_as(C.c_void_p), len(props),
+                                               _i32arr(list(props)), out.ctypes.data_as(C.c_void_p),
+                                               _stream(stream)), "sgb_pack_request")
+        return [int(x) for x in out]
+
+    def packFinalize(self, buf: torch.Tensor, props: Sequence[int], stream=None) -> int:
+        """Pack the queued boxes into the uint8 device tensor buf; returns the bytes written."""
+        boxes = getattr(self, "_pack", [])
+        return self.pack_boxes(boxes, props, buf, stream)
+
+    def pack_boxes(self, boxes, props: Sequence[int], buf: Optional[torch.Tensor] = None, stream=None):
+        """Pack the inclusive boxes [k, 6] (lo, hi) into buf (allocated when None; then the tensor
+        is returned, else the bytes written)."""
+        b = np.ascontiguousarray(np.asarray(boxes, dtype=np.int64).reshape(-1, 6))
+        ret_buf = buf is None
+        if buf is None:
+            buf = torch.empty(sum(self.pack_sizes(b, props, stream)), dtype=torch.uint8,
+                              device=f"cuda:{self.device}")
+        written = C.c_int64(0)
+        L.check(self._lib.sgb_pack(self._h, len(b), b.ctypes.data_as(C.c_void_p), len(props),
+                                   _i32arr(list(props)), buf.data_ptr() if buf.numel() else None, buf.numel(),
+                                   C.byref(written), _stream(stream)), "sgb_pack")
+        return buf if ret_buf else written.value
+
+    def unpack(self, buf: torch.Tensor, props: Sequence[int], start=None, offset: int = 0, stream=None) -> int:
+        """unpack one packed box at byte offset of buf into the box starting at start (None: its
+        packed place); the points are staged until removeAddUnpackFinalize.  Returns the offset
+        of the next box (Unpack_stat)."""
+        st = None if start is None else (C.c_int64 * 3)(*[int(v) for v in start])
+        used = C.c_int64(0)
+        L.check(self._lib.sgb_unpack(self._h, buf.data_ptr() + offset, buf.numel() - offset, len(props),
+                                     _i32arr(list(props)), st, C.byref(used), _stream(stream)), "sgb_unpack")
+        return offset + used.value
+
+    def removeAddUnpackReset(self) -> None:
+        self._rem = []
+
+    def removeAddUnpackFinalize(self, props: Sequence[int], stream=None) -> None:
+        """Apply the queued removals, then merge the unpacked points: their unpacked properties are
+        overwritten, the others keep their values (background for new points)."""
+        self.removePoints(stream)
+        ops = [L.OP_NONE] * len(self.ptypes)
+        for p in props:
+            ops[p] = L.OP_RIGHT
+        self.flush(ops, stream)
+
     def countExistingElements(self, stream=None) -> int:
         e = C.c_int64()
         L.check(self._lib.sgb_count_existing(self._h, C.byref(e), None, _stream(stream)), "sgb_count_existing")

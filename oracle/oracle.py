@@ -84,6 +84,14 @@ def _load():
     return _lib, _cpu
 
 
+def _up8(n: int) -> int:
+    return (n + 7) & ~7
+
+
+def _pad8(b: bytes) -> bytes:
+    return b + bytes(_up8(len(b)) - len(b))
+
+
 def _ptr(a: np.ndarray):
     return a.ctypes.data_as(C.c_void_p)
 
@@ -195,7 +203,76 @@ class OracleGrid:
             c = c[np.all((c >= lo) & (c <= hi), axis=1)]
         return c
 
+    # -- pack / unpack (SparseGridGpu.hpp:3041-3210 packRequest/packCalculate,
+    #    3244-3300 pack, 1293-1408 pack_sg_implement, 1420-1615 unpack) -----
+    def pack(self, boxes, props) -> bytes:
+        """The packed boxes back to back.  Per box (every section padded to 8 bytes):
+        uint64 n_cnk, int32 start[3] (box lower corner), int32 size[3] (grid size),
+        int64 chunk ids, uint32 scan[n_cnk + 1], per property its n_pnt values,
+        int16 offsets, uint8 masks (SparseGridGpu.hpp:3192-3200 size formula;
+        SparseGridGpu_kernels.cuh:1658-1697 pack_data).  Points: the existing points
+        inside the inclusive box (Box<dim,int>::isInside, kernels.cuh:1388-1399), chunks
+        in index order, points in offset order inside a chunk."""
+        keys, data, mask = self.export()
+        n = len(keys)
+        idx = np.nonzero(mask[: n * self.bs] & 1)[0]
+        lin = keys[idx // self.bs] * self.bs + idx % self.bs
+        c = self.inv_lin(lin) if len(lin) else np.zeros((0, 3), dtype=np.int64)
+        out = bytearray()
+        for b in np.asarray(boxes, dtype=np.int64).reshape(-1, 6):
+            sel = np.all((c >= b[:3]) & (c <= b[3:]), axis=1)
+            pidx = idx[sel]
+            cpos = pidx // self.bs
+            ids, first = np.unique(cpos, return_index=True)
+            n_cnk, n_pnt = len(ids), len(pidx)
+            sec = [np.array([n_cnk], dtype="<u8").tobytes(),
+                   np.array(list(b[:3]) + list(self.size), dtype="<i4").tobytes(),
+                   keys[ids].astype("<i8").tobytes(),
+                   _pad8(np.array(list(first) + [n_pnt], dtype="<u4").tobytes()),
+                   _pad8(b"".join(data[p][pidx].tobytes() for p in props)),
+                   _pad8((pidx % self.bs).astype("<i2").tobytes()),
+                   _pad8(mask[pidx].tobytes())]
+            out += b"".join(sec)
+        return bytes(out)
+
+    def unpack(self, buf, props, starts=None):
+        """Parse the packed boxes of buf (packed with props) and return, per box, the
+        points at packed coordinate - packed start + starts[k] (starts None: in place)
+        and their values: [(coords [m, 3], [values_p])]."""
+        es = [np.dtype(_NP[self.ptypes[p]]).itemsize for p in props]
+        res, pos, k = [], 0, 0
+        buf = bytes(buf)
+        while pos < len(buf):
+            n_cnk = int(np.frombuffer(buf, "<u8", 1, pos)[0])
+            hdr = np.frombuffer(buf, "<i4", 6, pos + 8).astype(np.int64)
+            q = pos + 32
+            ids = np.frombuffer(buf, "<i8", n_cnk, q)
+            q += 8 * n_cnk
+            scan = np.frombuffer(buf, "<u4", n_cnk + 1, q)
+            n_pnt = int(scan[-1])
+            q += _up8(4 * (n_cnk + 1))
+            vals = []
+            for p, e in zip(props, es):
+                vals.append(np.frombuffer(buf, _NP[self.ptypes[p]], n_pnt, q).copy())
+                q += n_pnt * e
+            q = pos + 32 + 8 * n_cnk + _up8(4 * (n_cnk + 1)) + _up8(n_pnt * sum(es))
+            offs = np.frombuffer(buf, "<i2", n_pnt, q).astype(np.int64)
+            q += _up8(2 * n_pnt)
+            q += _up8(n_pnt)
+            chunk = np.repeat(np.arange(n_cnk), np.diff(scan.astype(np.int64)))
+            bsz = [(int(s) + self.edge - 1) // self.edge for s in hdr[3:]]
+            key = ids[chunk]
+            org = np.stack([key % bsz[0], (key // bsz[0]) % bsz[1], key // (bsz[0] * bsz[1])], axis=1) * self.edge
+            e = self.edge
+            coords = org + np.stack([offs % e, (offs // e) % e, offs // (e * e)], axis=1)
+            if starts is not None:
+                coords = coords - hdr[:3] + np.asarray(starts[k], dtype=np.int64)
+            res.append((coords, vals))
+            pos, k = q, k + 1
+        return res
+
     # -- stencils ----------------------------------------------------------
+
     @staticmethod
     def _box(box):
         if box is None:

@@ -319,6 +319,51 @@ int main() {
               "removePoints_and_iterator");
     }
 
+    // ---------------------------------------------------------------- pack / unpack (ghost exchange)
+    {
+        // SparseGridGpu_tests.cu:1533-1700: pack two sub-boxes with properties 0 and 1,
+        // unpack them into another grid, the first one shifted by +3 in x
+        const grid_key_dx<3> a0({8, 10, 12}), a1({30, 40, 33}), b0({36, 0, 0}), b1({50, 63, 63});
+        auto it1 = grid.getIterator(a0, a1);
+        auto it2 = grid.getIterator(b0, b1);
+        size_t req = 0;
+        grid.packReset();
+        grid.packRequest<0, 1>(it1, req);
+        grid.packRequest<0, 1>(it2, req);
+        grid.packCalculate<0, 1>(req, ctx);
+        CudaMemory mem;
+        mem.resize(req);
+        Pack_stat sts;
+        grid.pack<0, 1>(mem, it1, sts);
+        grid.pack<0, 1>(mem, it2, sts);
+        grid.packFinalize<0, 1>(mem, sts);
+
+        Grid6 dst(sz);
+        dst.setBackgroundValue<0>(0.0f);
+        Unpack_stat ps;
+        dst.removeAddUnpackReset();
+        auto d1 = dst.getIterator(grid_key_dx<3>({11, 10, 12}), grid_key_dx<3>({33, 40, 33}));
+        auto d2 = dst.getIterator(b0, b1);
+        dst.remove(Box<3, int>{{11, 10, 12}, {33, 40, 33}});
+        dst.unpack<0, 1>(mem, d1, ps, ctx);
+        dst.remove(Box<3, int>{{36, 0, 0}, {50, 63, 63}});
+        dst.unpack<0, 1>(mem, d2, ps, ctx);
+        dst.removeAddUnpackFinalize<0, 1>(ctx, 0);
+
+        const auto s1 = grid.existingPoints(a0, a1), s2 = grid.existingPoints(b0, b1);
+        grid.deviceToHost<0, 1>();
+        dst.deviceToHost<0, 1>();
+        bool vals_ok = true;
+        for (const auto& k : s1) {
+            const grid_key_dx<3, int> t({k.get(0) + 3, k.get(1), k.get(2)});
+            vals_ok = vals_ok && dst.get<0>(t) == grid.get<0>(k) && dst.get<1>(t) == grid.get<1>(k);
+        }
+        for (const auto& k : s2) vals_ok = vals_ok && dst.get<0>(k) == grid.get<0>(k) && dst.get<1>(k) == grid.get<1>(k);
+        CHECK(req > 0 && sts.getOffset() == req && ps.getOffset() == req && !s1.empty() && !s2.empty() && vals_ok &&
+                  dst.countExistingElements() == s1.size() + s2.size(),
+              "pack_unpack");
+    }
+
     int st = sgb_check_device_errors(grid.handle(), nullptr);
     CHECK(st == SGB_OK, "device_error_word_clear");
     std::printf("%s: %d failure(s)\n", g_fail ? "FAILED" : "PASSED", g_fail);
