@@ -44,7 +44,7 @@ UNIT = "Gpts/s"
 ALG_BYTES_PER_PT = 17
 # the library's default launch configuration of the pipelined 8^3 kernel (automatic ring depth)
 DEFAULT_CTAS_PER_SM, DEFAULT_STAGES = "auto", "auto"
-WORKLOADS = ("gs512", "heat128", "insert1024", "batched256", "served")
+WORKLOADS = ("gs512", "heat128", "insert1024", "batched256", "served", "ghost512")
 
 
 def parse():
@@ -606,6 +606,143 @@ def run_served(args, dist: Dist):
                  gpu_launches=None, clocks=clk)
 
 
+def _ghost_boxes(size=512, width=1):
+    """The six ghost slabs of a 2x2x2 decomposition of the 512^3 grid: for each
+    mid-plane, the `width` layers on either side of it (inclusive boxes)."""
+    m, hi = size // 2, size - 1
+    boxes = []
+    for a in range(3):
+        for lo_a, hi_a in ((m - width, m - 1), (m, m + width - 1)):
+            lo, up = [0, 0, 0], [hi, hi, hi]
+            lo[a], up[a] = lo_a, hi_a
+            boxes.append(lo + up)
+    return np.array(boxes, dtype=np.int64)
+
+
+def run_ghost512(args, dist: Dist):
+    """Ghost exchange on the Gray-Scott 512^3 grid: one step packs the six
+    1-point ghost slabs around the three mid-planes (fields u, v), unpacks
+    them into a second grid at the same place and merges them
+    (removeAddUnpackFinalize).  Value: exchanged points per second."""
+    import torch
+
+    import openfpm_data_b200 as sgb
+    from openfpm_data_b200 import workloads as W
+    torch.cuda.set_device(dist.local)
+    nsteps = args.steps if args.steps <= 500 else 100
+    nwarm = max(3, min(args.warmup, 10))
+    ps = W.gray_scott()
+    keys, data, mask = W.build_block_map(ps.coords, ps.values, ps.size, 8, ps.bck)
+    grids = []
+    for _ in range(2):
+        g = sgb.SparseGridGpu(ps.size, ["f32"] * 4, edge=8, device=dist.local)
+        for p, b in enumerate([1.0, 0.0, 1.0, 0.0]):
+            g.setBackgroundValue(p, b)
+        g.load_map(keys, data + [d.copy() for d in data], mask)
+        grids.append(g)
+    a, b = grids
+    boxes = _ghost_boxes()
+    props = [0, 1]
+    sizes = a.pack_sizes(boxes, props)
+    buf = torch.empty(sum(sizes), dtype=torch.uint8, device=f"cuda:{dist.local}")
+    starts = [tuple(int(v) for v in bx[:3]) for bx in boxes]
+    phases = {"pack": 0.0, "unpack": 0.0, "merge": 0.0}
+    recorded = []
+
+    def one(timed):
+        ev = [_events()[0] for _ in range(4)]
+        ev[0].record()
+        a.pack_boxes(boxes, props, buf)
+        ev[1].record()
+        off = 0
+        for st in starts:
+            off = b.unpack(buf, props, st, off)
+        ev[2].record()
+        b.removeAddUnpackFinalize(props)
+        ev[3].record()
+        if timed:
+            recorded.append(ev)
+
+    for _ in range(nwarm):
+        one(False)
+    torch.cuda.synchronize()
+    # packed points and chunks per step, from the buffer's headers
+    hb = buf.cpu().numpy().tobytes()
+    npnt = ncnk = 0
+    pos = 0
+    for sz in sizes:
+        nc = int(np.frombuffer(hb, "<u8", 1, pos)[0])
+        npnt += int(np.frombuffer(hb, "<u4", 1, pos + 32 + 12 * nc)[0])
+        ncnk += nc
+        pos += sz
+    clocks = ClockSampler(dist.local)
+    dist.barrier()
+    e0, e1 = _events()
+    e0.record()
+    for _ in range(nsteps):
+        one(True)
+    e1.record()
+    torch.cuda.synchronize()
+    dist.barrier()
+    clk = clocks.stop()
+    for ev in recorded:
+        for k, name in enumerate(phases):
+            phases[name] += ev[k].elapsed_time(ev[k + 1]) / 1e3
+    a.check_device_errors()
+    b.check_device_errors()
+    t = dist.max(e0.elapsed_time(e1) / 1e3)
+    value = dist.world * npnt * nsteps / t / 1e6
+    # pack roofline: the touched chunks' masks once, the packed values read, the packed bytes written
+    alg = 512 * ncnk + 8 * npnt + sum(sizes)
+    peak, pk = _peak_hbm()
+    ach = alg * nsteps / phases["pack"] / 1e9
+    roof = {"bound": "hbm", "kernel": "pack (count + scans + emit, one call)", "achieved": round(ach, 1),
+            "peak": peak, "unit": "GB/s", "frac": round(ach / peak, 4), "traffic": None, "peak_kind": pk,
+            "alg_bytes_per_launch": alg}
+
+    # end to end: packed bytes to pinned host memory and back (the send / receive of a ghost exchange)
+    h_send = torch.empty(buf.numel(), dtype=torch.uint8).pin_memory()
+    rbuf = torch.empty_like(buf)
+    dist.barrier()
+    f0, f1 = _events()
+    f0.record()
+    for _ in range(nsteps):
+        a.pack_boxes(boxes, props, buf)
+        h_send.copy_(buf, non_blocking=True)
+        rbuf.copy_(h_send, non_blocking=True)
+        off = 0
+        for st in starts:
+            off = b.unpack(rbuf, props, st, off)
+        b.removeAddUnpackFinalize(props)
+    f1.record()
+    torch.cuda.synchronize()
+    t_e2e = dist.max(f0.elapsed_time(f1) / 1e3)
+    e2e = {"value": round(dist.world * npnt * nsteps / t_e2e / 1e6, 3), "unit": "Mpts/s",
+           "h2d_bytes_per_step": int(buf.numel()), "d2h_bytes_per_step": int(buf.numel()),
+           "step": "pack, packed buffer to pinned host memory and back, unpack, merge"}
+
+    cpu = None
+    if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
+        from oracle import oracle as O
+        O.build()
+        o = O.OracleGrid(ps.size, edge=8, ptypes=(O.T_F32,) * 4)
+        o.load_map(keys, data + [d.copy() for d in data], mask)
+        reps, t0 = 0, time.perf_counter()
+        while reps < 3 or (time.perf_counter() - t0 < 10 and reps < 50):
+            o.pack(boxes, props)
+            reps += 1
+        dtc = time.perf_counter() - t0
+        cpu = {"value": round(npnt * reps / dtc / 1e6, 3), "unit": "Mpts/s", "cores": 1, "kind": "port",
+               "sample": f"{reps} packs of the six slabs by the numpy oracle (pack only), {dtc:.1f} s"}
+    return _line("ghost exchange Mpts/s (pack + unpack + merge, six 1-point slabs of the Gray-Scott 512^3 grid)",
+                 round(value, 2), "Mpts/s", dist, args, nsteps, t,
+                 {"workload": "ghost_exchange_gray_scott_512^3_2x2x2_width1", "points_per_step": npnt,
+                  "chunks_packed_per_step": ncnk, "packed_bytes_per_step": int(sum(sizes)),
+                  "phase_seconds": {k: round(v, 5) for k, v in phases.items()},
+                  "l2": "grids 2 x 157 MiB > L2; the packed buffer (a few MB) stays in L2 between pack and unpack"},
+                 roofline=roof, cpu_baseline=cpu, e2e=e2e, gpu_launches=None, clocks=clk)
+
+
 def run_reference(args, dist: Dist):
     from openfpm_data_b200 import workloads as W
     if dist.rank != 0:
@@ -632,7 +769,7 @@ def main():
             line = run_reference(args, dist)
         else:
             runners = {"gs512": run_ours, "heat128": run_heat128, "insert1024": run_insert1024,
-                       "batched256": run_batched256, "served": run_served}
+                       "batched256": run_batched256, "served": run_served, "ghost512": run_ghost512}
             line = runners[args.workload](args, dist)
         if line is not None and dist.rank == 0:
             print(json.dumps(line), flush=True)

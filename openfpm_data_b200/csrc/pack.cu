@@ -30,7 +30,7 @@ static inline int64_t pad8(int64_t b) { return (b + 7) & ~(int64_t)7; }
 
 struct PackLayout {
     int64_t n_cnk, n_pnt;
-    int64_t off_ids, off_scan, off_data, off_offs, off_mask, bytes;
+    int64_t off_ids, off_scan, off_data, off_offs, off_mask, bytes, data_bytes;
     int64_t prop_off[kMaxProps];
 };
 
@@ -49,6 +49,7 @@ static PackLayout layout_of(int64_t n_cnk, int64_t n_pnt, int np, const int* es)
         L.prop_off[p] = d;
         d += n_pnt * es[p];
     }
+    L.data_bytes = d;
     o += pad8(d);
     L.off_offs = o;
     o += pad8(2 * n_pnt);
@@ -72,72 +73,147 @@ __device__ __forceinline__ bool inside6(const Box6& bx, int64_t x, int64_t y, in
     return x >= bx.b[0] && x <= bx.b[3] && y >= bx.b[1] && y <= bx.b[4] && z >= bx.b[2] && z <= bx.b[5];
 }
 
-// Existing points of each chunk inside the box, and whether the chunk has any.
+// Does the chunk at origin o (edge e) meet the box?
+__device__ __forceinline__ bool chunk_meets(const Box6& bx, const int64_t* o, int e) {
+    return o[0] <= bx.b[3] && o[0] + e - 1 >= bx.b[0] && o[1] <= bx.b[4] && o[1] + e - 1 >= bx.b[1] &&
+           o[2] <= bx.b[5] && o[2] + e - 1 >= bx.b[2];
+}
+
+// Counts for all boxes in one pass: cnt[k * (n + 1) + c] = existing points of
+// chunk c inside box k, flg[...] = (cnt != 0).  Both arrays are zeroed by the
+// caller (row entries c = n stay 0 so that one scan over all rows gives every
+// box's offsets).  One warp per chunk; boxes the chunk does not meet cost no
+// mask read.
 __global__ void k_pack_count(const int64_t* __restrict__ keys, int64_t n, Geometry geo, const uint8_t* __restrict__ mask,
-                             Box6 box, uint32_t* counts, uint32_t* flags) {
+                             const Box6* __restrict__ boxes, int nb, uint32_t* cnt, uint32_t* flg) {
     const int lane = threadIdx.x & 31;
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
     const int bs = geo.bs, e = geo.edge;
     for (int64_t c = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; c < n; c += nw) {
         int64_t o[3];
         origin_of(geo, keys[c], o);
-        uint32_t cnt = 0;
-        for (int pt = lane; pt < bs; pt += 32) {
-            const bool in = (mask[c * bs + pt] & 1) && inside6(box, o[0] + pt % e, o[1] + (pt / e) % e, o[2] + pt / (e * e));
-            cnt += __popc(__ballot_sync(0xffffffffu, in));
-        }
-        if (lane == 0) {
-            counts[c] = cnt;
-            flags[c] = cnt != 0;
+        for (int k = 0; k < nb; ++k) {
+            const Box6 bx = boxes[k];
+            if (!chunk_meets(bx, o, e)) continue;  // uniform over the warp
+            uint32_t t = 0;
+            for (int pt = lane; pt < bs; pt += 32) {
+                const bool in = (mask[c * bs + pt] & 1) && inside6(bx, o[0] + pt % e, o[1] + (pt / e) % e, o[2] + pt / (e * e));
+                t += __popc(__ballot_sync(0xffffffffu, in));
+            }
+            if (lane == 0 && t) {
+                cnt[(int64_t)k * (n + 1) + c] = t;
+                flg[(int64_t)k * (n + 1) + c] = 1;
+            }
         }
     }
+}
+
+// Row starts of the two scans (box k's first point / chunk) for k = 0..nb.
+__global__ void k_pack_rows(const uint32_t* __restrict__ scnt, const uint32_t* __restrict__ sflg, int64_t n, int nb,
+                            uint32_t* out) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k > nb) return;
+    out[2 * k] = scnt[(int64_t)k * (n + 1)];
+    out[2 * k + 1] = sflg[(int64_t)k * (n + 1)];
 }
 
 struct PackProps {
     const unsigned char* src[kMaxProps];
     int es[kMaxProps];
-    int64_t off[kMaxProps];  // byte offset of the property's block inside the data block
+    int wide[kMaxProps];  // 1: the property's packed block is aligned to its element size
     int np;
 };
 
+// One packed box: its place in the output, its layout, its box.
+struct PackBox {
+    Box6 box;
+    int64_t base;  // byte offset of the box in the output
+    PackLayout L;
+    uint32_t pnt0, cnk0;  // the box's row starts in the scans
+};
+
+template <typename T>
+__device__ __forceinline__ void copy_elem(unsigned char* d, const unsigned char* s) {
+    *reinterpret_cast<T*>(d) = *reinterpret_cast<const T*>(s);
+}
+
 __global__ void k_pack_emit(const int64_t* __restrict__ keys, int64_t n, Geometry geo, const uint8_t* __restrict__ mask,
-                            Box6 box, const uint32_t* __restrict__ counts, const uint32_t* __restrict__ pt_off,
-                            const uint32_t* __restrict__ c_off, PackProps pp, unsigned char* out, PackLayout L) {
+                            const PackBox* __restrict__ pbs, int nb, const uint32_t* __restrict__ scnt,
+                            const uint32_t* __restrict__ sflg, PackProps pp, unsigned char* out) {
     const int lane = threadIdx.x & 31;
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
     const int bs = geo.bs, e = geo.edge;
-    int64_t* ids = reinterpret_cast<int64_t*>(out + L.off_ids);
-    uint32_t* scan = reinterpret_cast<uint32_t*>(out + L.off_scan);
-    int16_t* offs = reinterpret_cast<int16_t*>(out + L.off_offs);
-    uint8_t* msk = out + L.off_mask;
     for (int64_t c = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; c < n; c += nw) {
-        if (counts[c] == 0) continue;  // uniform over the warp
         const int64_t key = keys[c];
-        if (lane == 0) {
-            ids[c_off[c]] = key;
-            scan[c_off[c]] = pt_off[c];
-        }
         int64_t o[3];
         origin_of(geo, key, o);
-        uint32_t base = pt_off[c];
-        for (int pt = lane; pt < bs; pt += 32) {
-            const uint8_t m = mask[c * bs + pt];
-            const bool in = (m & 1) && inside6(box, o[0] + pt % e, o[1] + (pt / e) % e, o[2] + pt / (e * e));
-            const unsigned bal = __ballot_sync(0xffffffffu, in);
-            if (in) {
-                const int64_t j = base + __popc(bal & lanemask_lt());
-                const int64_t idx = c * bs + pt;
-                for (int p = 0; p < pp.np; ++p) {
-                    const int es = pp.es[p];
-                    unsigned char* d = out + L.off_data + pp.off[p] + j * es;
-                    const unsigned char* sp = pp.src[p] + idx * es;
-                    for (int b = 0; b < es; ++b) d[b] = sp[b];
-                }
-                offs[j] = (int16_t)pt;
-                msk[j] = m;
+        for (int k = 0; k < nb; ++k) {
+            const int64_t r = (int64_t)k * (n + 1) + c;
+            uint32_t base = scnt[r];
+            if (scnt[r + 1] == base) continue;  // no packed point of box k here (uniform)
+            const PackBox& P = pbs[k];
+            const Box6 bx = P.box;
+            unsigned char* b = out + P.base;
+            base -= P.pnt0;
+            const uint32_t slot = sflg[r] - P.cnk0;
+            if (lane == 0) {
+                reinterpret_cast<int64_t*>(b + P.L.off_ids)[slot] = key;
+                reinterpret_cast<uint32_t*>(b + P.L.off_scan)[slot] = base;
             }
-            base += __popc(bal);
+            int16_t* offs = reinterpret_cast<int16_t*>(b + P.L.off_offs);
+            uint8_t* msk = b + P.L.off_mask;
+            for (int pt = lane; pt < bs; pt += 32) {
+                const uint8_t m = mask[c * bs + pt];
+                const bool in = (m & 1) && inside6(bx, o[0] + pt % e, o[1] + (pt / e) % e, o[2] + pt / (e * e));
+                const unsigned bal = __ballot_sync(0xffffffffu, in);
+                if (in) {
+                    const int64_t j = base + __popc(bal & lanemask_lt());
+                    const int64_t idx = c * bs + pt;
+                    for (int p = 0; p < pp.np; ++p) {
+                        const int es = pp.es[p];
+                        unsigned char* d = b + P.L.off_data + P.L.prop_off[p] + j * es;
+                        const unsigned char* sp = pp.src[p] + idx * es;
+                        if (pp.wide[p] && es == 4) copy_elem<uint32_t>(d, sp);
+                        else if (pp.wide[p] && es == 8) copy_elem<uint64_t>(d, sp);
+                        else
+                            for (int q = 0; q < es; ++q) d[q] = sp[q];
+                    }
+                    offs[j] = (int16_t)pt;
+                    msk[j] = m;
+                }
+                base += __popc(bal);
+            }
         }
+    }
+}
+
+// Per box: the header, scan[n_cnk] = n_pnt, and zeros in the padding tails.
+__global__ void k_pack_finish(const PackBox* __restrict__ pbs, int nb, int32_t sx, int32_t sy, int32_t sz,
+                              unsigned char* out) {
+    const int k = blockIdx.x;
+    if (k >= nb) return;
+    const PackBox& P = pbs[k];
+    unsigned char* b = out + P.base;
+    const PackLayout& L = P.L;
+    const int t = threadIdx.x;
+    if (t == 0) {
+        *reinterpret_cast<uint64_t*>(b) = (uint64_t)L.n_cnk;
+        int32_t* h = reinterpret_cast<int32_t*>(b + 8);
+        h[0] = (int32_t)P.box.b[0];
+        h[1] = (int32_t)P.box.b[1];
+        h[2] = (int32_t)P.box.b[2];
+        h[3] = sx;
+        h[4] = sy;
+        h[5] = sz;
+        reinterpret_cast<uint32_t*>(b + L.off_scan)[L.n_cnk] = (uint32_t)L.n_pnt;
+    }
+    // tails: [end of section, next section) for scan, data, offsets, masks
+    const int64_t ends[4] = {L.off_scan + 4 * (L.n_cnk + 1), L.off_data + L.data_bytes, L.off_offs + 2 * L.n_pnt,
+                             L.off_mask + L.n_pnt};
+    const int64_t next[4] = {L.off_data, L.off_offs, L.off_mask, L.bytes};
+    if (t < 32) {
+        const int s = t >> 3, q = t & 7;
+        if (ends[s] + q < next[s]) b[ends[s] + q] = 0;
     }
 }
 
@@ -182,7 +258,7 @@ __global__ void k_unpack_stage(const unsigned char* __restrict__ buf, PackLayout
     out_lin[j] = lin;
     for (int p = 0; p < pp.np; ++p) {
         const int es = pp.es[p];
-        const unsigned char* s = buf + L.off_data + pp.off[p] + j * es;
+        const unsigned char* s = buf + L.off_data + L.prop_off[p] + j * es;
         for (int b = 0; b < es; ++b) dst.p[p][j * es + b] = s[b];
     }
 }
@@ -191,26 +267,39 @@ static unsigned wgrid(const sgb_grid* g, int64_t n) {
     return (unsigned)std::max<int64_t>(1, std::min<int64_t>((int64_t)g->num_sms * 8, (n + 7) / 8));
 }
 
-// Counts of one box: fills scratch[1] (counts), [2] (point offsets), [3] (flags), [4] (chunk offsets);
-// returns n_pnt and n_cnk.
-static int box_counts(sgb_grid* g, const Box6& box, int64_t* n_pnt, int64_t* n_cnk, cudaStream_t s) {
+// The counting pass over all boxes: row starts of the point and chunk scans
+// to rows[2 * (nb + 1)] (host), scans in scratch[2] / scratch[4].
+static int pack_counts(sgb_grid* g, int64_t nboxes, const int64_t* boxes_host, std::vector<uint32_t>& rows,
+                       cudaStream_t s) {
     const int64_t n = g->n;
-    *n_pnt = *n_cnk = 0;
-    if (n == 0) return SGB_OK;
-    for (int k = 1; k <= 4; ++k) SGB_TRY(g->scratch[k].ensure((size_t)(n + 1) * 4 + 16));
-    uint32_t *cnt = g->scratch[1].as<uint32_t>(), *poff = g->scratch[2].as<uint32_t>(),
-             *flg = g->scratch[3].as<uint32_t>(), *coff = g->scratch[4].as<uint32_t>();
-    k_pack_count<<<wgrid(g, n), 256, 0, s>>>(g->keys.as<int64_t>(), n, g->geo, g->mask.as<uint8_t>(), box, cnt, flg);
+    const int64_t len = nboxes * (n + 1);  // rows of n + 1 entries; the scans' totals land at [len]
+    rows.assign(2 * (nboxes + 1), 0);
+    if (nboxes == 0 || n == 0) return SGB_OK;
+    if (len >= (int64_t(1) << 31)) {
+        set_error("too many boxes x chunks in one pack call");
+        return SGB_ERANGE;
+    }
+    SGB_TRY(g->scratch[0].ensure((size_t)nboxes * sizeof(Box6)));
+    for (int k = 1; k <= 4; ++k) SGB_TRY(g->scratch[k].ensure((size_t)(len + 1) * 4 + 16));
+    const size_t hb = std::max<size_t>((size_t)nboxes * sizeof(Box6), rows.size() * 4);
+    SGB_TRY(g->hscratch.ensure(hb));
+    std::memcpy(g->hscratch.p, boxes_host, (size_t)nboxes * sizeof(Box6));
+    SGB_CUDA(cudaMemcpyAsync(g->scratch[0].p, g->hscratch.p, (size_t)nboxes * sizeof(Box6), cudaMemcpyHostToDevice, s));
+    uint32_t *cnt = g->scratch[1].as<uint32_t>(), *scnt = g->scratch[2].as<uint32_t>(),
+             *flg = g->scratch[3].as<uint32_t>(), *sflg = g->scratch[4].as<uint32_t>();
+    SGB_CUDA(cudaMemsetAsync(cnt, 0, (size_t)len * 4, s));
+    SGB_CUDA(cudaMemsetAsync(flg, 0, (size_t)len * 4, s));
+    k_pack_count<<<wgrid(g, n), 256, 0, s>>>(g->keys.as<int64_t>(), n, g->geo, g->mask.as<uint8_t>(),
+                                             g->scratch[0].as<Box6>(), (int)nboxes, cnt, flg);
     SGB_CUDA(cudaGetLastError());
-    SGB_TRY(scan_exclusive_u32(cnt, poff, n, poff + n, &g->scratch[6], s));
-    SGB_TRY(scan_exclusive_u32(flg, coff, n, coff + n, &g->scratch[6], s));
-    SGB_TRY(g->hscratch.ensure(64));
-    uint32_t* h = (uint32_t*)g->hscratch.p;
-    SGB_CUDA(cudaMemcpyAsync(h, poff + n, 4, cudaMemcpyDeviceToHost, s));
-    SGB_CUDA(cudaMemcpyAsync(h + 1, coff + n, 4, cudaMemcpyDeviceToHost, s));
+    SGB_TRY(scan_exclusive_u32(cnt, scnt, len, scnt + len, &g->scratch[6], s));
+    SGB_TRY(scan_exclusive_u32(flg, sflg, len, sflg + len, &g->scratch[6], s));
+    // the row starts go through scratch[1], which the scans no longer need
+    k_pack_rows<<<(unsigned)((nboxes + 1 + 127) / 128), 128, 0, s>>>(scnt, sflg, n, (int)nboxes, cnt);
+    SGB_CUDA(cudaGetLastError());
+    SGB_CUDA(cudaMemcpyAsync(g->hscratch.p, cnt, rows.size() * 4, cudaMemcpyDeviceToHost, s));
     SGB_CUDA(cudaStreamSynchronize(s));
-    *n_pnt = h[0];
-    *n_cnk = h[1];
+    std::memcpy(rows.data(), g->hscratch.p, rows.size() * 4);
     return SGB_OK;
 }
 
@@ -233,14 +322,10 @@ extern "C" int sgb_pack_request(sgb_grid* g, int64_t nboxes, const int64_t* boxe
     if (g->geo.dim != 3) return SGB_ENOTSUP;
     int es[kMaxProps];
     SGB_TRY(check_props(g, nprops, props, es));
-    cudaStream_t s = (cudaStream_t)stream;
-    for (int64_t k = 0; k < nboxes; ++k) {
-        Box6 box;
-        std::memcpy(box.b, boxes_host + k * 6, sizeof(box.b));
-        int64_t np_, nc_;
-        SGB_TRY(box_counts(g, box, &np_, &nc_, s));
-        bytes_host[k] = layout_of(nc_, np_, nprops, es).bytes;
-    }
+    std::vector<uint32_t> rows;
+    SGB_TRY(pack_counts(g, nboxes, boxes_host, rows, (cudaStream_t)stream));
+    for (int64_t k = 0; k < nboxes; ++k)
+        bytes_host[k] = layout_of(rows[2 * k + 3] - rows[2 * k + 1], rows[2 * k + 2] - rows[2 * k], nprops, es).bytes;
     return SGB_OK;
 }
 
@@ -248,61 +333,59 @@ extern "C" int sgb_pack(sgb_grid* g, int64_t nboxes, const int64_t* boxes_host, 
                         void* out_dev, int64_t capacity, int64_t* bytes_written, sgb_stream stream) {
     if (!g || nboxes < 0 || (nboxes > 0 && (!boxes_host || !out_dev)) || !bytes_written) return SGB_EINVAL;
     if (g->geo.dim != 3) return SGB_ENOTSUP;
-    int es[kMaxProps];
-    SGB_TRY(check_props(g, nprops, props, es));
     if ((uintptr_t)out_dev % 8 != 0) {
         set_error("the pack buffer must be 8-byte aligned");
         return SGB_EINVAL;
     }
-    cudaStream_t s = (cudaStream_t)stream;
-    unsigned char* out = (unsigned char*)out_dev;
-    int64_t pos = 0;
+    int es[kMaxProps];
+    SGB_TRY(check_props(g, nprops, props, es));
     *bytes_written = 0;
-    SGB_TRY(g->hscratch.ensure(64));
+    if (nboxes == 0) return SGB_OK;
+    cudaStream_t s = (cudaStream_t)stream;
+    std::vector<uint32_t> rows;
+    SGB_TRY(pack_counts(g, nboxes, boxes_host, rows, s));
+    std::vector<PackBox> pb((size_t)nboxes);
+    int64_t pos = 0;
+    bool any_points = false;
     for (int64_t k = 0; k < nboxes; ++k) {
-        Box6 box;
-        std::memcpy(box.b, boxes_host + k * 6, sizeof(box.b));
-        int64_t np_, nc_;
-        SGB_TRY(box_counts(g, box, &np_, &nc_, s));
-        const PackLayout L = layout_of(nc_, np_, nprops, es);
-        if (pos + L.bytes > capacity) {
-            set_error("the pack buffer is smaller than sgb_pack_request reported");
-            return SGB_ERANGE;
-        }
-        unsigned char* b = out + pos;
-        // header: n_cnk, start = the box's lower corner, size = the grid's size
-        unsigned char hdr[32];
-        const uint64_t ncu = (uint64_t)nc_;
-        std::memcpy(hdr, &ncu, 8);
-        for (int d = 0; d < 3; ++d) {
-            const int32_t st = (int32_t)box.b[d], sz = (int32_t)g->geo.size[d];
-            std::memcpy(hdr + 8 + 4 * d, &st, 4);
-            std::memcpy(hdr + 20 + 4 * d, &sz, 4);
-        }
-        std::memcpy(g->hscratch.p, hdr, 32);
-        SGB_CUDA(cudaMemcpyAsync(b, g->hscratch.p, 32, cudaMemcpyHostToDevice, s));
-        // zero the padding so packed buffers compare bytewise
-        SGB_CUDA(cudaMemsetAsync(b + 32, 0, L.bytes - 32, s));
-        if (np_ > 0) {
-            PackProps pp{};
-            pp.np = nprops;
-            for (int p = 0; p < nprops; ++p) {
-                pp.src[p] = g->data[props[p]].as<unsigned char>();
-                pp.es[p] = es[p];
-                pp.off[p] = L.prop_off[p];
-            }
-            k_pack_emit<<<wgrid(g, g->n), 256, 0, s>>>(g->keys.as<int64_t>(), g->n, g->geo, g->mask.as<uint8_t>(), box,
-                                                      g->scratch[1].as<uint32_t>(), g->scratch[2].as<uint32_t>(),
-                                                      g->scratch[4].as<uint32_t>(), pp, b, L);
-            SGB_CUDA(cudaGetLastError());
-        }
-        // scan[n_cnk] = n_pnt
-        const uint32_t npu = (uint32_t)np_;
-        std::memcpy((unsigned char*)g->hscratch.p + 32, &npu, 4);
-        SGB_CUDA(cudaMemcpyAsync(b + L.off_scan + 4 * nc_, (unsigned char*)g->hscratch.p + 32, 4, cudaMemcpyHostToDevice, s));
-        SGB_CUDA(cudaStreamSynchronize(s));  // the host staging is reused by the next box
-        pos += L.bytes;
+        PackBox& P = pb[k];
+        std::memcpy(P.box.b, boxes_host + 6 * k, sizeof(P.box.b));
+        P.pnt0 = rows[2 * k];
+        P.cnk0 = rows[2 * k + 1];
+        P.L = layout_of(rows[2 * k + 3] - rows[2 * k + 1], rows[2 * k + 2] - rows[2 * k], nprops, es);
+        P.base = pos;
+        pos += P.L.bytes;
+        any_points |= P.L.n_pnt > 0;
     }
+    if (pos > capacity) {
+        set_error("the pack buffer is smaller than sgb_pack_request reported");
+        return SGB_ERANGE;
+    }
+    SGB_TRY(g->scratch[5].ensure(pb.size() * sizeof(PackBox)));
+    SGB_TRY(g->hscratch.ensure(pb.size() * sizeof(PackBox)));
+    std::memcpy(g->hscratch.p, pb.data(), pb.size() * sizeof(PackBox));
+    SGB_CUDA(cudaMemcpyAsync(g->scratch[5].p, g->hscratch.p, pb.size() * sizeof(PackBox), cudaMemcpyHostToDevice, s));
+    unsigned char* out = (unsigned char*)out_dev;
+    if (any_points) {
+        PackProps pp{};
+        pp.np = nprops;
+        for (int p = 0; p < nprops; ++p) {
+            pp.src[p] = g->data[props[p]].as<unsigned char>();
+            pp.es[p] = es[p];
+            // every box's block of property p starts at a multiple of es when the blocks before it do
+            bool wide = true;
+            for (const PackBox& P : pb) wide = wide && (P.base + P.L.off_data + P.L.prop_off[p]) % es[p] == 0;
+            pp.wide[p] = wide;
+        }
+        k_pack_emit<<<wgrid(g, g->n), 256, 0, s>>>(g->keys.as<int64_t>(), g->n, g->geo, g->mask.as<uint8_t>(),
+                                                  g->scratch[5].as<PackBox>(), (int)nboxes, g->scratch[2].as<uint32_t>(),
+                                                  g->scratch[4].as<uint32_t>(), pp, out);
+        SGB_CUDA(cudaGetLastError());
+    }
+    k_pack_finish<<<(unsigned)nboxes, 32, 0, s>>>(g->scratch[5].as<PackBox>(), (int)nboxes, (int32_t)g->geo.size[0],
+                                                 (int32_t)g->geo.size[1], (int32_t)g->geo.size[2], out);
+    SGB_CUDA(cudaGetLastError());
+    SGB_CUDA(cudaStreamSynchronize(s));  // the host staging of the box table is reused by the next call
     *bytes_written = pos;
     return SGB_OK;
 }
@@ -382,7 +465,6 @@ extern "C" int sgb_unpack(sgb_grid* g, const void* buf_dev, int64_t nbytes, int 
         pp.np = nprops;
         for (int k = 0; k < nprops; ++k) {
             pp.es[k] = es[k];
-            pp.off[k] = L.prop_off[k];
             dst.p[k] = g->pend_val[props[k]].as<unsigned char>() + (size_t)g->npend * es[k];
         }
         k_unpack_stage<<<(unsigned)((np_ + 255) / 256), 256, 0, s>>>(buf, L, src, g->geo, sh[0], sh[1], sh[2],
