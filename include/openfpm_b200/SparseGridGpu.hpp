@@ -125,6 +125,8 @@ class CudaMemory {
 
 enum flush_type { FLUSH_ON_HOST = 0, FLUSH_ON_DEVICE = 1 };
 enum StencilMode { STENCIL_MODE_INPLACE = 1, STENCIL_MODE_INPLACE_NO_SHARED = 3 };
+enum class tag_boundaries { NO_CALCULATE_EXISTING_POINTS, CALCULATE_EXISTING_POINTS };
+struct No_check {};
 enum mask_sparse { NOT_EXIST = 0, EXIST = 1, PADDING = 2, EXIST_AND_PADDING = 3 };
 
 template <unsigned dim>
@@ -153,6 +155,11 @@ struct HeatStencil {
 template <unsigned dim, unsigned p_src, unsigned p_dst>
 struct Conv3x3x3 {
     static constexpr int kind = SGB_BOX27;
+    static constexpr unsigned src = p_src, dst = p_dst;
+};
+template <unsigned dim, unsigned p_src, unsigned p_dst>
+struct Conv3x3x3_noshared {
+    static constexpr int kind = SGB_BOX27_NS;
     static constexpr unsigned src = p_src, dst = p_dst;
 };
 struct conv_coeff {
@@ -478,8 +485,11 @@ class SparseGridGpu {
         nn_kind_ = NN::kind;
     }
     template <typename NN = NNStar<dim>>
-    void tagBoundaries(gpu::ofp_context_t&) {
+    void tagBoundaries(gpu::ofp_context_t&, No_check = No_check(),
+                       tag_boundaries opt = tag_boundaries::NO_CALCULATE_EXISTING_POINTS) {
         check(sgb_tag_boundaries(g_, NN::kind, nullptr), "tagBoundaries");
+        if (opt == tag_boundaries::CALCULATE_EXISTING_POINTS)
+            check(sgb_calc_existing_points(g_, nullptr, nullptr), "tagBoundaries (existing points)");
         cudaDeviceSynchronize();  // as the reference (SparseGridGpu.hpp:2393)
     }
 
@@ -497,7 +507,7 @@ class SparseGridGpu {
     }
     template <typename S>
     void applyStencils(const Box<dim, int>& box, StencilMode, const conv_coeff& cc) {
-        static_assert(S::kind == SGB_BOX27, "Conv3x3x3 takes conv_coeff");
+        static_assert(S::kind == SGB_BOX27 || S::kind == SGB_BOX27_NS, "Conv3x3x3 takes conv_coeff");
         float c[27];
         for (int i = 0; i < 3; ++i)
             for (int j = 0; j < 3; ++j)

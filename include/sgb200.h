@@ -74,8 +74,14 @@ typedef enum { SGB_NN_STAR = 0, SGB_NN_FULL = 1 } sgb_nn;
  *              dst {u',v'}, params {Du, Dv, F, k, dt}; writes active points.
  *  SGB_BOX27 : Conv3x3x3<3,src,dst> (src/SparseGridGpu/tests/
  *              SparseGridGpu_tests.cu:887-952); params = 27 coefficients
- *              c[i][j][k], i along x; writes active points; NNFull halo. */
-typedef enum { SGB_HEAT7 = 0, SGB_GS7 = 1, SGB_BOX27 = 2 } sgb_stencil;
+ *              c[i][j][k], i along x; writes active points; NNFull halo.
+ *  SGB_BOX27_NS : Conv3x3x3_noshared<3,src,dst> applied in
+ *              STENCIL_MODE_INPLACE_NO_SHARED (SparseGridGpu_tests.cu:955-1010,
+ *              SparseGridGpu.hpp:1051-1075): one thread per existing point
+ *              of the existing-point list, neighbours read point by point
+ *              through the NNFull table; params = 27 coefficients c[i][j][k],
+ *              i along z; writes active points. */
+typedef enum { SGB_HEAT7 = 0, SGB_GS7 = 1, SGB_BOX27 = 2, SGB_BOX27_NS = 3 } sgb_stencil;
 
 const char* sgb_status_string(int status);
 const char* sgb_last_error_string(void);
@@ -241,6 +247,17 @@ int sgb_pack(sgb_grid* g, int64_t nboxes, const int64_t* boxes_host, int nprops,
  * before the unpacks plays the queued remove(box). */
 int sgb_unpack(sgb_grid* g, const void* buf_dev, int64_t nbytes, int nprops, const int* props,
                const int64_t* start_host, int64_t* consumed, sgb_stream s);
+
+/* The existing-point list of tagBoundaries(..., CALCULATE_EXISTING_POINTS)
+ * (SparseGridGpu.hpp:2354-2387): every existing point as uint32 chunk
+ * position * chunk size + offset, in (chunk position, offset) order (the
+ * reference's order inside a chunk is arbitrary).  Built on demand and kept
+ * until existence changes; SGB_BOX27_NS builds it itself.  Grids of at most
+ * 2^32 chunk points.  *count may be NULL. */
+int sgb_calc_existing_points(sgb_grid* g, int64_t* count, sgb_stream s);
+
+/* The same list's device array (valid until existence changes) and length. */
+int sgb_existing_point_list(sgb_grid* g, const uint32_t** ids_dev, int64_t* count, sgb_stream s);
 
 /* countExistingElements / countBoundaryElements (SparseGridGpu.hpp:2422-2474). */
 int sgb_count_existing(sgb_grid* g, int64_t* existing, int64_t* padding, sgb_stream s);

@@ -21,7 +21,7 @@ OP_NONE, OP_RIGHT, OP_LEFT, OP_ADD, OP_MAX, OP_MIN, OP_OR = range(7)
 # neighbourhoods (sgb_nn)
 NN_STAR, NN_FULL = 0, 1
 # stencils (sgb_stencil)
-HEAT7, GS7, BOX27 = 0, 1, 2
+HEAT7, GS7, BOX27, BOX27_NS = 0, 1, 2, 3
 
 # every entry point of include/sgb200.h: name -> (restype, argtypes)
 _vp, _i32, _i64 = C.c_void_p, C.c_int, C.c_int64
@@ -39,6 +39,8 @@ SIGNATURES = {
     "sgb_get_view": (_i32, [_vp, _i32, _vp, _vp]),
     "sgb_remove_boxes": (_i32, [_vp, _i64, _vp, _vp]),
     "sgb_existing_points": (_i32, [_vp, _vp, _vp, _i64, _vp, _vp]),
+    "sgb_calc_existing_points": (_i32, [_vp, _vp, _vp]),
+    "sgb_existing_point_list": (_i32, [_vp, _vp, _vp, _vp]),
     "sgb_pack_request": (_i32, [_vp, _i64, _vp, _i32, _vp, _vp, _vp]),
     "sgb_pack": (_i32, [_vp, _i64, _vp, _i32, _vp, _vp, _i64, _vp, _vp]),
     "sgb_unpack": (_i32, [_vp, _vp, _i64, _i32, _vp, _vp, _vp, _vp]),

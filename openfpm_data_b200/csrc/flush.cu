@@ -466,5 +466,6 @@ extern "C" int sgb_flush(sgb_grid* g, const int* ops, sgb_stream stream) {
     g->npend = 0;
     g->nn_valid[0] = g->nn_valid[1] = false;
     g->bits_valid = false;
+    g->epts_valid = false;
     return st;
 }

@@ -141,6 +141,7 @@ int grid_reserve(sgb_grid* g, int64_t chunks, bool keep) {
 static void invalidate_derived(sgb_grid* g) {
     g->nn_valid[0] = g->nn_valid[1] = false;
     g->bits_valid = false;
+    g->epts_valid = false;
 }
 
 // Points whose mask byte is 0 take the background value: 16 mask bytes per
@@ -549,6 +550,7 @@ int sgb_mask_buffer(sgb_grid* g, uint8_t** dev) {
     *dev = g->mask.as<uint8_t>();
     for (int p = 0; p < g->nprop; ++p) g->clean[p] = false;  // existence may change
     g->bits_valid = false;
+    g->epts_valid = false;
     return SGB_OK;
 }
 

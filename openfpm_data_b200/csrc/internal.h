@@ -118,6 +118,10 @@ struct sgb_grid {
     bool nn_valid[2] = {false, false};
     sgb::DevBuf bits;     // uint64 existence bitmaps, bs/64 words per chunk
     bool bits_valid = false;
+    // existing-point list (e_points): uint32 chunk position * bs + offset
+    sgb::DevBuf epts;
+    int64_t nepts = 0;
+    bool epts_valid = false;
 
     // clean[p]: every point of property p whose mask byte is 0 holds the
     // background value.  The reference substitutes the background for such
@@ -141,6 +145,10 @@ namespace sgb {
 // neighbours.cu
 int ensure_neighbours(sgb_grid* g, int nn, cudaStream_t s);
 int ensure_bits(sgb_grid* g, cudaStream_t s);
+
+// points.cu
+int ensure_point_list(sgb_grid* g, cudaStream_t s);
+int launch_points_box27(sgb_grid* g, const int* src, const int* dst, const StencilParams& prm, cudaStream_t s);
 
 // stencil.cu
 int launch_stencil(sgb_grid* g, int kind, const int* src, const int* dst, const StencilParams& prm,

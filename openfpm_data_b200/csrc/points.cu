@@ -1,0 +1,167 @@
+// The existing-point list and the point-list ("no shared memory") stencil mode.
+//
+// tagBoundaries(..., CALCULATE_EXISTING_POINTS) (SparseGridGpu.hpp:2354-2387,
+// kernels calc_exist_points / fill_e_points, SparseGridGpu_kernels.cuh:
+// 1152-1225) lists every existing point as chunk position * chunk size +
+// offset (e_points).  applyStencils in STENCIL_MODE_INPLACE_NO_SHARED
+// (SparseGridGpu.hpp:1051-1075 -> applyStencilInPlaceNoShared,
+// SparseGridGpu_kernels.cuh:1096-1150) runs one thread per listed point, and
+// the stencil reads its neighbours point by point through the NNFull table
+// (getNNPoint, SparseGridGpu_ker.cuh:297-327) instead of a shared-memory tile.
+// The stencil of that mode in the reference is Conv3x3x3_noshared
+// (src/SparseGridGpu/tests/SparseGridGpu_tests.cu:955-1010).
+//
+// The list here is in (chunk position, offset) order (the reference fills it
+// through a shared-memory atomic counter, any order inside a chunk; the
+// stencil results do not depend on it) and is rebuilt whenever existence
+// changed since it was made.
+#include <algorithm>
+
+#include "common.cuh"
+#include "internal.h"
+#include "stencil.cuh"
+
+namespace sgb {
+
+// Existing points per chunk: one warp per chunk, ballot counts.
+__global__ void k_ep_count(const uint8_t* __restrict__ mask, int64_t n, int bs, uint32_t* counts) {
+    const int lane = threadIdx.x & 31;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t c = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; c < n; c += nw) {
+        uint32_t t = 0;
+        for (int pt = lane; pt < bs; pt += 32) t += __popc(__ballot_sync(0xffffffffu, mask[c * bs + pt] & 1));
+        if (lane == 0) counts[c] = t;
+    }
+}
+
+__global__ void k_ep_emit(const uint8_t* __restrict__ mask, int64_t n, int bs, const uint32_t* __restrict__ offs,
+                          uint32_t* out) {
+    const int lane = threadIdx.x & 31;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t c = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; c < n; c += nw) {
+        uint32_t base = offs[c];
+        for (int pt = lane; pt < bs; pt += 32) {
+            const bool ex = mask[c * bs + pt] & 1;
+            const unsigned bal = __ballot_sync(0xffffffffu, ex);
+            if (ex) out[base + __popc(bal & lanemask_lt())] = (uint32_t)(c * bs + pt);
+            base += __popc(bal);
+        }
+    }
+}
+
+int ensure_point_list(sgb_grid* g, cudaStream_t s) {
+    if (g->epts_valid) return SGB_OK;
+    const int64_t n = g->n, bs = g->geo.bs;
+    if (n * bs >= (int64_t(1) << 32)) {
+        set_error("the existing-point list holds 32-bit point ids: at most 2^32 chunk points");
+        return SGB_ERANGE;
+    }
+    g->nepts = 0;
+    if (n > 0) {
+        SGB_TRY(g->scratch[1].ensure((size_t)n * 4 + 16));
+        SGB_TRY(g->scratch[2].ensure((size_t)(n + 1) * 4 + 16));
+        uint32_t* counts = g->scratch[1].as<uint32_t>();
+        uint32_t* offs = g->scratch[2].as<uint32_t>();
+        const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>((int64_t)g->num_sms * 8, (n + 7) / 8));
+        k_ep_count<<<blocks, 256, 0, s>>>(g->mask.as<uint8_t>(), n, (int)bs, counts);
+        SGB_CUDA(cudaGetLastError());
+        SGB_TRY(scan_exclusive_u32(counts, offs, n, offs + n, &g->scratch[6], s));
+        SGB_TRY(g->hscratch.ensure(64));
+        SGB_CUDA(cudaMemcpyAsync(g->hscratch.p, offs + n, 4, cudaMemcpyDeviceToHost, s));
+        SGB_CUDA(cudaStreamSynchronize(s));
+        g->nepts = *(uint32_t*)g->hscratch.p;
+        SGB_TRY(g->epts.ensure((size_t)g->nepts * 4 + 16));
+        k_ep_emit<<<blocks, 256, 0, s>>>(g->mask.as<uint8_t>(), n, (int)bs, offs, g->epts.as<uint32_t>());
+        SGB_CUDA(cudaGetLastError());
+    }
+    g->epts_valid = true;
+    return SGB_OK;
+}
+
+// Conv3x3x3_noshared over the point list: tot = fma(value, c[i][j][k], tot)
+// with the neighbour at (x+k-1, y+j-1, z+i-1), i outermost.  Neighbour values
+// are read as stored (the grid keeps the background in non-existing points
+// and in the background chunk, where absent neighbours point).
+template <int E>
+__global__ void __launch_bounds__(256) k_box27_points(const float* __restrict__ src, float* __restrict__ dst,
+                                                      const uint8_t* __restrict__ mask, const int32_t* __restrict__ nn,
+                                                      const int64_t* __restrict__ keys, const uint32_t* __restrict__ pts,
+                                                      int64_t npts, int64_t n, Geometry geo, StencilParams prm) {
+    constexpr int BS = E * E * E;
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= npts) return;
+    const uint32_t id = pts[t];
+    const int64_t c = id / BS;
+    const int off = (int)(id % BS);
+    const uint8_t m = mask[id];
+    const int x = off % E, y = (off / E) % E, z = off / (E * E);
+    bool act = (m & 1) && !(m & 2);
+    if (prm.has_box) {
+        const int64_t key = keys[c];
+        const int64_t ox = (key % geo.bsz[0]) * E, oy = ((key / geo.bsz[0]) % geo.bsz[1]) * E,
+                      oz = (key / (geo.bsz[0] * geo.bsz[1])) * E;
+        act = act && in_box(prm, ox + x, oy + y, oz + z);
+    }
+    if (!act) return;
+    float tot = 0.0f;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        const int qz = z + i - 1, pz = qz < 0 ? 0 : (qz >= E ? 2 : 1), lz = qz + (1 - pz) * E;
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            const int qy = y + j - 1, py = qy < 0 ? 0 : (qy >= E ? 2 : 1), ly = qy + (1 - py) * E;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const int qx = x + k - 1, px = qx < 0 ? 0 : (qx >= E ? 2 : 1), lx = qx + (1 - px) * E;
+                const int slot = px + 3 * py + 9 * pz;
+                int64_t pos = c;
+                if (slot != 13) {
+                    const int32_t v = nn[c * 27 + slot];
+                    pos = v < 0 ? n : v;
+                }
+                tot = __fmaf_rn(src[pos * BS + lx + E * (ly + E * lz)], prm.coeff[i * 9 + j * 3 + k], tot);
+            }
+        }
+    }
+    dst[id] = tot;
+}
+
+int launch_points_box27(sgb_grid* g, const int* src, const int* dst, const StencilParams& prm, cudaStream_t s) {
+    if (g->n == 0) return SGB_OK;
+    SGB_TRY(ensure_neighbours(g, SGB_NN_FULL, s));
+    SGB_TRY(ensure_clean(g, src[0], s));
+    SGB_TRY(ensure_point_list(g, s));
+    if (g->nepts == 0) return SGB_OK;
+    const unsigned blocks = (unsigned)((g->nepts + 255) / 256);
+    const float* in = g->data[src[0]].as<float>();
+    float* out = g->data[dst[0]].as<float>();
+    if (g->geo.edge == 8)
+        k_box27_points<8><<<blocks, 256, 0, s>>>(in, out, g->mask.as<uint8_t>(), g->nn[SGB_NN_FULL].as<int32_t>(),
+                                                 g->keys.as<int64_t>(), g->epts.as<uint32_t>(), g->nepts, g->n, g->geo,
+                                                 prm);
+    else
+        k_box27_points<4><<<blocks, 256, 0, s>>>(in, out, g->mask.as<uint8_t>(), g->nn[SGB_NN_FULL].as<int32_t>(),
+                                                 g->keys.as<int64_t>(), g->epts.as<uint32_t>(), g->nepts, g->n, g->geo,
+                                                 prm);
+    SGB_CUDA(cudaGetLastError());
+    return SGB_OK;
+}
+
+}  // namespace sgb
+
+using namespace sgb;
+
+extern "C" int sgb_calc_existing_points(sgb_grid* g, int64_t* count, sgb_stream stream) {
+    if (!g) return SGB_EINVAL;
+    SGB_TRY(ensure_point_list(g, (cudaStream_t)stream));
+    if (count) *count = g->nepts;
+    return SGB_OK;
+}
+
+extern "C" int sgb_existing_point_list(sgb_grid* g, const uint32_t** ids_dev, int64_t* count, sgb_stream stream) {
+    if (!g || !ids_dev || !count) return SGB_EINVAL;
+    SGB_TRY(ensure_point_list(g, (cudaStream_t)stream));
+    *ids_dev = g->epts.as<uint32_t>();
+    *count = g->nepts;
+    return SGB_OK;
+}

@@ -165,7 +165,9 @@ extern "C" int sgb_remove_boxes(sgb_grid* g, int64_t nboxes, const int64_t* boxe
     SGB_CUDA(cudaGetLastError());
     // the host copy of the boxes must outlive the asynchronous upload
     SGB_CUDA(cudaStreamSynchronize(s));
-    g->bits_valid = false;  // existence changed; chunks, neighbours and backgrounds did not
+    // existence changed; chunks, neighbours and backgrounds did not
+    g->bits_valid = false;
+    g->epts_valid = false;
     return SGB_OK;
 }
 

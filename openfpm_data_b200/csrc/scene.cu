@@ -191,5 +191,6 @@ extern "C" int sgb_build_balls(sgb_grid* g, int nballs, const float* balls, int 
     SGB_TRY(write_background(g, n, s, g->data, g->mask));
     g->nn_valid[0] = g->nn_valid[1] = false;
     g->bits_valid = false;
+    g->epts_valid = false;
     return SGB_OK;
 }

@@ -129,7 +129,7 @@ int make_params(sgb_grid* g, int kind, const int* src, const int* dst, const flo
                 const int64_t* box, StencilParams& prm) {
     std::memset(&prm, 0, sizeof(prm));
     if (!src || !dst || (nparams > 0 && !params)) return SGB_EINVAL;
-    if (kind < SGB_HEAT7 || kind > SGB_BOX27) return SGB_EINVAL;
+    if (kind < SGB_HEAT7 || kind > SGB_BOX27_NS) return SGB_EINVAL;
     const int np = kind == SGB_GS7 ? 2 : 1;
     for (int j = 0; j < np; ++j) {
         if (src[j] < 0 || src[j] >= g->nprop || dst[j] < 0 || dst[j] >= g->nprop) return SGB_EINVAL;
@@ -215,6 +215,7 @@ int launch_fields(const LaunchDesc& L, cudaStream_t s) {
 int launch_stencil_impl(sgb_grid* g, int kind, const int* src, const int* dst, const StencilParams& prm,
                         cudaStream_t s, bool use_tile) {
     if (g->n == 0) return SGB_OK;
+    if (kind == SGB_BOX27_NS) return launch_points_box27(g, src, dst, prm, s);
     const int nnk = kind == SGB_BOX27 ? SGB_NN_FULL : SGB_NN_STAR;
     SGB_TRY(ensure_neighbours(g, nnk, s));
     const int np = kind == SGB_GS7 ? 2 : 1;
@@ -287,7 +288,8 @@ int sgb_run_steps(sgb_grid* g, int kind, const int* src, const int* dst, const f
     SGB_TRY(make_params(g, kind, dst, src, params, nparams, nullptr, bwd));
     if (final_is_dst) *final_is_dst = nsteps % 2;
     if (nsteps == 0 || g->n == 0) return SGB_OK;
-    SGB_TRY(ensure_neighbours(g, kind == SGB_BOX27 ? SGB_NN_FULL : SGB_NN_STAR, s));
+    SGB_TRY(ensure_neighbours(g, kind == SGB_BOX27 || kind == SGB_BOX27_NS ? SGB_NN_FULL : SGB_NN_STAR, s));
+    if (kind == SGB_BOX27_NS) SGB_TRY(ensure_point_list(g, s));  // built outside the capture
     // both halves of the ping-pong are read as sources; no sanitising inside a capture
     for (int j = 0; j < (kind == SGB_GS7 ? 2 : 1); ++j) {
         SGB_TRY(ensure_clean(g, src[j], s));

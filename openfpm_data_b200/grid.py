@@ -156,8 +156,28 @@ class SparseGridGpu:
                 "sgb_neighbour_table")
         return out.reshape(self.nchunks, k)
 
-    def tagBoundaries(self, nn: int = L.NN_STAR, stream=None) -> None:
+    def tagBoundaries(self, nn: int = L.NN_STAR, calculate_existing_points: bool = False, stream=None) -> None:
+        """tagBoundaries<NN>(ctx, No_check(), opt); calculate_existing_points builds the
+        existing-point list (tag_boundaries::CALCULATE_EXISTING_POINTS)."""
         L.check(self._lib.sgb_tag_boundaries(self._h, nn, _stream(stream)), "sgb_tag_boundaries")
+        if calculate_existing_points:
+            self.calc_existing_points(stream)
+
+    def calc_existing_points(self, stream=None) -> int:
+        cnt = C.c_int64()
+        L.check(self._lib.sgb_calc_existing_points(self._h, C.byref(cnt), _stream(stream)),
+                "sgb_calc_existing_points")
+        return cnt.value
+
+    def existing_point_list(self, stream=None) -> torch.Tensor:
+        """The e_points list: int64 copy of the uint32 ids chunk position * bs + offset."""
+        p, cnt = C.c_void_p(), C.c_int64()
+        L.check(self._lib.sgb_existing_point_list(self._h, C.byref(p), C.byref(cnt), _stream(stream)),
+                "sgb_existing_point_list")
+        if cnt.value == 0:
+            return torch.empty(0, dtype=torch.int64, device=f"cuda:{self.device}")
+        v = torch.as_tensor(_DevView(p.value, (cnt.value,), "<i4"), device=f"cuda:{self.device}")
+        return v.to(torch.int64) & 0xFFFFFFFF
 
     # ---------------------------------------------------------------- stencils
     @staticmethod

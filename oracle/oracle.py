@@ -67,6 +67,7 @@ def _load():
         _lib.sgo_heat7.argtypes = [vp, i32, i32, f, vp]
         _lib.sgo_gs7.argtypes = [vp, i32, i32, i32, i32, f, f, f, f, f, vp]
         _lib.sgo_box27.argtypes = [vp, i32, i32, vp, vp]
+        _lib.sgo_box27_ns.argtypes = [vp, i32, i32, vp, vp]
         d = C.c_double
         _lib.sgo_heat7_f64.argtypes = [vp, vp, vp, d, d, i32]
         _lib.sgo_gs7_f64.argtypes = [vp, vp, vp, vp, vp, d, d, d, d, d, d, d, i32]
@@ -292,6 +293,12 @@ class OracleGrid:
         c = np.ascontiguousarray(coeff, dtype=np.float32).reshape(27)
         b = self._box(box)
         _lib.sgo_box27(self._h, src, dst, _ptr(c), None if b is None else _ptr(b))
+
+    def box27_noshared(self, src, dst, coeff, box=None):
+        """Conv3x3x3_noshared through applyStencilInPlaceNoShared: coeff[i][j][k], i along z."""
+        c = np.ascontiguousarray(coeff, dtype=np.float32).reshape(27)
+        b = self._box(box)
+        _lib.sgo_box27_ns(self._h, src, dst, _ptr(c), None if b is None else _ptr(b))
 
     def heat7_f64(self, field, dt, bck, steps):
         a = np.ascontiguousarray(field, dtype=np.float64).copy()

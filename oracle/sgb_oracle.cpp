@@ -668,6 +668,46 @@ void sgo_box27(void* h, int src, int dst, const float* coeff, const int64_t* box
     g->data[dst].swap(out);
 }
 
+// Conv3x3x3_noshared (src/SparseGridGpu/tests/SparseGridGpu_tests.cu:955-1010)
+// applied by applyStencilInPlaceNoShared (SparseGridGpu_kernels.cuh:1096-1150)
+// over the existing points: for an active point, tot += get(getNNPoint(key)) *
+// coeff[i][j][k] with key = (k-1, j-1, i-1), i outermost (so i runs along z
+// and k along x, the transpose of Conv3x3x3), contracted to an FMA.  The
+// neighbour value is read from the chunk data as it is (no background
+// substitution for non-existing points; an absent chunk is the background
+// chunk, SparseGridGpu.hpp:269-291, getNNPoint SparseGridGpu_ker.cuh:297-327).
+void sgo_box27_ns(void* h, int src, int dst, const float* coeff, const int64_t* box) {
+    FtzScope ftz;
+    Grid* g = (Grid*)h;
+    auto nn = find_neighbours(*g, NN_FULL);
+    const int e = g->edge, bs = g->bs;
+    const float* in = (const float*)g->data[src].data();
+    std::vector<uint8_t> out(g->data[dst]);
+    for (int64_t c = 0; c < g->n(); ++c) {
+        for (int o = 0; o < bs; ++o) {
+            if (!active(cur_mask(*g, c, o, box))) continue;
+            int lc[3] = {0, 0, 0};
+            local_coord(*g, o, lc);
+            float tot = 0.0f;
+            for (int i = 0; i < 3; ++i)
+                for (int j = 0; j < 3; ++j)
+                    for (int k = 0; k < 3; ++k) {
+                        const int q[3] = {lc[0] + k - 1, lc[1] + j - 1, lc[2] + i - 1};
+                        int nidx = 0, off = 0;
+                        for (int d = 2; d >= 0; --d) {
+                            const int p = q[d] < 0 ? 0 : (q[d] >= e ? 2 : 1);
+                            nidx = nidx * 3 + p;
+                            off = off * e + (q[d] + (1 - p) * e);
+                        }
+                        const int64_t pos = nidx == 13 ? c : nn[(size_t)c * 27 + nidx];
+                        tot = std::fmaf(in[(size_t)pos * bs + off], coeff[i * 9 + j * 3 + k], tot);
+                    }
+            std::memcpy(&out[((size_t)c * bs + o) * 4], &tot, 4);
+        }
+    }
+    g->data[dst].swap(out);
+}
+
 // FP64 references for error statements: the same updates in double precision
 // on caller-owned double fields laid out like the chunk data ((n+1)*bs, the
 // background chunk last).  Active set and neighbourhoods come from the grid.

@@ -297,6 +297,22 @@ int main() {
     HostMap Q = download(grid.handle(), 6);
     CHECK(same(Q, 2, Q, 3, active), "conv3x3x3_vs_conv_nnfull");
 
+    // ------------------------------------------- Conv3x3x3_noshared (point list) vs conv over NNFull
+    // SparseGridGpu_tests.cu:1073-1141: tagBoundaries with CALCULATE_EXISTING_POINTS, then
+    // applyStencils in STENCIL_MODE_INPLACE_NO_SHARED; coefficient [i][j][k] with i along z
+    grid.tagBoundaries<NNFull<3>>(ctx, No_check(), tag_boundaries::CALCULATE_EXISTING_POINTS);
+    grid.applyStencils<Conv3x3x3_noshared<3, 0, 2>>(all, STENCIL_MODE_INPLACE_NO_SHARED, cc);
+    grid.conv<0, 3, 1>(lo, hi, [cc] __device__(cp_block<float, 8>& u, int i, int j, int k) {
+        float tot = 0.0f;
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b)
+                for (int d = 0; d < 3; ++d) tot = __fmaf_rn(u(i + d - 1, j + b - 1, k + a - 1), cc.coeff[a][b][d], tot);
+        return tot;
+    });
+    cudaDeviceSynchronize();
+    HostMap Q2 = download(grid.handle(), 6);
+    CHECK(same(Q2, 2, Q2, 3, active), "conv3x3x3_noshared_vs_conv_nnfull");
+
     // ---------------------------------------------------------------- removePoints + iterator
     {
         const auto before = grid.existingPoints();

@@ -65,3 +65,19 @@ def test_pack_unpack_sphere():
             rel = p - np.asarray(lo) + np.asarray(slo) - K.CENTRE
             np.testing.assert_array_equal(dst.get(0, p), rel.sum(axis=1).astype(np.float32))
             np.testing.assert_array_equal(dst.get(3, p), rel[:, 2].astype(np.float32))
+
+
+def test_conv3x3x3_noshared_all_ones():
+    """SparseGridGpu_tests.cu:1073-1141 test3x3x3convolution_no_shared: the
+    hollow sphere (edge 4), NNFull, every coefficient 1: out = 27 * in at the
+    active points (mask byte 1)."""
+    g = O.OracleGrid(K.SIZE, edge=K.EDGE, ptypes=(O.T_F32, O.T_F32))
+    c, rel = K.sphere()
+    g.insert_flush(c, [K.sphere_values(rel)[0], np.zeros(len(c), np.float32)], [O.OP_MAX, O.OP_NONE])
+    g.tag_boundaries(O.NN_FULL)
+    g.box27_noshared(0, 1, np.ones(27, np.float32))
+    keys, data, mask = g.export()
+    n = len(keys) * g.bs
+    act = mask[:n] == 1
+    assert act.sum() > 100000
+    np.testing.assert_array_equal(data[1][:n][act], data[0][:n][act] * 27)
