@@ -74,6 +74,12 @@ struct Box {
     __host__ __device__ void setHigh(unsigned i, T v) { hi[i] = v; }
 };
 
+template <unsigned dim, typename T>
+struct Point {
+    T x[dim];
+    __host__ __device__ T get(unsigned i) const { return x[i]; }
+};
+
 namespace gpu {
 struct ofp_context_t {};
 }  // namespace gpu
@@ -606,6 +612,23 @@ class SparseGridGpu {
         return existing_points_impl(b);
     }
 
+    // ---- multi-resolution links (SparseGridGpu.hpp:2113-2262)
+    void construct_link_dw(SparseGridGpu& grid_dw, const Box<dim, int>& db, Point<dim, int> p_dw,
+                           gpu::ofp_context_t&) {
+        int64_t b[6], sh[3];
+        for (unsigned d = 0; d < 3; ++d) b[d] = db.getLow(d), b[3 + d] = db.getHigh(d), sh[d] = p_dw.get(d);
+        check(sgb_construct_link_dw(g_, grid_dw.handle(), b, sh, nullptr), "construct_link_dw");
+    }
+    void construct_link_up(SparseGridGpu& grid_up, const Box<dim, int>& db, Point<dim, int> p_up,
+                           gpu::ofp_context_t&) {
+        int64_t b[6], sh[3];
+        for (unsigned d = 0; d < 3; ++d) b[d] = db.getLow(d), b[3 + d] = db.getHigh(d), sh[d] = p_up.get(d);
+        check(sgb_construct_link_up(g_, grid_up.handle(), b, sh, nullptr), "construct_link_up");
+    }
+    // getDownLinks / getDownLinksOffsets and the up pair, as one device view per direction
+    sgb_links getDownLinks() const { return links(0); }
+    sgb_links getUpLinks() const { return links(1); }
+
     // getIterator(start, stop): the sub-grid iterator of the inclusive box
     SparseGridGpu_iterator_sub<dim> getIterator(const grid_key_dx<dim>& start, const grid_key_dx<dim>& stop) const {
         return SparseGridGpu_iterator_sub<dim>{start, stop};
@@ -711,6 +734,12 @@ class SparseGridGpu {
    private:
     std::vector<Box<dim, int>> rem_sects_;
     std::vector<SparseGridGpu_iterator_sub<dim>> pack_subs_;
+
+    sgb_links links(int up) const {
+        sgb_links l{};
+        check(sgb_get_links(g_, up, &l), "links");
+        return l;
+    }
 
     std::vector<int64_t> pack_rows() const {
         std::vector<int64_t> b;

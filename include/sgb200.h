@@ -259,6 +259,41 @@ int sgb_calc_existing_points(sgb_grid* g, int64_t* count, sgb_stream s);
 /* The same list's device array (valid until existence changes) and length. */
 int sgb_existing_point_list(sgb_grid* g, const uint32_t** ids_dev, int64_t* count, sgb_stream s);
 
+/* Links between the levels of a multi-resolution hierarchy
+ * (construct_link_dw / construct_link_up, SparseGridGpu.hpp:2113-2262;
+ * kernels SparseGridGpu_kernels.cuh:775-1000).  The padding points (mask
+ * bit 1) of g inside the inclusive box {lo[3], hi[3]} are listed in (chunk
+ * position, offset) order; a padding point at p links
+ *   down: to the existing points of grid_dw at 2p + p_dw + (j & 1,
+ *         (j >> 1) & 1, (j >> 2) & 1), j = 0 .. 5 (the reference's loop
+ *         bound 2*dim: the children (0,1,1) and (1,1,1) are not visited);
+ *   up:   to the existing point of grid_up at (p - p_up) / 2, truncating.
+ * The other grid is addressed as the reference's device get does
+ * (grid_smb::LinId without bounds checks, cast to unsigned int).  Both
+ * grids share the chunk edge and the device; each call replaces g's links of
+ * that direction and synchronises the stream. */
+int sgb_construct_link_dw(sgb_grid* g, const sgb_grid* grid_dw, const int64_t* box_host, const int64_t* p_dw_host,
+                          sgb_stream s);
+int sgb_construct_link_up(sgb_grid* g, const sgb_grid* grid_up, const int64_t* box_host, const int64_t* p_up_host,
+                          sgb_stream s);
+
+/* The links of one direction (up = 0 down, 1 up): getDownLinks /
+ * getDownLinksOffsets / getUpLinks / getUpLinksOffsets.  Device arrays valid
+ * until the next construct call: the padding points (pad_pos chunk
+ * position, pad_off offset), offsets[npad + 1] (first link of each padding
+ * point, nlinks last) and the links (link_pos chunk position in the other
+ * grid, link_off offset; only existing points are linked). */
+typedef struct {
+    int64_t npad;
+    const int32_t* pad_pos;
+    const int16_t* pad_off;
+    const uint32_t* offsets;
+    int64_t nlinks;
+    const int32_t* link_pos;
+    const int16_t* link_off;
+} sgb_links;
+int sgb_get_links(sgb_grid* g, int up, sgb_links* out);
+
 /* countExistingElements / countBoundaryElements (SparseGridGpu.hpp:2422-2474). */
 int sgb_count_existing(sgb_grid* g, int64_t* existing, int64_t* padding, sgb_stream s);
 

@@ -41,6 +41,9 @@ SIGNATURES = {
     "sgb_existing_points": (_i32, [_vp, _vp, _vp, _i64, _vp, _vp]),
     "sgb_calc_existing_points": (_i32, [_vp, _vp, _vp]),
     "sgb_existing_point_list": (_i32, [_vp, _vp, _vp, _vp]),
+    "sgb_construct_link_dw": (_i32, [_vp, _vp, _vp, _vp, _vp]),
+    "sgb_construct_link_up": (_i32, [_vp, _vp, _vp, _vp, _vp]),
+    "sgb_get_links": (_i32, [_vp, _i32, _vp]),
     "sgb_pack_request": (_i32, [_vp, _i64, _vp, _i32, _vp, _vp, _vp]),
     "sgb_pack": (_i32, [_vp, _i64, _vp, _i32, _vp, _vp, _i64, _vp, _vp]),
     "sgb_unpack": (_i32, [_vp, _vp, _i64, _i32, _vp, _vp, _vp, _vp]),

@@ -90,6 +90,14 @@ struct FieldSet {
     float* out[2][2];
 };
 
+// Links of one direction (construct_link_dw / construct_link_up).
+struct LinkSet {
+    DevBuf pad_pos, pad_off;  // padding points: int32 chunk position, int16 offset
+    DevBuf scan;              // uint32 [npad + 1]: first link of each padding point, nlinks last
+    DevBuf pos, off;          // links: int32 chunk position, int16 offset in the other grid
+    int64_t npad = 0, nlinks = 0;
+};
+
 }  // namespace sgb
 
 struct sgb_grid {
@@ -122,6 +130,8 @@ struct sgb_grid {
     sgb::DevBuf epts;
     int64_t nepts = 0;
     bool epts_valid = false;
+    // multi-resolution links: [0] down, [1] up
+    sgb::LinkSet links[2];
 
     // clean[p]: every point of property p whose mask byte is 0 holds the
     // background value.  The reference substitutes the background for such

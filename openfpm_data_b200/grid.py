@@ -25,6 +25,12 @@ OPS = {"sRight_": L.OP_RIGHT, "sLeft_": L.OP_LEFT, "sadd_": L.OP_ADD, "smax_": L
        "sBitwiseOr_": L.OP_OR, None: L.OP_NONE, "none": L.OP_NONE}
 
 
+class _Links(C.Structure):
+    """sgb_links of include/sgb200.h."""
+    _fields_ = [("npad", C.c_int64), ("pad_pos", C.c_void_p), ("pad_off", C.c_void_p), ("offsets", C.c_void_p),
+                ("nlinks", C.c_int64), ("link_pos", C.c_void_p), ("link_off", C.c_void_p)]
+
+
 class _View(C.Structure):
     """sgb_view of include/sgb200.h."""
     _fields_ = [("n", C.c_int64), ("edge", C.c_int), ("bs", C.c_int), ("nprop", C.c_int), ("nn_kind", C.c_int),
@@ -294,6 +300,40 @@ class SparseGridGpu:
         box = None if start is None else (start, stop)
         for p in self.existing_points(box).cpu().numpy():
             yield tuple(int(v) for v in p)
+
+    # ---------------------------------------------------------------- multi-resolution links
+    def construct_link_dw(self, grid_dw: "SparseGridGpu", box, p_dw=(0, 0, 0), stream=None) -> None:
+        """Links from the padding points inside box ((lo), (hi)) to the finer grid grid_dw."""
+        b = (C.c_int64 * 6)(*(list(box[0]) + list(box[1])))
+        sh = (C.c_int64 * 3)(*[int(v) for v in p_dw])
+        L.check(self._lib.sgb_construct_link_dw(self._h, grid_dw._h, b, sh, _stream(stream)), "sgb_construct_link_dw")
+
+    def construct_link_up(self, grid_up: "SparseGridGpu", box, p_up=(0, 0, 0), stream=None) -> None:
+        """Links from the padding points inside box to the coarser grid grid_up."""
+        b = (C.c_int64 * 6)(*(list(box[0]) + list(box[1])))
+        sh = (C.c_int64 * 3)(*[int(v) for v in p_up])
+        L.check(self._lib.sgb_construct_link_up(self._h, grid_up._h, b, sh, _stream(stream)), "sgb_construct_link_up")
+
+    def _links(self, up: int) -> dict:
+        v = _Links()
+        L.check(self._lib.sgb_get_links(self._h, up, C.byref(v)), "sgb_get_links")
+        dev = f"cuda:{self.device}"
+
+        def arr(ptr, n, ts):
+            if n == 0 or not ptr:
+                return torch.empty(0, dtype=torch.int64, device=dev)
+            return torch.as_tensor(_DevView(ptr, (n,), ts), device=dev).to(torch.int64)
+        offs = arr(v.offsets, v.npad + 1, "<i4") & 0xFFFFFFFF if v.offsets else torch.zeros(1, dtype=torch.int64)
+        return {"pad_pos": arr(v.pad_pos, v.npad, "<i4"), "pad_off": arr(v.pad_off, v.npad, "<i2"),
+                "offsets": offs, "link_pos": arr(v.link_pos, v.nlinks, "<i4"),
+                "link_off": arr(v.link_off, v.nlinks, "<i2")}
+
+    def getDownLinks(self) -> dict:
+        """Padding points, per-point link offsets (npad + 1) and links (chunk position, offset)."""
+        return self._links(0)
+
+    def getUpLinks(self) -> dict:
+        return self._links(1)
 
     # ---------------------------------------------------------------- pack / unpack
     def packReset(self) -> None:

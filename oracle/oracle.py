@@ -272,7 +272,59 @@ class OracleGrid:
             pos, k = q, k + 1
         return res
 
+    # -- multi-resolution links (SparseGridGpu.hpp:2113-2262, kernels
+    #    SparseGridGpu_kernels.cuh:775-1000) ---------------------------------
+    def _other_exists(self, c):
+        """SparseGridGpu_ker::get<pMask>(coord) & 1 for int64 coords [m, 3]: grid_smb::LinId
+        with C (truncating) division and no bounds checks, cast to unsigned int, then the
+        chunk looked up (absent: the background chunk).  Returns (exists, pos, off)."""
+        keys, _, mask = self.export()
+        e = self.edge
+        bsz = [(s + e - 1) // e for s in self.size]
+        q = lambda a: np.sign(a) * (np.abs(a) // e)  # noqa: E731  (truncating division by e)
+        r = lambda a: a - q(a) * e  # noqa: E731
+        blk, loc = q(c[:, 2]), r(c[:, 2])
+        for d in (1, 0):
+            blk = blk * bsz[d] + q(c[:, d])
+            loc = loc * e + r(c[:, d])
+        lin = (blk * self.bs + loc) & 0xFFFFFFFF
+        b, off = lin // self.bs, lin % self.bs
+        pos = np.searchsorted(keys, b)
+        found = (pos < len(keys)) & (keys[np.minimum(pos, max(len(keys) - 1, 0))] == b) if len(keys) else \
+            np.zeros(len(b), bool)
+        pos = np.where(found, pos, len(keys))
+        ex = (mask[pos * self.bs + off] & 1) != 0
+        return ex, pos, off
+
+    def construct_links(self, other, box, shift, up):
+        """Padding points inside the inclusive box in (chunk, offset) order, and their links
+        to `other`: down (up=False) to the existing points at 2p + shift + (j&1, j>>1&1,
+        j>>2&1) for j < 6, up to the existing point at (p - shift) / 2 truncated."""
+        keys, _, mask = self.export()
+        n = len(keys)
+        idx = np.nonzero(mask[: n * self.bs] & 2)[0]
+        lin = keys[idx // self.bs] * self.bs + idx % self.bs
+        p = self.inv_lin(lin) if len(lin) else np.zeros((0, 3), np.int64)
+        lo, hi = np.asarray(box[0]), np.asarray(box[1])
+        sel = np.all((p >= lo) & (p <= hi), axis=1)
+        idx, p = idx[sel], p[sel]
+        sh = np.asarray(shift, dtype=np.int64)
+        if up:
+            t = p - sh
+            cands = [np.sign(t) * (np.abs(t) // 2)]
+        else:
+            cands = [p * 2 + sh + np.array([(j >> d) & 1 for d in range(3)]) for j in range(6)]
+        hits = [other._other_exists(c) for c in cands]
+        ex = np.stack([h[0] for h in hits], axis=1)     # [npad, candidates]
+        pos = np.stack([h[1] for h in hits], axis=1)
+        off = np.stack([h[2] for h in hits], axis=1)
+        offsets = np.concatenate([[0], np.cumsum(ex.sum(axis=1))]).astype(np.int64)
+        # links point by point, candidates in loop order inside a point
+        return {"pad_pos": idx // self.bs, "pad_off": idx % self.bs, "offsets": offsets,
+                "link_pos": pos[ex].astype(np.int64), "link_off": off[ex].astype(np.int64)}
+
     # -- stencils ----------------------------------------------------------
+
 
     @staticmethod
     def _box(box):
