@@ -199,6 +199,41 @@ struct data_block {
 };
 
 namespace detail {
+// chunk ids of the two linearizers (grid_smb: block x fastest; grid_zmb:
+// 3-D Morton code of the block coordinate, 21 bits per coordinate)
+__host__ __device__ inline uint64_t morton_spread3(uint64_t v) {
+    v &= 0x1fffffull;
+    v = (v | v << 32) & 0x1f00000000ffffull;
+    v = (v | v << 16) & 0x1f0000ff0000ffull;
+    v = (v | v << 8) & 0x100f00f00f00f00full;
+    v = (v | v << 4) & 0x10c30c30c30c30c3ull;
+    v = (v | v << 2) & 0x1249249249249249ull;
+    return v;
+}
+__host__ __device__ inline uint64_t morton_compact3(uint64_t v) {
+    v &= 0x1249249249249249ull;
+    v = (v ^ (v >> 2)) & 0x10c30c30c30c30c3ull;
+    v = (v ^ (v >> 4)) & 0x100f00f00f00f00full;
+    v = (v ^ (v >> 8)) & 0x1f0000ff0000ffull;
+    v = (v ^ (v >> 16)) & 0x1f00000000ffffull;
+    v = (v ^ (v >> 32)) & 0x1fffffull;
+    return v;
+}
+__host__ __device__ inline int64_t block_key(int zorder, const int64_t* bsz, int64_t bx, int64_t by, int64_t bz) {
+    if (zorder) return (int64_t)(morton_spread3(bx) | morton_spread3(by) << 1 | morton_spread3(bz) << 2);
+    return bx + bsz[0] * (by + bsz[1] * bz);
+}
+__host__ __device__ inline void block_coords(int zorder, const int64_t* bsz, int64_t key, int64_t* bc) {
+    if (zorder) {
+        bc[0] = (int64_t)morton_compact3((uint64_t)key);
+        bc[1] = (int64_t)morton_compact3((uint64_t)key >> 1);
+        bc[2] = (int64_t)morton_compact3((uint64_t)key >> 2);
+        return;
+    }
+    bc[0] = key % bsz[0];
+    bc[1] = (key / bsz[0]) % bsz[1];
+    bc[2] = key / (bsz[0] * bsz[1]);
+}
 template <typename T> struct sgb_type_of;
 template <> struct sgb_type_of<float> { static constexpr int value = SGB_F32; };
 template <> struct sgb_type_of<int> { static constexpr int value = SGB_I32; };
@@ -251,8 +286,9 @@ __global__ void conv_kernel(sgb_view v, int src0, int src1, int dst0, int dst1, 
             for (int p = 0; p < NP; ++p) tile[p][cell] = sc >= 0 ? src[p][idx] : bck[p];
         }
         __syncthreads();
-        const int64_t key = v.keys[chunk];
-        const int64_t bx = key % v.bsz[0], by = (key / v.bsz[0]) % v.bsz[1], bz = key / (v.bsz[0] * v.bsz[1]);
+        int64_t bcd[3];
+        detail::block_coords(v.zorder, v.bsz, v.keys[chunk], bcd);
+        const int64_t bx = bcd[0], by = bcd[1], bz = bcd[2];
         for (int pnt = threadIdx.x; pnt < BS; pnt += blockDim.x) {
             const int i = pnt % E, j = (pnt / E) % E, k = pnt / (E * E);
             const uint8_t m = v.mask[chunk * BS + pnt];
@@ -316,11 +352,8 @@ struct SparseGridGpu_ker {
     // grid_smb::LinId (src/Grid/Geometry/grid_smb.hpp:176-190)
     template <typename CoordT>
     __device__ int64_t getLinId(const grid_key_dx<3, CoordT>& c) const {
-        int64_t b = c.get(2) / E, l = c.get(2) % E;
-        b = b * v.bsz[1] + c.get(1) / E;
-        l = l * E + c.get(1) % E;
-        b = b * v.bsz[0] + c.get(0) / E;
-        l = l * E + c.get(0) % E;
+        const int64_t b = detail::block_key(v.zorder, v.bsz, c.get(0) / E, c.get(1) / E, c.get(2) / E);
+        const int64_t l = ((c.get(2) % E) * E + c.get(1) % E) * E + c.get(0) % E;
         return b * (E * E * E) + l;
     }
 
@@ -373,8 +406,21 @@ struct SparseGridGpu_ker {
 };
 
 // ------------------------------------------------------------------ host class
+// layout and linearizer tags of the reference's template parameters
+template <typename T>
+struct memory_traits_inte {};
+template <unsigned dim, unsigned blockEdgeSize, typename indexT = long>
+struct grid_smb {
+    static constexpr int zorder = 0;
+};
+template <unsigned dim, unsigned blockEdgeSize, typename indexT = long>
+struct grid_zmb {
+    static constexpr int zorder = 1;
+};
+
 template <unsigned dim, typename AggregateT, unsigned blockEdgeSize = 8, unsigned threadBlockSize = 512,
-          typename indexT = long>
+          typename indexT = long, template <typename> class layout_base = memory_traits_inte,
+          typename linearizer = grid_smb<dim, blockEdgeSize, indexT>>
 class SparseGridGpu {
     static_assert(dim == 3, "this build runs 3-D sparse grids");
     static_assert(blockEdgeSize == 8 || blockEdgeSize == 4, "chunk edge 8 or 4");
@@ -425,6 +471,7 @@ class SparseGridGpu {
         for (unsigned d = 0; d < 3; ++d) size_[d] = res[d], sz[d] = (int64_t)res[d];
         auto types = detail::types_of<props>::get();
         check(sgb_create(&g_, 3, blockEdgeSize, sz, (int)nprop, types.data(), device), "sgb_create");
+        if (linearizer::zorder) check(sgb_set_linearizer(g_, SGB_LIN_ZMB), "sgb_set_linearizer");
     }
     SparseGridGpu(const SparseGridGpu&) = delete;
     SparseGridGpu& operator=(const SparseGridGpu&) = delete;
@@ -563,7 +610,8 @@ class SparseGridGpu {
         using T = typename std::tuple_element<p, props>::type;
         int64_t bsz[3];
         for (int d = 0; d < 3; ++d) bsz[d] = ((int64_t)size_[d] + blockEdgeSize - 1) / blockEdgeSize;
-        const int64_t b = ((c.get(2) / blockEdgeSize) * bsz[1] + c.get(1) / blockEdgeSize) * bsz[0] + c.get(0) / blockEdgeSize;
+        const int64_t b = detail::block_key(linearizer::zorder, bsz, c.get(0) / blockEdgeSize, c.get(1) / blockEdgeSize,
+                                            c.get(2) / blockEdgeSize);
         const int64_t l = ((c.get(2) % blockEdgeSize) * blockEdgeSize + c.get(1) % blockEdgeSize) * blockEdgeSize +
                           c.get(0) % blockEdgeSize;
         const int64_t n = (int64_t)h_keys_.size();
@@ -581,7 +629,8 @@ class SparseGridGpu {
     unsigned char getFlag(const grid_key_dx<dim, CoordT>& c) const {
         int64_t bsz[3];
         for (int d = 0; d < 3; ++d) bsz[d] = ((int64_t)size_[d] + blockEdgeSize - 1) / blockEdgeSize;
-        const int64_t b = ((c.get(2) / blockEdgeSize) * bsz[1] + c.get(1) / blockEdgeSize) * bsz[0] + c.get(0) / blockEdgeSize;
+        const int64_t b = detail::block_key(linearizer::zorder, bsz, c.get(0) / blockEdgeSize, c.get(1) / blockEdgeSize,
+                                            c.get(2) / blockEdgeSize);
         const int64_t l = ((c.get(2) % blockEdgeSize) * blockEdgeSize + c.get(1) % blockEdgeSize) * blockEdgeSize +
                           c.get(0) % blockEdgeSize;
         for (size_t i = 0; i < h_keys_.size(); ++i)
@@ -793,5 +842,11 @@ class SparseGridGpu {
         }
     }
 };
+
+// SparseGridGpu_z (src/SparseGridGpu/SparseGridGpu.hpp:3948-3960): chunk ids by Morton code
+template <unsigned dim, typename AggregateT, unsigned blockEdgeSize = 8, unsigned threadBlockSize = 512,
+          typename indexT = long, template <typename> class layout_base = memory_traits_inte,
+          typename linearizer = grid_zmb<dim, blockEdgeSize, indexT>>
+using SparseGridGpu_z = SparseGridGpu<dim, AggregateT, blockEdgeSize, threadBlockSize, indexT, layout_base, linearizer>;
 
 }  // namespace openfpm_b200

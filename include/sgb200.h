@@ -96,6 +96,17 @@ int sgb_create(sgb_grid** out, int dim, int edge, const int64_t* size, int nprop
                int device);
 int sgb_destroy(sgb_grid* g);
 
+/* Chunk-id linearizer: SGB_LIN_SMB, grid_smb (block x fastest, the
+ * default), or SGB_LIN_ZMB, grid_zmb (3-D Morton code of the block
+ * coordinate, SparseGridGpu_z, src/Grid/Geometry/grid_zmb.hpp:25-104,
+ * src/SparseGridGpu/SparseGridGpu.hpp:3948-3960); offsets inside a chunk
+ * are x fastest for both.  Chosen while the grid is empty; SGB_LIN_ZMB needs
+ * 3-D and at most 2^21 blocks per dimension.  Stencils on Morton grids run
+ * the one-chunk-per-CTA kernel; batches and the scene builder take
+ * SGB_LIN_SMB grids only. */
+typedef enum { SGB_LIN_SMB = 0, SGB_LIN_ZMB = 1 } sgb_linearizer;
+int sgb_set_linearizer(sgb_grid* g, int kind);
+
 /* setBackgroundValue<p> (SparseGridGpu.hpp:2878-2884); value host. */
 int sgb_set_background(sgb_grid* g, int prop, const void* value_host);
 
@@ -136,6 +147,7 @@ typedef struct {
     void* data[8];
     const uint8_t* mask;
     const int32_t* nn;
+    int zorder; /* chunk ids: 0 grid_smb (x fastest), 1 grid_zmb (Morton) */
 } sgb_view;
 int sgb_get_view(sgb_grid* g, int nn_kind, sgb_view* out, sgb_stream s);
 

@@ -22,6 +22,7 @@ OP_NONE, OP_RIGHT, OP_LEFT, OP_ADD, OP_MAX, OP_MIN, OP_OR = range(7)
 NN_STAR, NN_FULL = 0, 1
 # stencils (sgb_stencil)
 HEAT7, GS7, BOX27, BOX27_NS = 0, 1, 2, 3
+LIN_SMB, LIN_ZMB = 0, 1
 
 # every entry point of include/sgb200.h: name -> (restype, argtypes)
 _vp, _i32, _i64 = C.c_void_p, C.c_int, C.c_int64
@@ -41,6 +42,7 @@ SIGNATURES = {
     "sgb_existing_points": (_i32, [_vp, _vp, _vp, _i64, _vp, _vp]),
     "sgb_calc_existing_points": (_i32, [_vp, _vp, _vp]),
     "sgb_existing_point_list": (_i32, [_vp, _vp, _vp, _vp]),
+    "sgb_set_linearizer": (_i32, [_vp, _i32]),
     "sgb_construct_link_dw": (_i32, [_vp, _vp, _vp, _vp, _vp]),
     "sgb_construct_link_up": (_i32, [_vp, _vp, _vp, _vp, _vp]),
     "sgb_get_links": (_i32, [_vp, _i32, _vp]),

@@ -210,6 +210,10 @@ int sgb_batch_add(sgb_batch* b, sgb_grid* g, int kind, const int* src, const int
         set_error("batches run HEAT7 or GS7");
         return SGB_ENOTSUP;
     }
+    if (g->geo.zorder) {
+        set_error("batches hold grids with x-fastest chunk ids");
+        return SGB_ENOTSUP;
+    }
     if (b->kind >= 0 && (b->kind != kind || b->edge != g->geo.edge)) {
         set_error("all grids of a batch share the stencil kind and the chunk edge");
         return SGB_EINVAL;

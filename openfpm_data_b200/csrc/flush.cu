@@ -457,7 +457,7 @@ extern "C" int sgb_flush(sgb_grid* g, const int* ops, sgb_stream stream) {
                       : "an insert pool counted more points than its slots; the staged inserts were dropped");
         return SGB_ERANGE;
     }
-    const int64_t maxlin = g->geo.bsz[0] * g->geo.bsz[1] * g->geo.bsz[2] * g->geo.bs;
+    const int64_t maxlin = key_space(g->geo) * g->geo.bs;
     int bits = 0;
     while (bits < 63 && (int64_t(1) << bits) < maxlin) ++bits;
     int st;

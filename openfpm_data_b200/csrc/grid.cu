@@ -187,8 +187,9 @@ int fill_background_all(sgb_grid* g, int p, cudaStream_t s) {
     return SGB_OK;
 }
 
-// grid_smb::LinId on device (src/Grid/Geometry/grid_smb.hpp:176-190), with a
-// domain check that the reference does not do.
+// grid_smb::LinId / grid_zmb::LinId on device (src/Grid/Geometry/
+// grid_smb.hpp:176-190, grid_zmb.hpp:63-76), with a domain check that the
+// reference does not do.
 __global__ void k_lin_from_coords(const int32_t* coords, int64_t n, Geometry geo, int64_t* lin, unsigned* err) {
     int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -203,19 +204,16 @@ __global__ void k_lin_from_coords(const int32_t* coords, int64_t n, Geometry geo
         lin[i] = -1;
         return;
     }
-    int64_t b = c[geo.dim - 1] / geo.edge, l = c[geo.dim - 1] % geo.edge;
-    for (int d = geo.dim - 2; d >= 0; --d) {
-        b = b * geo.bsz[d] + c[d] / geo.edge;
-        l = l * geo.edge + c[d] % geo.edge;
-    }
+    int64_t b, l;
+    point_key(geo, c, &b, &l);
     lin[i] = b * geo.bs + l;
 }
 
-__global__ void k_check_lin(const int64_t* lin_in, int64_t n, int64_t maxlin, int64_t* lin_out, unsigned* err) {
+__global__ void k_check_lin(const int64_t* lin_in, int64_t n, Geometry geo, int64_t* lin_out, unsigned* err) {
     int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= n) return;
     int64_t v = lin_in[i];
-    if (v < 0 || v >= maxlin) {
+    if (v < 0 || !key_in_domain(geo, v / geo.bs)) {
         atomicOr(err, kErrOutOfDomain);
         v = -1;
     }
@@ -242,13 +240,18 @@ __global__ void k_get(const int32_t* coords, int64_t n, Geometry geo, const int6
                       const T* data, const uint8_t* mask, T* out) {
     int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= n) return;
-    int64_t c[3];
-    for (int d = 0; d < geo.dim; ++d) c[d] = coords[i * geo.dim + d];
-    int64_t b = c[geo.dim - 1] / geo.edge, l = c[geo.dim - 1] % geo.edge;
-    for (int d = geo.dim - 2; d >= 0; --d) {
-        b = b * geo.bsz[d] + c[d] / geo.edge;
-        l = l * geo.edge + c[d] % geo.edge;
+    int64_t c[3] = {0, 0, 0};
+    bool inside = true;
+    for (int d = 0; d < geo.dim; ++d) {
+        c[d] = coords[i * geo.dim + d];
+        inside &= c[d] >= 0 && c[d] < geo.size[d];
     }
+    if (!inside) {  // outside the domain: the background
+        out[i] = data[(size_t)nchunks * geo.bs];
+        return;
+    }
+    int64_t b, l;
+    point_key(geo, c, &b, &l);
     int64_t pos = find_key(keys, nchunks, b);
     if (pos < 0) pos = nchunks;
     // BlockMapGpu_ker::get (src/SparseGridGpu/BlockMapGpu_ker.cuh:117-135)
@@ -280,13 +283,13 @@ struct PoolCopy {
 // One CTA per pool: its first counts[b] slots, in slot order, after the
 // pools before it.
 __global__ void k_pool_copy(const uint32_t* counts, const uint32_t* off, int64_t nslot, const int64_t* lin,
-                            int64_t maxlin, int64_t* out_lin, PoolCopy pc, unsigned* err) {
+                            Geometry geo, int64_t* out_lin, PoolCopy pc, unsigned* err) {
     const int64_t b = blockIdx.x;
     const uint32_t c = counts[b], o = off[b];
     for (uint32_t k = threadIdx.x; k < c; k += blockDim.x) {
         const int64_t src = b * nslot + k, dst = (int64_t)o + k;
         int64_t v = lin[src];
-        if (v < 0 || v >= maxlin) {
+        if (v < 0 || !key_in_domain(geo, v / geo.bs)) {
             atomicOr(err, kErrOutOfDomain);
             v = -1;
         }
@@ -456,8 +459,7 @@ int sgb_insert_lin(sgb_grid* g, int64_t n, const int64_t* lin, const void* const
     if (n == 0) return SGB_OK;
     cudaStream_t s = (cudaStream_t)stream;
     SGB_TRY(g->pend_lin.reserve((size_t)(g->npend + n) * 8));
-    const int64_t maxlin = g->geo.bsz[0] * g->geo.bsz[1] * g->geo.bsz[2] * g->geo.bs;
-    k_check_lin<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(lin, n, maxlin, g->pend_lin.as<int64_t>() + g->npend,
+    k_check_lin<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(lin, n, g->geo, g->pend_lin.as<int64_t>() + g->npend,
                                                              g->err.as<unsigned>());
     SGB_CUDA(cudaGetLastError());
     SGB_TRY(stage_values(g, n, values, s));
@@ -496,11 +498,29 @@ int sgb_insert_pools(sgb_grid* g, int64_t npools, int64_t nslot, const int32_t* 
         pc.es[p] = es;
         pc.bck[p] = bck_pattern(g, p);
     }
-    const int64_t maxlin = g->geo.bsz[0] * g->geo.bsz[1] * g->geo.bsz[2] * g->geo.bs;
-    k_pool_copy<<<(unsigned)npools, 128, 0, s>>>(cnt.as<uint32_t>(), off.as<uint32_t>(), nslot, lin, maxlin,
+    k_pool_copy<<<(unsigned)npools, 128, 0, s>>>(cnt.as<uint32_t>(), off.as<uint32_t>(), nslot, lin, g->geo,
                                                  g->pend_lin.as<int64_t>() + g->npend, pc, g->err.as<unsigned>());
     SGB_CUDA(cudaGetLastError());
     g->npend += add;
+    return SGB_OK;
+}
+
+int sgb_set_linearizer(sgb_grid* g, int kind) {
+    if (!g || (kind != SGB_LIN_SMB && kind != SGB_LIN_ZMB)) return SGB_EINVAL;
+    if (g->n != 0 || g->npend != 0) {
+        set_error("the chunk linearizer is chosen while the grid is empty");
+        return SGB_ESTATE;
+    }
+    if (kind == SGB_LIN_ZMB) {
+        if (g->geo.dim != 3) return SGB_ENOTSUP;
+        for (int d = 0; d < 3; ++d)
+            if (g->geo.bsz[d] > (int64_t(1) << 21)) {
+                set_error("Morton chunk ids hold 21 bits per block coordinate");
+                return SGB_ENOTSUP;
+            }
+    }
+    g->geo.zorder = kind == SGB_LIN_ZMB;
+    g->nn_valid[0] = g->nn_valid[1] = false;
     return SGB_OK;
 }
 
@@ -519,6 +539,7 @@ int sgb_get_view(sgb_grid* g, int nn_kind, sgb_view* out, sgb_stream stream) {
         out->size[d] = g->geo.size[d];
         out->bsz[d] = g->geo.bsz[d];
     }
+    out->zorder = g->geo.zorder;
     out->keys = g->keys.as<int64_t>();
     for (int p = 0; p < g->nprop; ++p) out->data[p] = g->data[p].p;
     out->mask = g->mask.as<uint8_t>();

@@ -60,7 +60,96 @@ struct Geometry {
     int dim = 3, edge = 8, bs = 512;
     int64_t size[3] = {1, 1, 1};
     int64_t bsz[3] = {1, 1, 1};
+    int zorder = 0;  // chunk ids: 0 grid_smb (x fastest), 1 grid_zmb (Morton)
 };
+
+// Morton spreading / compaction of 21-bit coordinates (the published
+// "magic bits" bit-interleaving method): bit i of v moves to bit 3i.
+__host__ __device__ inline uint64_t morton_spread3(uint64_t v) {
+    v &= 0x1fffffull;
+    v = (v | v << 32) & 0x1f00000000ffffull;
+    v = (v | v << 16) & 0x1f0000ff0000ffull;
+    v = (v | v << 8) & 0x100f00f00f00f00full;
+    v = (v | v << 4) & 0x10c30c30c30c30c3ull;
+    v = (v | v << 2) & 0x1249249249249249ull;
+    return v;
+}
+__host__ __device__ inline uint64_t morton_compact3(uint64_t v) {
+    v &= 0x1249249249249249ull;
+    v = (v ^ (v >> 2)) & 0x10c30c30c30c30c3ull;
+    v = (v ^ (v >> 4)) & 0x100f00f00f00f00full;
+    v = (v ^ (v >> 8)) & 0x1f0000ff0000ffull;
+    v = (v ^ (v >> 16)) & 0x1f00000000ffffull;
+    v = (v ^ (v >> 32)) & 0x1fffffull;
+    return v;
+}
+
+// Chunk id of an in-domain block coordinate: grid_smb::BlockLinId
+// (src/Grid/Geometry/grid_smb.hpp:280-299) or grid_zmb::BlockLinId = lin_zid
+// (src/Grid/Geometry/grid_zmb.hpp:100-104, src/util/zmorton.hpp:72-98).
+__host__ __device__ inline int64_t block_key(const Geometry& g, int64_t bx, int64_t by, int64_t bz) {
+    if (g.zorder)
+        return (int64_t)(morton_spread3((uint64_t)bx) | morton_spread3((uint64_t)by) << 1 |
+                         morton_spread3((uint64_t)bz) << 2);
+    return bx + g.bsz[0] * (by + g.bsz[1] * bz);
+}
+
+// Block coordinate of a chunk id (BlockInvLinId of either linearizer).
+__host__ __device__ inline void block_coords(const Geometry& g, int64_t key, int64_t* bc) {
+    if (g.zorder) {
+        bc[0] = (int64_t)morton_compact3((uint64_t)key);
+        bc[1] = (int64_t)morton_compact3((uint64_t)key >> 1);
+        bc[2] = (int64_t)morton_compact3((uint64_t)key >> 2);
+        return;
+    }
+    bc[0] = key % g.bsz[0];
+    bc[1] = (key / g.bsz[0]) % g.bsz[1];
+    bc[2] = key / (g.bsz[0] * g.bsz[1]);
+}
+
+// Lowest point of a chunk.
+__host__ __device__ inline void chunk_origin(const Geometry& g, int64_t key, int64_t* o) {
+    block_coords(g, key, o);
+    for (int d = 0; d < 3; ++d) o[d] *= g.edge;
+}
+
+// Number of chunk ids the linearizer can produce for the domain (ids are below it).
+__host__ __device__ inline int64_t key_space(const Geometry& g) {
+    if (!g.zorder) return g.bsz[0] * g.bsz[1] * g.bsz[2];
+    int64_t m = g.bsz[0] > g.bsz[1] ? g.bsz[0] : g.bsz[1];
+    m = m > g.bsz[2] ? m : g.bsz[2];
+    int64_t p = 1;
+    while (p < m) p <<= 1;
+    return p * p * p;
+}
+
+// Chunk id and offset in the chunk of an in-domain point: grid_smb::LinId
+// (src/Grid/Geometry/grid_smb.hpp:176-190) / grid_zmb::LinId
+// (src/Grid/Geometry/grid_zmb.hpp:63-76); the offset is x fastest for both.
+__host__ __device__ inline void point_key(const Geometry& g, const int64_t* c, int64_t* key, int64_t* local) {
+    const int e = g.edge;
+    if (g.zorder) {
+        *key = block_key(g, c[0] / e, c[1] / e, c[2] / e);
+        *local = c[0] % e + e * (c[1] % e + e * (c[2] % e));
+        return;
+    }
+    int64_t b = c[g.dim - 1] / e, l = c[g.dim - 1] % e;
+    for (int d = g.dim - 2; d >= 0; --d) {
+        b = b * g.bsz[d] + c[d] / e;
+        l = l * e + c[d] % e;
+    }
+    *key = b;
+    *local = l;
+}
+
+// Is a chunk id one of a block inside the domain?
+__host__ __device__ inline bool key_in_domain(const Geometry& g, int64_t key) {
+    if (key < 0 || key >= key_space(g)) return false;
+    if (!g.zorder) return true;
+    int64_t bc[3];
+    block_coords(g, key, bc);
+    return bc[0] < g.bsz[0] && bc[1] < g.bsz[1] && bc[2] < g.bsz[2];
+}
 
 // Launch parameters of the fixed-function stencils.
 struct StencilParams {

@@ -41,20 +41,22 @@ struct OtherGrid {
 
 __device__ __forceinline__ void coords_of(const Geometry& geo, int64_t key, int off, int64_t* p) {
     const int e = geo.edge;
-    p[0] = (key % geo.bsz[0]) * e + off % e;
-    p[1] = ((key / geo.bsz[0]) % geo.bsz[1]) * e + (off / e) % e;
-    p[2] = (key / (geo.bsz[0] * geo.bsz[1])) * e + off / (e * e);
+    chunk_origin(geo, key, p);
+    p[0] += off % e;
+    p[1] += (off / e) % e;
+    p[2] += off / (e * e);
 }
 
 // grid_smb::LinId (src/Grid/Geometry/grid_smb.hpp:176-190) then
 // BlockMapGpu_ker::get_sparse(unsigned int linId) (BlockMapGpu_ker.cuh:234-249).
 __device__ __forceinline__ bool other_exists(const OtherGrid& o, const int64_t* c, int32_t* pos, int16_t* off) {
-    const int64_t e = o.geo.edge;
-    int64_t blk = c[2] / e, loc = c[2] % e;
-    for (int d = 1; d >= 0; --d) {
-        blk = blk * o.geo.bsz[d] + c[d] / e;
-        loc = loc * e + c[d] % e;
+    int64_t blk, loc;
+    if (o.geo.zorder && (c[0] < 0 || c[1] < 0 || c[2] < 0)) {
+        *pos = (int32_t)o.n;  // absent: see sgb_construct_link_dw
+        *off = 0;
+        return false;
     }
+    point_key(o.geo, c, &blk, &loc);
     const uint32_t lin = (uint32_t)(blk * o.geo.bs + loc);
     const uint32_t b = lin / (uint32_t)o.geo.bs, ofs = lin % (uint32_t)o.geo.bs;
     int64_t p = find_key(o.keys, o.n, (int64_t)b);

@@ -10,7 +10,15 @@ namespace sgb {
 // upper bound is checked, so a block coordinate of -1 along x or y yields the
 // id of a block one row (or slice) back -- reproduced on purpose, it decides
 // which chunk an NNFull neighbour lookup returns at the low faces.
+//
+// grid_zmb::BlockLinId (lin_zid, src/util/zmorton.hpp:72-98) checks nothing;
+// a negative coordinate there gives an id far above every chunk's, so it is
+// absent like one past the upper faces: -1 here.
 __device__ __forceinline__ int64_t block_lin_ref(const Geometry& geo, const int64_t* bc) {
+    if (geo.zorder) {
+        if (bc[0] < 0 || bc[1] < 0 || bc[2] < 0) return -1;
+        return block_key(geo, bc[0], bc[1], bc[2]);
+    }
     int64_t lin = bc[geo.dim - 1];
     if (lin >= geo.bsz[geo.dim - 1]) return -1;
     for (int d = geo.dim - 2; d >= 0; --d) {
@@ -31,12 +39,8 @@ __global__ void k_find_nn(const int64_t* keys, int64_t n, Geometry geo, int kind
     const int64_t chunk = t / nnn;
     const int o = (int)(t - chunk * nnn);
     if (chunk >= n) return;
-    int64_t b = keys[chunk];
     int64_t bc[3];
-    for (int d = 0; d < geo.dim; ++d) {
-        bc[d] = b % geo.bsz[d];
-        b /= geo.bsz[d];
-    }
+    block_coords(geo, keys[chunk], bc);
     int64_t pos = -1;
     if (kind == SGB_NN_STAR) {
         if (o < 2 * geo.dim) {

@@ -59,11 +59,7 @@ static PackLayout layout_of(int64_t n_cnk, int64_t n_pnt, int np, const int* es)
     return L;
 }
 
-__device__ __forceinline__ void origin_of(const Geometry& geo, int64_t key, int64_t* o) {
-    o[0] = (key % geo.bsz[0]) * geo.edge;
-    o[1] = ((key / geo.bsz[0]) % geo.bsz[1]) * geo.edge;
-    o[2] = (key / (geo.bsz[0] * geo.bsz[1])) * geo.edge;
-}
+__device__ __forceinline__ void origin_of(const Geometry& geo, int64_t key, int64_t* o) { chunk_origin(geo, key, o); }
 
 struct Box6 {
     int64_t b[6];
@@ -245,12 +241,8 @@ __global__ void k_unpack_stage(const unsigned char* __restrict__ buf, PackLayout
     for (int d = 0; d < 3; ++d) ok = ok && c[d] >= 0 && c[d] < dst_geo.size[d];
     int64_t lin = -1;
     if (ok) {
-        const int de = dst_geo.edge;
-        int64_t b = c[2] / de, l = c[2] % de;
-        b = b * dst_geo.bsz[1] + c[1] / de;
-        l = l * de + c[1] % de;
-        b = b * dst_geo.bsz[0] + c[0] / de;
-        l = l * de + c[0] % de;
+        int64_t b, l;
+        point_key(dst_geo, c, &b, &l);
         lin = b * dst_geo.bs + l;
     } else {
         atomicOr(err, kErrOutOfDomain);

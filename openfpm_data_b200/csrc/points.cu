@@ -97,10 +97,9 @@ __global__ void __launch_bounds__(256) k_box27_points(const float* __restrict__ 
     const int x = off % E, y = (off / E) % E, z = off / (E * E);
     bool act = (m & 1) && !(m & 2);
     if (prm.has_box) {
-        const int64_t key = keys[c];
-        const int64_t ox = (key % geo.bsz[0]) * E, oy = ((key / geo.bsz[0]) % geo.bsz[1]) * E,
-                      oz = (key / (geo.bsz[0] * geo.bsz[1])) * E;
-        act = act && in_box(prm, ox + x, oy + y, oz + z);
+        int64_t o[3];
+        chunk_origin(geo, keys[c], o);
+        act = act && in_box(prm, o[0] + x, o[1] + y, o[2] + z);
     }
     if (!act) return;
     float tot = 0.0f;

@@ -22,12 +22,6 @@ struct UBox {
     uint32_t lo[3], hi[3];
 };
 
-__device__ __forceinline__ void chunk_origin(const Geometry& geo, int64_t key, int64_t* o) {
-    o[0] = (key % geo.bsz[0]) * geo.edge;
-    o[1] = ((key / geo.bsz[0]) % geo.bsz[1]) * geo.edge;
-    o[2] = (key / (geo.bsz[0] * geo.bsz[1])) * geo.edge;
-}
-
 struct BckSet {
     unsigned char* p[kMaxProps];
     uint64_t pat[kMaxProps];

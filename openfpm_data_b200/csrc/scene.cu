@@ -160,6 +160,10 @@ using namespace sgb;
 extern "C" int sgb_build_balls(sgb_grid* g, int nballs, const float* balls, int init, uint64_t seed, const int* props,
                                sgb_stream stream) {
     if (!g || !props || (init != 0 && init != 1)) return SGB_EINVAL;
+    if (g->geo.zorder) {
+        set_error("the scene builder writes x-fastest chunk ids");
+        return SGB_ENOTSUP;
+    }
     const int np = init == 1 ? 2 : 1;
     for (int j = 0; j < np; ++j)
         if (props[j] < 0 || props[j] >= g->nprop || g->ptype[props[j]] != SGB_F32) return SGB_EINVAL;

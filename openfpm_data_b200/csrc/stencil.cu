@@ -76,10 +76,11 @@ __global__ void __launch_bounds__(256) k_stencil_tile(FieldSet fs, const uint8_t
         __syncthreads();
         int64_t cx = 0, cy = 0, cz = 0;
         if (prm.has_box) {
-            const int64_t key = keys[chunk];
-            cx = (key % geo.bsz[0]) * E;
-            cy = ((key / geo.bsz[0]) % geo.bsz[1]) * E;
-            cz = (key / (geo.bsz[0] * geo.bsz[1])) * E;
+            int64_t o[3];
+            chunk_origin(geo, keys[chunk], o);
+            cx = o[0];
+            cy = o[1];
+            cz = o[2];
         }
         float* d0 = par ? fs.out[1][0] : fs.out[0][0];
         float* d1 = par ? fs.out[1][NP - 1] : fs.out[0][NP - 1];
@@ -193,7 +194,9 @@ GridInfo grid_info_of(const StencilParams& prm) {
 
 int launch_fields(const LaunchDesc& L, cudaStream_t s) {
     if (L.n == 0) return SGB_OK;
-    if (L.kind != SGB_BOX27 && L.edge == 8 && !L.use_tile) return launch_e8(L, s);
+    // the pipelined kernel takes the x halo from the neighbouring index positions, which hold the
+    // x neighbours only under the x-fastest chunk ids
+    if (L.kind != SGB_BOX27 && L.edge == 8 && !L.use_tile && !L.geo.zorder) return launch_e8(L, s);
     const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>(L.n, (int64_t)L.num_sms * 8));
 #define SGB_TILE(K, E) \
     k_stencil_tile<K, E><<<blocks, 256, 0, s>>>(L.fs, L.mask, L.nn, L.keys, L.gid, L.grids, L.g0, L.n, L.geo, L.prm, L.t)

@@ -136,9 +136,11 @@ __global__ void __launch_bounds__(kThreads8, KIND == SGB_GS7 ? 6 : 8)
         if (lane == 0) {
             if (BOX) {
                 const int64_t key = keys[c];
-                st.cx = (int32_t)((key % geo.bsz[0]) * 8);
-                st.cy = (int32_t)(((key / geo.bsz[0]) % geo.bsz[1]) * 8);
-                st.cz = (int32_t)((key / (geo.bsz[0] * geo.bsz[1])) * 8);
+                int64_t o[3];
+                chunk_origin(geo, key, o);
+                st.cx = (int32_t)o[0];
+                st.cy = (int32_t)o[1];
+                st.cz = (int32_t)o[2];
             }
             st.gi = gi;
 #pragma unroll

@@ -35,7 +35,7 @@ class _View(C.Structure):
     """sgb_view of include/sgb200.h."""
     _fields_ = [("n", C.c_int64), ("edge", C.c_int), ("bs", C.c_int), ("nprop", C.c_int), ("nn_kind", C.c_int),
                 ("size", C.c_int64 * 3), ("bsz", C.c_int64 * 3), ("keys", C.c_void_p), ("data", C.c_void_p * 8),
-                ("mask", C.c_void_p), ("nn", C.c_void_p)]
+                ("mask", C.c_void_p), ("nn", C.c_void_p), ("zorder", C.c_int)]
 
 
 def _stream(stream=None) -> int:
@@ -59,7 +59,10 @@ class _DevView:
 class SparseGridGpu:
     """SparseGridGpu(size, props, edge): a 3-D sparse block grid on one GPU."""
 
-    def __init__(self, size: Sequence[int], props: Sequence[str] = ("f32",), edge: int = 8, device: int = 0):
+    def __init__(self, size: Sequence[int], props: Sequence[str] = ("f32",), edge: int = 8, device: int = 0,
+                 linearizer: str = "smb"):
+        """linearizer "smb" (grid_smb, block x fastest) or "zmb" (grid_zmb Morton chunk ids,
+        SparseGridGpu_z)."""
         lib = L.load()
         self.size = tuple(int(s) for s in size)
         self.edge = int(edge)
@@ -73,6 +76,11 @@ class SparseGridGpu:
         self._h = h
         self._lib = lib
         self.bck = [0] * len(self.ptypes)
+        self.linearizer = linearizer
+        if linearizer not in ("smb", "zmb"):
+            raise ValueError("linearizer is 'smb' or 'zmb'")
+        if linearizer == "zmb":
+            L.check(lib.sgb_set_linearizer(h, L.LIN_ZMB), "sgb_set_linearizer")
 
     def close(self):
         if getattr(self, "_h", None):
@@ -143,7 +151,8 @@ class SparseGridGpu:
         L.check(self._lib.sgb_get_view(self._h, nn, C.byref(v), _stream(stream)), "sgb_get_view")
         return {"n": v.n, "edge": v.edge, "bs": v.bs, "nprop": v.nprop, "nn_kind": v.nn_kind,
                 "size": tuple(v.size), "bsz": tuple(v.bsz), "keys": v.keys or 0,
-                "data": [v.data[p] or 0 for p in range(v.nprop)], "mask": v.mask or 0, "nn": v.nn or 0}
+                "data": [v.data[p] or 0 for p in range(v.nprop)], "mask": v.mask or 0, "nn": v.nn or 0,
+                "zorder": v.zorder}
 
     def flush(self, ops: Iterable, stream=None) -> None:
         """flush<ops...>: one reduction per property (sgb_op ids or reference names)."""

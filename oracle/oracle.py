@@ -68,6 +68,7 @@ def _load():
         _lib.sgo_gs7.argtypes = [vp, i32, i32, i32, i32, f, f, f, f, f, vp]
         _lib.sgo_box27.argtypes = [vp, i32, i32, vp, vp]
         _lib.sgo_box27_ns.argtypes = [vp, i32, i32, vp, vp]
+        _lib.sgo_set_zorder.argtypes = [vp, i32]
         d = C.c_double
         _lib.sgo_heat7_f64.argtypes = [vp, vp, vp, d, d, i32]
         _lib.sgo_gs7_f64.argtypes = [vp, vp, vp, vp, vp, d, d, d, d, d, d, d, i32]
@@ -104,8 +105,9 @@ def _ptr_array(arrs):
 class OracleGrid:
     """CPU restatement of one SparseGridGpu block map."""
 
-    def __init__(self, size, edge=8, ptypes=(T_F32,), dim=None):
+    def __init__(self, size, edge=8, ptypes=(T_F32,), dim=None, zorder=False):
         lib, _ = _load()
+        self.zorder = bool(zorder)
         self.dim = dim if dim is not None else len(size)
         self.edge = edge
         self.bs = edge ** self.dim
@@ -114,6 +116,37 @@ class OracleGrid:
         sz = np.array(self.size, dtype=np.int64)
         pt = np.array(self.ptypes, dtype=np.int32)
         self._h = lib.sgo_create(self.dim, edge, _ptr(sz), len(self.ptypes), _ptr(pt))
+        if self.zorder:
+            lib.sgo_set_zorder(self._h, 1)
+
+    # -- chunk ids (grid_smb: block x fastest; grid_zmb: Morton code, src/util/zmorton.hpp) --
+    def _bsz(self):
+        return [(int(s) + self.edge - 1) // self.edge for s in self.size]
+
+    def block_key(self, bc):
+        """Chunk ids of non-negative block coordinates [m, 3]."""
+        bc = np.asarray(bc, dtype=np.int64).reshape(-1, 3)
+        if not self.zorder:
+            b = self._bsz()
+            return bc[:, 0] + b[0] * (bc[:, 1] + b[1] * bc[:, 2])
+        k = np.zeros(len(bc), dtype=np.uint64)
+        for i in range(21):
+            for d in range(3):
+                k |= ((bc[:, d].astype(np.uint64) >> np.uint64(i)) & np.uint64(1)) << np.uint64(3 * i + d)
+        return k.astype(np.int64)
+
+    def block_coords(self, keys, size=None):
+        """Block coordinates [m, 3] of chunk ids (size: the grid size the ids were made for)."""
+        keys = np.asarray(keys, dtype=np.int64)
+        if not self.zorder:
+            b = self._bsz() if size is None else [(int(s) + self.edge - 1) // self.edge for s in size]
+            return np.stack([keys % b[0], (keys // b[0]) % b[1], keys // (b[0] * b[1])], axis=1)
+        u = keys.astype(np.uint64)
+        bc = np.zeros((len(keys), 3), dtype=np.int64)
+        for i in range(21):
+            for d in range(3):
+                bc[:, d] |= (((u >> np.uint64(3 * i + d)) & np.uint64(1)).astype(np.int64)) << i
+        return bc
 
     def __del__(self):
         if getattr(self, "_h", None) and _lib is not None:
@@ -261,9 +294,7 @@ class OracleGrid:
             q += _up8(2 * n_pnt)
             q += _up8(n_pnt)
             chunk = np.repeat(np.arange(n_cnk), np.diff(scan.astype(np.int64)))
-            bsz = [(int(s) + self.edge - 1) // self.edge for s in hdr[3:]]
-            key = ids[chunk]
-            org = np.stack([key % bsz[0], (key // bsz[0]) % bsz[1], key // (bsz[0] * bsz[1])], axis=1) * self.edge
+            org = self.block_coords(ids[chunk], size=hdr[3:]) * self.edge
             e = self.edge
             coords = org + np.stack([offs % e, (offs // e) % e, offs // (e * e)], axis=1)
             if starts is not None:
@@ -283,11 +314,20 @@ class OracleGrid:
         bsz = [(s + e - 1) // e for s in self.size]
         q = lambda a: np.sign(a) * (np.abs(a) // e)  # noqa: E731  (truncating division by e)
         r = lambda a: a - q(a) * e  # noqa: E731
-        blk, loc = q(c[:, 2]), r(c[:, 2])
-        for d in (1, 0):
-            blk = blk * bsz[d] + q(c[:, d])
-            loc = loc * e + r(c[:, d])
-        lin = (blk * self.bs + loc) & 0xFFFFFFFF
+        if self.zorder:
+            # Morton ids: a negative coordinate is absent (its id lies above every chunk's)
+            neg = np.any(c < 0, axis=1)
+            cc = np.where(neg[:, None], 0, c)
+            blk = self.block_key(cc // e)
+            loc = cc[:, 0] % e + e * (cc[:, 1] % e + e * (cc[:, 2] % e))
+            blk = np.where(neg, -1, blk)
+        else:
+            blk, loc = q(c[:, 2]), r(c[:, 2])
+            for d in (1, 0):
+                blk = blk * bsz[d] + q(c[:, d])
+                loc = loc * e + r(c[:, d])
+        lin = np.where(blk < 0, -1, (blk * self.bs + loc) & 0xFFFFFFFF) if self.zorder else \
+            (blk * self.bs + loc) & 0xFFFFFFFF
         b, off = lin // self.bs, lin % self.bs
         pos = np.searchsorted(keys, b)
         found = (pos < len(keys)) & (keys[np.minimum(pos, max(len(keys) - 1, 0))] == b) if len(keys) else \

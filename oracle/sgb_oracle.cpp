@@ -45,6 +45,7 @@ int elem_size(int t) { return t == T_F64 ? 8 : (t == T_U8 ? 1 : 4); }
 
 struct Grid {
     int dim = 3, edge = 8, bs = 512;
+    bool zorder = false;  // chunk ids: grid_smb (false) or grid_zmb Morton codes (true)
     int64_t sz[3] = {1, 1, 1}, bsz[3] = {1, 1, 1};
     int nprop = 0;
     std::vector<int> ptype;
@@ -69,9 +70,30 @@ struct Grid {
     }
 };
 
+// ---------------------------------------------------------------- grid_zmb
+// lin_zid / invlin_zid (src/util/zmorton.hpp:72-135): bit i of the block
+// coordinate along d is bit 3i + d of the chunk id (written here bit by bit).
+int64_t morton3(const int64_t* bc) {
+    uint64_t r = 0;
+    for (int i = 0; i < 21; ++i)
+        for (int d = 0; d < 3; ++d) r |= (((uint64_t)bc[d] >> i) & 1u) << (3 * i + d);
+    return (int64_t)r;
+}
+void inv_morton3(int64_t key, int64_t* bc) {
+    for (int d = 0; d < 3; ++d) {
+        bc[d] = 0;
+        for (int i = 0; i < 21; ++i) bc[d] |= (int64_t)((((uint64_t)key >> (3 * i + d)) & 1u) << i);
+    }
+}
+
 // ---------------------------------------------------------------- grid_smb
-// grid_smb::LinId (src/Grid/Geometry/grid_smb.hpp:176-190)
+// grid_smb::LinId (src/Grid/Geometry/grid_smb.hpp:176-190); grid_zmb::LinId
+// (grid_zmb.hpp:63-76) for Morton grids
 int64_t lin_id(const Grid& g, const int64_t* c) {
+    if (g.zorder) {
+        const int64_t bc[3] = {c[0] / g.edge, c[1] / g.edge, c[2] / g.edge};
+        return morton3(bc) * g.bs + (c[0] % g.edge) + g.edge * ((c[1] % g.edge) + g.edge * (c[2] % g.edge));
+    }
     int64_t b = c[g.dim - 1] / g.edge, l = c[g.dim - 1] % g.edge;
     for (int d = g.dim - 2; d >= 0; --d) {
         b = b * g.bsz[d] + c[d] / g.edge;
@@ -83,6 +105,14 @@ int64_t lin_id(const Grid& g, const int64_t* c) {
 // grid_smb::InvLinId (grid_smb.hpp:263-277)
 void inv_lin(const Grid& g, int64_t lin, int64_t* c) {
     int64_t b = lin / g.bs, l = lin % g.bs;
+    if (g.zorder) {
+        inv_morton3(b, c);
+        for (int d = 0; d < 3; ++d) {
+            c[d] = c[d] * g.edge + l % g.edge;
+            l /= g.edge;
+        }
+        return;
+    }
     for (int d = 0; d < g.dim; ++d) {
         c[d] = (b % g.bsz[d]) * g.edge + l % g.edge;
         b /= g.bsz[d];
@@ -92,6 +122,10 @@ void inv_lin(const Grid& g, int64_t lin, int64_t* c) {
 
 // grid_smb::BlockInvLinId (grid_smb.hpp:313-323)
 void block_coord(const Grid& g, int64_t b, int64_t* bc) {
+    if (g.zorder) {
+        inv_morton3(b, bc);
+        return;
+    }
     for (int d = 0; d < g.dim; ++d) {
         bc[d] = b % g.bsz[d];
         b /= g.bsz[d];
@@ -100,7 +134,10 @@ void block_coord(const Grid& g, int64_t b, int64_t* bc) {
 
 // grid_smb::BlockLinId (grid_smb.hpp:280-299).  Only the upper bound is
 // checked: a block coordinate of -1 produces a (possibly valid) wrapped id.
+// grid_zmb::BlockLinId checks nothing; its id of a negative coordinate lies
+// above every chunk's, i.e. absent (-1 here).
 int64_t block_lin_ref(const Grid& g, const int64_t* bc) {
+    if (g.zorder) return (bc[0] < 0 || bc[1] < 0 || bc[2] < 0) ? -1 : morton3(bc);
     int64_t lin = bc[g.dim - 1];
     if (lin >= g.bsz[g.dim - 1]) return -1;
     for (int d = g.dim - 2; d >= 0; --d) {
@@ -328,6 +365,8 @@ void relayout(Grid& g, const std::vector<int64_t>& merged, const std::vector<int
 
 // =================================================================== C API
 extern "C" {
+
+void sgo_set_zorder(void* h, int z) { ((Grid*)h)->zorder = z != 0; }
 
 void* sgo_create(int dim, int edge, const int64_t* size, int nprop, const int* ptypes) {
     Grid* g = new Grid();

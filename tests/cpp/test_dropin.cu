@@ -380,6 +380,42 @@ int main() {
               "pack_unpack");
     }
 
+    // ---------------------------------------------------------------- SparseGridGpu_z (Morton chunk ids)
+    {
+        Grid6 sg(sz);
+        SparseGridGpu_z<3, Agg6, 8> zg(sz);
+        sg.setBackgroundValue<0>(0.0f);
+        zg.setBackgroundValue<0>(0.0f);
+        sg.setGPUInsertBuffer(dim3(N / 8, N / 8, N / 8), dim3(1024, 1, 1));
+        zg.setGPUInsertBuffer(dim3(N / 8, N / 8, N / 8), dim3(1024, 1, 1));
+        insert_shape<0><<<dim3(N / 8, N / 8, N / 8), dim3(8, 8, 8)>>>(sg.toKernel());
+        insert_shape<0><<<dim3(N / 8, N / 8, N / 8), dim3(8, 8, 8)>>>(zg.toKernel());
+        sg.flush<smax_<0>>(ctx, FLUSH_ON_DEVICE);
+        zg.flush<smax_<0>>(ctx, FLUSH_ON_DEVICE);
+        sg.tagBoundaries<NNStar<3>>(ctx);
+        zg.tagBoundaries<NNStar<3>>(ctx);
+        sg.applyStencils<HeatStencil<3, 0, 1>>(sg.getBox(), STENCIL_MODE_INPLACE, 0.1f);
+        zg.applyStencils<HeatStencil<3, 0, 1>>(zg.getBox(), STENCIL_MODE_INPLACE, 0.1f);
+        cudaDeviceSynchronize();
+        sg.deviceToHost<0, 1>();
+        zg.deviceToHost<0, 1>();
+        bool eq = zg.countExistingElements() == npts && sg.nchunks() == zg.nchunks();
+        for (int z = 0; z < N && eq; ++z)
+            for (int y = 0; y < N; ++y)
+                for (int x = 0; x < N; ++x) {
+                    const grid_key_dx<3, int> k({x, y, z});
+                    const float a0 = sg.get<0>(k), b0 = zg.get<0>(k), a1 = sg.get<1>(k), b1 = zg.get<1>(k);
+                    eq = eq && std::memcmp(&a0, &b0, 4) == 0 && std::memcmp(&a1, &b1, 4) == 0 &&
+                         sg.getFlag(k) == zg.getFlag(k);
+                }
+        // the chunk ids differ: Morton codes, sorted
+        std::vector<int64_t> zk(zg.nchunks());
+        cudaMemcpy(zk.data(), zg.private_get_index_array(), zk.size() * 8, cudaMemcpyDeviceToHost);
+        bool morton = true;
+        for (size_t i = 1; i < zk.size(); ++i) morton = morton && zk[i] > zk[i - 1];
+        CHECK(eq && morton, "sparsegridgpu_z_insert_tag_heat");
+    }
+
     int st = sgb_check_device_errors(grid.handle(), nullptr);
     CHECK(st == SGB_OK, "device_error_word_clear");
     std::printf("%s: %d failure(s)\n", g_fail ? "FAILED" : "PASSED", g_fail);

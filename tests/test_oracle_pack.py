@@ -81,3 +81,26 @@ def test_conv3x3x3_noshared_all_ones():
     act = mask[:n] == 1
     assert act.sum() > 100000
     np.testing.assert_array_equal(data[1][:n][act], data[0][:n][act] * 27)
+
+
+@pytest.mark.parametrize("noshared", [False, True])
+def test_conv3x3x3_all_ones_morton(noshared):
+    """SparseGridGpu_tests.cu:1145-1180: the same all-ones known answers on
+    SparseGridGpu_z (chunk ids by Morton code)."""
+    g = O.OracleGrid(K.SIZE, edge=K.EDGE, ptypes=(O.T_F32, O.T_F32), zorder=True)
+    c, rel = K.sphere()
+    g.insert_flush(c, [K.sphere_values(rel)[0], np.zeros(len(c), np.float32)], [O.OP_MAX, O.OP_NONE])
+    keys, _, _ = g.export()
+    # the ids are the Morton codes of the chunk coordinates, in order
+    bc = np.unique(c // K.EDGE, axis=0)
+    morton = np.zeros(len(bc), np.int64)
+    for i in range(10):
+        for d in range(3):
+            morton |= ((bc[:, d] >> i) & 1) << (3 * i + d)
+    assert np.array_equal(keys, np.sort(morton))
+    g.tag_boundaries(O.NN_FULL)
+    (g.box27_noshared if noshared else g.box27)(0, 1, np.ones(27, np.float32))
+    keys, data, mask = g.export()
+    n = len(keys) * g.bs
+    act = mask[:n] == 1
+    np.testing.assert_array_equal(data[1][:n][act], data[0][:n][act] * 27)
