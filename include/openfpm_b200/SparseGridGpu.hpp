@@ -25,10 +25,12 @@
 #include <array>
 #include <cstdint>
 #include <cstring>
+#include <fstream>
 #include <stdexcept>
 #include <string>
 #include <tuple>
 #include <type_traits>
+#include <utility>
 #include <vector>
 
 #include "../sgb200.h"
@@ -638,6 +640,18 @@ class SparseGridGpu {
         return 0;
     }
 
+    // write / write_with_spacing_offset (SparseGridGpu.hpp:3844-3903): every point whose mask
+    // byte is not 0 at coord * spacing + offset * spacing, its properties and its mask byte, as a
+    // binary legacy VTK poly-data file of vertices (the reference passes the same data to
+    // openfpm_io's VTKWriter).  Reads the device data itself.
+    bool write(const std::string& output) {
+        const double one[3] = {1, 1, 1}, zero[3] = {0, 0, 0};
+        return write_impl(output, one, zero);
+    }
+    bool write_with_spacing_offset(const std::string& output, Point<dim, double> spacing, Point<dim, double> offset) {
+        return write_impl(output, spacing.x, offset.x);
+    }
+
     // remove(box): queue a section whose points removePoints deletes (SparseGridGpu.hpp:3528-3531)
     void remove(const Box<dim, int>& section_to_delete) { rem_sects_.push_back(section_to_delete); }
 
@@ -783,6 +797,56 @@ class SparseGridGpu {
    private:
     std::vector<Box<dim, int>> rem_sects_;
     std::vector<SparseGridGpu_iterator_sub<dim>> pack_subs_;
+
+    template <typename T>
+    static void put_be(std::ofstream& f, T v) {
+        unsigned char b[sizeof(T)];
+        std::memcpy(b, &v, sizeof(T));
+        for (int i = (int)sizeof(T) - 1; i >= 0; --i) f.put((char)b[i]);
+    }
+    template <size_t... I>
+    void write_props(std::ofstream& f, const std::vector<size_t>& sel, std::index_sequence<I...>) {
+        (write_prop<I>(f, sel), ...);
+    }
+    template <size_t p>
+    void write_prop(std::ofstream& f, const std::vector<size_t>& sel) {
+        using T = typename std::tuple_element<p, props>::type;
+        const char* vt = std::is_same<T, float>::value ? "float"
+                         : std::is_same<T, double>::value ? "double"
+                         : std::is_same<T, int>::value ? "int" : "unsigned_char";
+        f << "SCALARS attr" << p << " " << vt << "\nLOOKUP_TABLE default\n";
+        const T* d = reinterpret_cast<const T*>(h_data_[p].data());
+        for (size_t i : sel) put_be(f, d[i]);
+        f << "\n";
+    }
+    bool write_impl(const std::string& output, const double* sp, const double* of) {
+        deviceToHost<>();
+        int64_t bsz[3];
+        for (int d = 0; d < 3; ++d) bsz[d] = ((int64_t)size_[d] + blockEdgeSize - 1) / blockEdgeSize;
+        std::vector<size_t> sel;
+        for (size_t i = 0; i < h_keys_.size() * bs; ++i)
+            if (h_mask_[i] != 0) sel.push_back(i);
+        std::ofstream f(output, std::ios::binary);
+        if (!f) return false;
+        f << "# vtk DataFile Version 3.0\nsparse_grid\nBINARY\nDATASET POLYDATA\nPOINTS " << sel.size() << " float\n";
+        for (size_t i : sel) {
+            int64_t bc[3];
+            detail::block_coords(linearizer::zorder, bsz, h_keys_[i / bs], bc);
+            const int64_t o = (int64_t)(i % bs);
+            const int64_t c[3] = {bc[0] * blockEdgeSize + o % blockEdgeSize,
+                                  bc[1] * blockEdgeSize + (o / blockEdgeSize) % blockEdgeSize,
+                                  bc[2] * blockEdgeSize + o / (blockEdgeSize * blockEdgeSize)};
+            for (int d = 0; d < 3; ++d) put_be(f, (float)((double)c[d] * sp[d] + of[d] * sp[d]));
+        }
+        f << "\nVERTICES " << sel.size() << " " << 2 * sel.size() << "\n";
+        for (size_t k = 0; k < sel.size(); ++k) put_be(f, (int32_t)1), put_be(f, (int32_t)k);
+        f << "\nPOINT_DATA " << sel.size() << "\n";
+        write_props(f, sel, std::make_index_sequence<nprop>{});
+        f << "SCALARS mask unsigned_char\nLOOKUP_TABLE default\n";
+        for (size_t i : sel) f.put((char)h_mask_[i]);
+        f << "\n";
+        return (bool)f;
+    }
 
     sgb_links links(int up) const {
         sgb_links l{};

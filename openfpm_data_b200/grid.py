@@ -271,6 +271,58 @@ class SparseGridGpu:
                                            mask.ctypes.data_as(C.c_void_p), _stream(stream)), "sgb_download_map")
         return keys, data, mask
 
+    # ---------------------------------------------------------------- VTK output
+    _VTK_TYPES = {L.F32: ("float", ">f4"), L.I32: ("int", ">i4"), L.F64: ("double", ">f8"),
+                  L.U8: ("unsigned_char", "u1")}
+
+    def write(self, output: str, spacing=(1.0, 1.0, 1.0), offset=(0.0, 0.0, 0.0), names=None) -> bool:
+        """write / write_with_spacing_offset (src/SparseGridGpu/SparseGridGpu.hpp:3844-3903): every
+        point whose mask byte is not 0, at coord * spacing + offset * spacing (float32), with all
+        properties and the mask byte as point data, as a binary legacy VTK poly-data file of
+        vertices.  The reference hands the same points and values to openfpm_io's VTKWriter
+        (VECTOR_POINTS), which is not part of this project; the file layout here is the VTK
+        legacy format's."""
+        keys, data, mask = self.deviceToHost()
+        n = len(keys)
+        idx = np.nonzero(mask[: n * self.bs])[0]
+        coords = self.existing_coords_of(keys, idx)
+        sp = np.asarray(spacing, dtype=np.float64)
+        pos = (coords * sp + np.asarray(offset, dtype=np.float64) * sp).astype(">f4")
+        m = len(idx)
+        names = list(names) if names else [f"attr{p}" for p in range(len(self.ptypes))]
+        with open(output, "wb") as f:
+            f.write(b"# vtk DataFile Version 3.0\nsparse_grid\nBINARY\nDATASET POLYDATA\n")
+            f.write(f"POINTS {m} float\n".encode())
+            f.write(pos.tobytes())
+            f.write(f"\nVERTICES {m} {2 * m}\n".encode())
+            f.write(np.stack([np.ones(m, ">i4"), np.arange(m, dtype=">i4")], axis=1).tobytes())
+            f.write(f"\nPOINT_DATA {m}\n".encode())
+            for p, t in enumerate(self.ptypes):
+                vt, dt = self._VTK_TYPES[t]
+                f.write(f"SCALARS {names[p]} {vt}\nLOOKUP_TABLE default\n".encode())
+                f.write(data[p][idx].astype(dt).tobytes())
+                f.write(b"\n")
+            f.write(b"SCALARS mask unsigned_char\nLOOKUP_TABLE default\n")
+            f.write(mask[idx].astype("u1").tobytes())
+            f.write(b"\n")
+        return True
+
+    def existing_coords_of(self, keys: np.ndarray, idx: np.ndarray) -> np.ndarray:
+        """Coordinates [m, 3] of chunk-data positions idx (chunk position * bs + offset)."""
+        e = self.edge
+        key = keys[idx // self.bs]
+        off = idx % self.bs
+        if self.linearizer == "zmb":
+            u = key.astype(np.uint64)
+            bc = np.zeros((len(key), 3), dtype=np.int64)
+            for i in range(21):
+                for d in range(3):
+                    bc[:, d] |= ((u >> np.uint64(3 * i + d)) & np.uint64(1)).astype(np.int64) << i
+        else:
+            b = [(s + e - 1) // e for s in self.size]
+            bc = np.stack([key % b[0], (key // b[0]) % b[1], key // (b[0] * b[1])], axis=1)
+        return bc * e + np.stack([off % e, (off // e) % e, off // (e * e)], axis=1)
+
     # ---------------------------------------------------------------- remove / iterate
     def remove(self, box) -> None:
         """remove(box): queue an inclusive box ((lo), (hi)) of points to remove at removePoints()."""

@@ -13,6 +13,10 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <fstream>
+#include <iterator>
+#include <string>
+#include <unistd.h>
 #include <vector>
 
 #include "openfpm_b200/SparseGridGpu.hpp"
@@ -414,6 +418,17 @@ int main() {
         bool morton = true;
         for (size_t i = 1; i < zk.size(); ++i) morton = morton && zk[i] > zk[i - 1];
         CHECK(eq && morton, "sparsegridgpu_z_insert_tag_heat");
+        // write(): a VTK file of every point whose mask byte is not 0
+        const std::string vtk = "/tmp/sgb_dropin_" + std::to_string((long)getpid()) + ".vtk";
+        bool wrote = zg.write(vtk);
+        std::ifstream in(vtk, std::ios::binary);
+        std::string head;
+        std::getline(in, head);
+        std::string all((std::istreambuf_iterator<char>(in)), std::istreambuf_iterator<char>());
+        wrote = wrote && head == "# vtk DataFile Version 3.0" &&
+                all.find("POINTS " + std::to_string(npts) + " float") != std::string::npos;
+        std::remove(vtk.c_str());
+        CHECK(wrote, "write_vtk");
     }
 
     int st = sgb_check_device_errors(grid.handle(), nullptr);
