@@ -654,9 +654,7 @@ def run_ghost512(args, dist: Dist):
         ev[0].record()
         a.pack_boxes(boxes, props, buf)
         ev[1].record()
-        off = 0
-        for st in starts:
-            off = b.unpack(buf, props, st, off)
+        b.unpack_boxes(buf, props, starts)
         ev[2].record()
         b.removeAddUnpackFinalize(props)
         ev[3].record()
@@ -710,9 +708,7 @@ def run_ghost512(args, dist: Dist):
         a.pack_boxes(boxes, props, buf)
         h_send.copy_(buf, non_blocking=True)
         rbuf.copy_(h_send, non_blocking=True)
-        off = 0
-        for st in starts:
-            off = b.unpack(rbuf, props, st, off)
+        b.unpack_boxes(rbuf, props, starts)
         b.removeAddUnpackFinalize(props)
     f1.record()
     torch.cuda.synchronize()

@@ -260,6 +260,15 @@ int sgb_pack(sgb_grid* g, int64_t nboxes, const int64_t* boxes_host, int nprops,
 int sgb_unpack(sgb_grid* g, const void* buf_dev, int64_t nbytes, int nprops, const int* props,
                const int64_t* start_host, int64_t* consumed, sgb_stream s);
 
+/* sgb_unpack of nboxes consecutive packed boxes in one call (no reference
+ * counterpart: the reference unpacks box by box, reading each header on the
+ * host).  The headers are walked on the device, so the call synchronises
+ * the stream once instead of twice per box.  starts_host: nboxes x 3
+ * destination corners, or NULL (points at their packed coordinates).
+ * *consumed = bytes of the nboxes boxes. */
+int sgb_unpack_boxes(sgb_grid* g, const void* buf_dev, int64_t nbytes, int nprops, const int* props, int64_t nboxes,
+                     const int64_t* starts_host, int64_t* consumed, sgb_stream s);
+
 /* The existing-point list of tagBoundaries(..., CALCULATE_EXISTING_POINTS)
  * (SparseGridGpu.hpp:2354-2387): every existing point as uint32 chunk
  * position * chunk size + offset, in (chunk position, offset) order (the

@@ -49,6 +49,7 @@ SIGNATURES = {
     "sgb_pack_request": (_i32, [_vp, _i64, _vp, _i32, _vp, _vp, _vp]),
     "sgb_pack": (_i32, [_vp, _i64, _vp, _i32, _vp, _vp, _i64, _vp, _vp]),
     "sgb_unpack": (_i32, [_vp, _vp, _i64, _i32, _vp, _vp, _vp, _vp]),
+    "sgb_unpack_boxes": (_i32, [_vp, _vp, _i64, _i32, _vp, _i64, _vp, _vp, _vp]),
     "sgb_flush": (_i32, [_vp, _vp, _vp]),
     "sgb_find_neighbours": (_i32, [_vp, _i32, _vp]),
     "sgb_neighbour_table": (_i32, [_vp, _i32, _vp, _vp]),

@@ -26,7 +26,7 @@
 
 namespace sgb {
 
-static inline int64_t pad8(int64_t b) { return (b + 7) & ~(int64_t)7; }
+__host__ __device__ inline int64_t pad8(int64_t b) { return (b + 7) & ~(int64_t)7; }
 
 struct PackLayout {
     int64_t n_cnk, n_pnt;
@@ -34,7 +34,7 @@ struct PackLayout {
     int64_t prop_off[kMaxProps];
 };
 
-static PackLayout layout_of(int64_t n_cnk, int64_t n_pnt, int np, const int* es) {
+__host__ __device__ inline PackLayout layout_of(int64_t n_cnk, int64_t n_pnt, int np, const int* es) {
     PackLayout L{};
     L.n_cnk = n_cnk;
     L.n_pnt = n_pnt;
@@ -255,6 +255,116 @@ __global__ void k_unpack_stage(const unsigned char* __restrict__ buf, PackLayout
     }
 }
 
+// One packed box of a buffer, as found by k_unpack_walk.
+struct UnpackBox {
+    int64_t pos;       // byte offset of the box in the buffer
+    int64_t n_cnk, n_pnt;
+    int64_t start[3];  // packed box lower corner
+    int64_t size[3];   // packing grid size
+    int64_t pnt0;      // points of the boxes before this one
+    int64_t shift[3];  // destination - packed coordinates
+    int32_t bad;       // 1: the header does not fit the buffer
+};
+
+struct ElemSizes {
+    int es[kMaxProps];
+    int np;
+};
+
+// Walk the headers of nb packed boxes (one thread: each box's place follows
+// from the sizes of the boxes before it).
+__global__ void k_unpack_walk(const unsigned char* __restrict__ buf, int64_t nbytes, int nb, ElemSizes es,
+                              UnpackBox* out) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    int64_t pos = 0, pts = 0;
+    for (int k = 0; k < nb; ++k) {
+        UnpackBox B{};
+        B.pos = pos;
+        B.pnt0 = pts;
+        B.bad = 1;
+        if (nbytes - pos >= 40) {
+            const uint64_t nc = *reinterpret_cast<const uint64_t*>(buf + pos);
+            if (nc <= (uint64_t)(nbytes - pos - 36) / 12) {
+                const int32_t* h = reinterpret_cast<const int32_t*>(buf + pos + 8);
+                const uint32_t np_ = *reinterpret_cast<const uint32_t*>(buf + pos + 32 + 12 * (int64_t)nc);
+                const PackLayout L = layout_of((int64_t)nc, np_, es.np, es.es);
+                bool ok = L.bytes <= nbytes - pos && !(nc == 0 && np_ != 0);
+                for (int d = 0; d < 3; ++d) ok = ok && h[3 + d] >= 1;
+                if (ok) {
+                    B.n_cnk = (int64_t)nc;
+                    B.n_pnt = np_;
+                    for (int d = 0; d < 3; ++d) {
+                        B.start[d] = h[d];
+                        B.size[d] = h[3 + d];
+                    }
+                    B.bad = 0;
+                    pos += L.bytes;
+                    pts += np_;
+                }
+            }
+        }
+        out[k] = B;
+        if (B.bad) {
+            for (int j = k + 1; j < nb; ++j) out[j].bad = 1;
+            return;
+        }
+    }
+}
+
+// Staged inserts of every packed point of the boxes: thread j finds its box
+// by the point offsets, then proceeds as k_unpack_stage.
+__global__ void k_unpack_stage_all(const unsigned char* __restrict__ buf, const UnpackBox* __restrict__ boxes, int nb,
+                                   int64_t total, ElemSizes es, Geometry dst_geo, int64_t* out_lin, UnpackDst dst,
+                                   unsigned* err) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= total) return;
+    int lo = 0, hi = nb;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (boxes[mid].pnt0 <= t) lo = mid;
+        else hi = mid;
+    }
+    const UnpackBox& B = boxes[lo];
+    const PackLayout L = layout_of(B.n_cnk, B.n_pnt, es.np, es.es);
+    const int64_t j = t - B.pnt0;
+    const unsigned char* b = buf + B.pos;
+    const int64_t* ids = reinterpret_cast<const int64_t*>(b + L.off_ids);
+    const uint32_t* scan = reinterpret_cast<const uint32_t*>(b + L.off_scan);
+    const int16_t* offs = reinterpret_cast<const int16_t*>(b + L.off_offs);
+    int64_t clo = 0, chi = L.n_cnk;
+    while (chi - clo > 1) {
+        const int64_t mid = (clo + chi) >> 1;
+        if (scan[mid] <= (uint32_t)j) clo = mid;
+        else chi = mid;
+    }
+    Geometry src = dst_geo;
+    for (int d = 0; d < 3; ++d) {
+        src.size[d] = B.size[d];
+        src.bsz[d] = (B.size[d] + src.edge - 1) / src.edge;
+    }
+    int64_t o[3];
+    origin_of(src, ids[clo], o);
+    const int e = src.edge, pt = offs[j];
+    const int64_t c[3] = {o[0] + pt % e + B.shift[0], o[1] + (pt / e) % e + B.shift[1],
+                          o[2] + pt / (e * e) + B.shift[2]};
+    bool ok = pt >= 0 && pt < src.bs;
+    for (int d = 0; d < 3; ++d) ok = ok && c[d] >= 0 && c[d] < dst_geo.size[d];
+    int64_t lin = -1;
+    if (ok) {
+        int64_t kb, kl;
+        point_key(dst_geo, c, &kb, &kl);
+        lin = kb * dst_geo.bs + kl;
+    } else {
+        atomicOr(err, kErrOutOfDomain);
+    }
+    out_lin[t] = lin;
+    for (int p = 0; p < es.np; ++p) {
+        const int sz = es.es[p];
+        const unsigned char* sp = b + L.off_data + L.prop_off[p] + j * sz;
+        for (int q = 0; q < sz; ++q) dst.p[p][t * sz + q] = sp[q];
+    }
+}
+
 static unsigned wgrid(const sgb_grid* g, int64_t n) {
     return (unsigned)std::max<int64_t>(1, std::min<int64_t>((int64_t)g->num_sms * 8, (n + 7) / 8));
 }
@@ -466,5 +576,68 @@ extern "C" int sgb_unpack(sgb_grid* g, const void* buf_dev, int64_t nbytes, int 
         g->npend += np_;
     }
     *consumed = L.bytes;
+    return SGB_OK;
+}
+
+extern "C" int sgb_unpack_boxes(sgb_grid* g, const void* buf_dev, int64_t nbytes, int nprops, const int* props,
+                                int64_t nboxes, const int64_t* starts_host, int64_t* consumed, sgb_stream stream) {
+    if (!g || !consumed || nbytes < 0 || nboxes < 0 || (nbytes > 0 && !buf_dev)) return SGB_EINVAL;
+    *consumed = 0;
+    if (g->geo.dim != 3) return SGB_ENOTSUP;
+    if ((uintptr_t)buf_dev % 8 != 0) {
+        set_error("the pack buffer must be 8-byte aligned");
+        return SGB_EINVAL;
+    }
+    ElemSizes es{};
+    SGB_TRY(check_props(g, nprops, props, es.es));
+    es.np = nprops;
+    for (int k = 0; k < nprops; ++k)
+        for (int j = 0; j < k; ++j)
+            if (props[j] == props[k]) return SGB_EINVAL;
+    if (nboxes == 0) return SGB_OK;
+    if (nboxes > (int64_t(1) << 20)) return SGB_EINVAL;
+    cudaStream_t s = (cudaStream_t)stream;
+    const size_t tb = (size_t)nboxes * sizeof(UnpackBox);
+    SGB_TRY(g->scratch[0].ensure(tb));
+    SGB_TRY(g->hscratch.ensure(tb));
+    UnpackBox* dboxes = g->scratch[0].as<UnpackBox>();
+    k_unpack_walk<<<1, 1, 0, s>>>((const unsigned char*)buf_dev, nbytes, (int)nboxes, es, dboxes);
+    SGB_CUDA(cudaGetLastError());
+    SGB_CUDA(cudaMemcpyAsync(g->hscratch.p, dboxes, tb, cudaMemcpyDeviceToHost, s));
+    SGB_CUDA(cudaStreamSynchronize(s));
+    std::vector<UnpackBox> hb((size_t)nboxes);
+    std::memcpy(hb.data(), g->hscratch.p, tb);
+    for (const UnpackBox& B : hb)
+        if (B.bad) {
+            set_error("corrupt or truncated pack buffer, or one packed with other properties");
+            return SGB_EINVAL;
+        }
+    const int64_t total = hb.back().pnt0 + hb.back().n_pnt;
+    for (int64_t k = 0; k < nboxes; ++k)
+        for (int d = 0; d < 3; ++d) hb[k].shift[d] = starts_host ? starts_host[3 * k + d] - hb[k].start[d] : 0;
+    if (total > 0) {
+        std::memcpy(g->hscratch.p, hb.data(), tb);
+        SGB_CUDA(cudaMemcpyAsync(dboxes, g->hscratch.p, tb, cudaMemcpyHostToDevice, s));
+        SGB_TRY(g->pend_lin.reserve((size_t)(g->npend + total) * 8));
+        for (int p = 0; p < g->nprop; ++p)
+            SGB_TRY(g->pend_val[p].reserve((size_t)(g->npend + total) * elem_size(g->ptype[p])));
+        bool packed[kMaxProps] = {};
+        for (int k = 0; k < nprops; ++k) packed[props[k]] = true;
+        for (int p = 0; p < g->nprop; ++p) {
+            const int pe = elem_size(g->ptype[p]);
+            if (packed[p]) g->pend_has[p] = true;
+            else SGB_TRY(fill(g->pend_val[p].as<unsigned char>() + (size_t)g->npend * pe, total, pe, bck_pattern(g, p), s));
+        }
+        UnpackDst dst{};
+        for (int k = 0; k < nprops; ++k) dst.p[k] = g->pend_val[props[k]].as<unsigned char>() + (size_t)g->npend * es.es[k];
+        k_unpack_stage_all<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(
+            (const unsigned char*)buf_dev, dboxes, (int)nboxes, total, es, g->geo, g->pend_lin.as<int64_t>() + g->npend,
+            dst, g->err.as<unsigned>());
+        SGB_CUDA(cudaGetLastError());
+        SGB_CUDA(cudaStreamSynchronize(s));  // the host staging of the box table is reused by the next call
+        g->npend += total;
+    }
+    const PackLayout Ll = layout_of(hb.back().n_cnk, hb.back().n_pnt, nprops, es.es);
+    *consumed = hb.back().pos + Ll.bytes;
     return SGB_OK;
 }

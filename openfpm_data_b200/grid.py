@@ -448,6 +448,25 @@ class SparseGridGpu:
                                      _i32arr(list(props)), st, C.byref(used), _stream(stream)), "sgb_unpack")
         return offset + used.value
 
+    def unpack_boxes(self, buf: torch.Tensor, props: Sequence[int], starts=None, nboxes: Optional[int] = None,
+                     offset: int = 0, stream=None) -> int:
+        """unpack of nboxes consecutive packed boxes (len(starts) when starts are given) in one call;
+        returns the offset after them."""
+        if nboxes is None:
+            if starts is None:
+                raise ValueError("give starts or nboxes")
+            nboxes = len(starts)
+        st = None
+        if starts is not None:
+            st = np.ascontiguousarray(np.asarray(starts, dtype=np.int64).reshape(-1, 3))
+            assert len(st) == nboxes
+        used = C.c_int64(0)
+        L.check(self._lib.sgb_unpack_boxes(self._h, buf.data_ptr() + offset, buf.numel() - offset, len(props),
+                                           _i32arr(list(props)), nboxes,
+                                           None if st is None else st.ctypes.data_as(C.c_void_p), C.byref(used),
+                                           _stream(stream)), "sgb_unpack_boxes")
+        return offset + used.value
+
     def removeAddUnpackReset(self) -> None:
         self._rem = []
 

@@ -196,3 +196,32 @@ def test_pack_errors(sgb):
     with pytest.raises(sgb.SgbError):
         g.removeAddUnpackFinalize([0])
     g.check_device_errors()
+
+
+@pytest.mark.parametrize("with_starts", [True, False])
+def test_unpack_boxes_equals_box_by_box(sgb, with_starts):
+    src, osrc = _random_pair(sgb, (96, 96, 96), 60000, 51)
+    boxes = RBOXES  # includes empty and inverted boxes
+    props = [0, 3, 1]
+    buf = src.pack_boxes(K.box_rows(boxes), props)
+    starts = [tuple(np.add(lo, 7)) for lo, _ in boxes] if with_starts else None
+    a, _ = _random_pair(sgb, (128, 128, 128), 20000, 52)
+    b, _ = _random_pair(sgb, (128, 128, 128), 20000, 52)
+    off = 0
+    for k in range(len(boxes)):
+        off = a.unpack(buf, props, None if starts is None else starts[k], off)
+    assert b.unpack_boxes(buf, props, starts, nboxes=len(boxes)) == off == buf.numel()
+    a.removeAddUnpackFinalize(props)
+    b.removeAddUnpackFinalize(props)
+    ka, da, ma = a.deviceToHost()
+    kb, db, mb = b.deviceToHost()
+    assert np.array_equal(ka, kb) and np.array_equal(ma, mb)
+    for p in range(4):
+        assert np.array_equal(da[p].view(np.uint8), db[p].view(np.uint8))
+    # a truncated buffer is refused before anything is staged
+    n_before = b.countExistingElements()
+    with pytest.raises(sgb.SgbError):
+        b.unpack_boxes(buf[: buf.numel() - 8], props, starts, nboxes=len(boxes))
+    b.removeAddUnpackFinalize(props)
+    assert b.countExistingElements() == n_before
+    b.check_device_errors()
