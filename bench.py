@@ -44,7 +44,7 @@ UNIT = "Gpts/s"
 ALG_BYTES_PER_PT = 17
 # the library's default launch configuration of the pipelined 8^3 kernel (automatic ring depth)
 DEFAULT_CTAS_PER_SM, DEFAULT_STAGES = "auto", "auto"
-WORKLOADS = ("gs512", "heat128", "insert1024", "batched256", "served", "ghost512")
+WORKLOADS = ("gs512", "heat128", "insert1024", "batched256", "served", "ghost512", "conv1000")
 
 
 def parse():
@@ -739,6 +739,98 @@ def run_ghost512(args, dist: Dist):
                  roofline=roof, cpu_baseline=cpu, e2e=e2e, gpu_launches=None, clocks=clk)
 
 
+def _shell_1000():
+    """The grid of the reference's Conv3x3x3 benchmarks (SparseGridGpu_util_test.cuh:488-680):
+    insertSphere3D_radius on 32^3 chunks of 8 from (256, 256, 256), radii 128 / 56 -- the
+    points with 56 < sqrtf(|p - (384, 384, 384)|^2) < 128, value x + y + z relative to the
+    centre -- in a 1000^3 domain."""
+    r = np.arange(256, 512, dtype=np.int64)
+    out_c, out_v = [], []
+    for z in r:
+        y, x = np.meshgrid(r, r, indexing="ij")
+        rel = np.stack([x.ravel() - 384, y.ravel() - 384, np.full(x.size, z - 384)], axis=1)
+        rad = np.sqrt((rel * rel).sum(axis=1).astype(np.float32))
+        keep = (rad < np.float32(128)) & (rad > np.float32(56))
+        out_c.append(rel[keep] + 384)
+        out_v.append(rel[keep].sum(axis=1).astype(np.float32))
+    return np.concatenate(out_c), np.concatenate(out_v)
+
+
+def run_conv1000(args, dist: Dist):
+    """Conv3x3x3 on the reference's benchmark grid, in its four variants: the
+    one-chunk-per-CTA tile kernel (STENCIL_MODE_INPLACE) and the point-list kernel
+    (STENCIL_MODE_INPLACE_NO_SHARED), on x-fastest and on Morton chunk ids.  GElem/s =
+    (existing - boundary points) x applications / time, the reference's measure."""
+    import torch
+
+    import openfpm_data_b200 as sgb
+    torch.cuda.set_device(dist.local)
+    nsteps = args.steps if args.steps <= 500 else 100
+    nwarm = max(3, min(args.warmup, 10))
+    coords, vals = _shell_1000()
+    c_dev = torch.from_numpy(coords.astype(np.int32)).cuda()
+    v_dev = torch.from_numpy(vals).cuda()
+    coeff = [1.0] * 27
+    flush = torch.empty(256 * 2 ** 20 // 4, dtype=torch.float32, device="cuda")
+    res, clk, nelem, nchunks = {}, None, 0, 0
+    peak, pk = _peak_hbm()
+    for lin in ("smb", "zmb"):
+        g = sgb.SparseGridGpu((1000, 1000, 1000), ["f32", "f32"], edge=8, device=dist.local, linearizer=lin)
+        g.insert(c_dev, [v_dev, None])
+        g.flush(["smax_", None])
+        g.findNeighbours(sgb.NN_FULL)
+        g.tagBoundaries(sgb.NN_FULL, calculate_existing_points=True)
+        nelem = g.countExistingElements() - g.countBoundaryElements()
+        nchunks = g.nchunks
+        for mode, kind in (("shared", sgb.BOX27), ("noshared", sgb.BOX27_NS)):
+            for _ in range(nwarm):
+                g.applyStencils(kind, [0], [1], coeff)
+            torch.cuda.synchronize()
+            sampler = ClockSampler(dist.local) if (lin, mode) == ("smb", "shared") else None
+            dist.barrier()
+            evs = []
+            for k in range(nsteps):
+                flush.fill_(float(k))  # the grid (about 100 MB) would stay in L2 between applications
+                e0, e1 = _events()
+                e0.record()
+                g.applyStencils(kind, [0], [1], coeff)
+                e1.record()
+                evs.append((e0, e1))
+            torch.cuda.synchronize()
+            dist.barrier()
+            if sampler:
+                clk = sampler.stop()
+            t = dist.max(sum(a.elapsed_time(b) for a, b in evs) / 1e3)
+            res[f"{lin}_{mode}"] = {"gelem_s": round(dist.world * nelem * nsteps / t / 1e9, 3),
+                                    "us_per_application": round(t / nsteps * 1e6, 2)}
+        g.check_device_errors()
+        del g
+    head = res["smb_shared"]
+    t_one = head["us_per_application"] / 1e6
+    ach = 9 * nelem / t_one / 1e9
+    roof = {"bound": "hbm", "kernel": "k_stencil_tile<BOX27,8> (Conv3x3x3, one CTA per chunk)",
+            "achieved": round(ach, 1), "peak": peak, "unit": "GB/s", "frac": round(ach / peak, 4), "traffic": None,
+            "peak_kind": pk, "alg_bytes_per_launch": 9 * nelem}
+    cpu = None
+    if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
+        from oracle import oracle as O
+        O.build()
+        o = O.OracleGrid((1000, 1000, 1000), edge=8, ptypes=[O.T_F32, O.T_F32])
+        o.insert_flush(coords, [vals, np.zeros(len(vals), np.float32)], [O.OP_MAX, O.OP_NONE])
+        o.tag_boundaries(O.NN_FULL)
+        t0 = time.perf_counter()
+        o.box27(0, 1, np.ones(27, np.float32))
+        dtc = time.perf_counter() - t0
+        cpu = {"value": round(nelem / dtc / 1e9, 5), "unit": "GElem/s", "cores": 1, "kind": "port",
+               "sample": f"one Conv3x3x3 application on the full grid by the oracle, 1 thread, {dtc:.1f} s"}
+    return _line("Conv3x3x3 GElem/s (1000^3 domain, 56 < r < 128 shell, 8^3 chunks)", head["gelem_s"], "GElem/s",
+                 dist, args, nsteps, head["us_per_application"] / 1e6 * nsteps,
+                 {"workload": "conv3x3x3_1000^3_shell_r56_r128_chunk8", "elements": nelem, "chunks": nchunks,
+                  "variants": res, "l2": "256 MiB L2-flushing write before every timed application "
+                                         "(the grid fits in L2); events around each application"},
+                 roofline=roof, cpu_baseline=cpu, e2e=None, gpu_launches=None, clocks=clk)
+
+
 def run_reference(args, dist: Dist):
     from openfpm_data_b200 import workloads as W
     if dist.rank != 0:
@@ -765,7 +857,8 @@ def main():
             line = run_reference(args, dist)
         else:
             runners = {"gs512": run_ours, "heat128": run_heat128, "insert1024": run_insert1024,
-                       "batched256": run_batched256, "served": run_served, "ghost512": run_ghost512}
+                       "batched256": run_batched256, "served": run_served, "ghost512": run_ghost512,
+                       "conv1000": run_conv1000}
             line = runners[args.workload](args, dist)
         if line is not None and dist.rank == 0:
             print(json.dumps(line), flush=True)

@@ -126,6 +126,119 @@ __global__ void __launch_bounds__(256) k_stencil_tile(FieldSet fs, const uint8_t
     }
 }
 
+// ------------------------------------------------------------------ Conv3x3x3 on 8^3 chunks
+// One chunk per 64-thread CTA (grid-stride).  The 10^3 tile is built from
+// the chunk (16-byte loads of its rows) and its 26 NNFull neighbours (the six
+// faces, then the edges and corners); an absent neighbour gives the
+// background.  Thread t owns the column (x, y) = (t % 8, t / 8) and marches
+// z, holding the 3 x 3 x 3 window in registers: per point 9 shared loads
+// and the 27 FMAs in Conv3x3x3's order (x offset outermost, z innermost).
+// Results equal the tile kernel's bit for bit (the background invariant
+// makes reading a stored non-existing point the same as substituting the
+// background).
+__global__ void __launch_bounds__(64) k_box27_e8(const float* __restrict__ src, float* __restrict__ dst,
+                                                 const uint8_t* __restrict__ mask, const int32_t* __restrict__ nn,
+                                                 const int64_t* __restrict__ keys, int64_t n, Geometry geo,
+                                                 StencilParams prm, float bck) {
+    constexpr int T = 10;
+    __shared__ __align__(16) float tile[T * T * T];
+    __shared__ int32_t nb[27];
+    const int t = threadIdx.x;
+    const int cx = t & 7, cy = t >> 3;
+    for (int64_t c = blockIdx.x; c < n; c += gridDim.x) {
+        if (t < 27) nb[t] = t == 13 ? (int32_t)c : nn[c * 27 + t];
+        // interior: row (y, z) = (t % 8, t / 8) of the chunk, two 16-byte loads
+        {
+            const float4* row = reinterpret_cast<const float4*>(src + c * 512 + t * 8);
+            const float4 a = __ldg(row), b = __ldg(row + 1);
+            float* d = &tile[((t >> 3) + 1) * 100 + ((t & 7) + 1) * 10 + 1];
+            d[0] = a.x; d[1] = a.y; d[2] = a.z; d[3] = a.w;
+            d[4] = b.x; d[5] = b.y; d[6] = b.z; d[7] = b.w;
+        }
+        __syncthreads();
+        // faces: thread t takes the cell (u, v) = (t % 8, t / 8) of each of the six faces
+        {
+            const int u = t & 7, v = t >> 3;
+            // slot = px + 3 py + 9 pz; (tile cell, neighbour point)
+            const int32_t sxm = nb[12], sxp = nb[14], sym = nb[10], syp = nb[16], szm = nb[4], szp = nb[22];
+            tile[(v + 1) * 100 + (u + 1) * 10 + 0] = sxm >= 0 ? src[(int64_t)sxm * 512 + v * 64 + u * 8 + 7] : bck;
+            tile[(v + 1) * 100 + (u + 1) * 10 + 9] = sxp >= 0 ? src[(int64_t)sxp * 512 + v * 64 + u * 8 + 0] : bck;
+            tile[(v + 1) * 100 + 0 * 10 + (u + 1)] = sym >= 0 ? src[(int64_t)sym * 512 + v * 64 + 7 * 8 + u] : bck;
+            tile[(v + 1) * 100 + 9 * 10 + (u + 1)] = syp >= 0 ? src[(int64_t)syp * 512 + v * 64 + 0 * 8 + u] : bck;
+            tile[0 * 100 + (v + 1) * 10 + (u + 1)] = szm >= 0 ? src[(int64_t)szm * 512 + 7 * 64 + v * 8 + u] : bck;
+            tile[9 * 100 + (v + 1) * 10 + (u + 1)] = szp >= 0 ? src[(int64_t)szp * 512 + 0 * 64 + v * 8 + u] : bck;
+        }
+        // edges (12 x 8 cells) and corners (8): cells 0..103 of the remaining halo
+        for (int e = t; e < 104; e += 64) {
+            int tx, ty, tz;
+            if (e < 96) {
+                const int k = e >> 3, w = (e & 7) + 1;  // edge k, position w along it
+                const int a = (k & 1) ? 9 : 0, b = (k & 2) ? 9 : 0;
+                if (k < 4) { tx = w; ty = a; tz = b; }          // edges along x
+                else if (k < 8) { tx = a; ty = w; tz = b; }     // along y
+                else { tx = a; ty = b; tz = w; }                // along z
+            } else {
+                const int k = e - 96;
+                tx = (k & 1) ? 9 : 0;
+                ty = (k & 2) ? 9 : 0;
+                tz = (k & 4) ? 9 : 0;
+            }
+            const int px = tx == 0 ? 0 : (tx == 9 ? 2 : 1), py = ty == 0 ? 0 : (ty == 9 ? 2 : 1),
+                      pz = tz == 0 ? 0 : (tz == 9 ? 2 : 1);
+            const int32_t sc = nb[px + 3 * py + 9 * pz];
+            const int lx = (tx + 7) & 7, ly = (ty + 7) & 7, lz = (tz + 7) & 7;
+            tile[tz * 100 + ty * 10 + tx] = sc >= 0 ? src[(int64_t)sc * 512 + lz * 64 + ly * 8 + lx] : bck;
+        }
+        __syncthreads();
+        int64_t ox = 0, oy = 0, oz = 0;
+        if (prm.has_box) {
+            int64_t o[3];
+            chunk_origin(geo, keys[c], o);
+            ox = o[0];
+            oy = o[1];
+            oz = o[2];
+        }
+        // window w[a][b][d] = tile[z + d][y + b][x + a] (a, b, d in 0..2, tile coordinates)
+        float w[3][3][3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int b = 0; b < 3; ++b) {
+                w[a][b][0] = tile[0 * 100 + (cy + b) * 10 + (cx + a)];
+                w[a][b][1] = tile[1 * 100 + (cy + b) * 10 + (cx + a)];
+            }
+#pragma unroll
+        for (int z = 0; z < 8; ++z) {
+#pragma unroll
+            for (int a = 0; a < 3; ++a)
+#pragma unroll
+                for (int b = 0; b < 3; ++b) w[a][b][2] = tile[(z + 2) * 100 + (cy + b) * 10 + (cx + a)];
+            const int64_t gi = c * 512 + z * 64 + cy * 8 + cx;
+            const uint8_t m = mask[gi];
+            bool act = (m & 3) == 1;
+            if (prm.has_box) act = act && in_box(prm, ox + cx, oy + cy, oz + z);
+            if (act) {
+                float tot = 0.0f;
+#pragma unroll
+                for (int a = 0; a < 3; ++a)
+#pragma unroll
+                    for (int b = 0; b < 3; ++b)
+#pragma unroll
+                        for (int d = 0; d < 3; ++d) tot = __fmaf_rn(w[a][b][d], prm.coeff[a * 9 + b * 3 + d], tot);
+                dst[gi] = tot;
+            }
+#pragma unroll
+            for (int a = 0; a < 3; ++a)
+#pragma unroll
+                for (int b = 0; b < 3; ++b) {
+                    w[a][b][0] = w[a][b][1];
+                    w[a][b][1] = w[a][b][2];
+                }
+        }
+        __syncthreads();
+    }
+}
+
 int make_params(sgb_grid* g, int kind, const int* src, const int* dst, const float* params, int nparams,
                 const int64_t* box, StencilParams& prm) {
     std::memset(&prm, 0, sizeof(prm));
@@ -197,6 +310,13 @@ int launch_fields(const LaunchDesc& L, cudaStream_t s) {
     // the pipelined kernel takes the x halo from the neighbouring index positions, which hold the
     // x neighbours only under the x-fastest chunk ids
     if (L.kind != SGB_BOX27 && L.edge == 8 && !L.use_tile && !L.geo.zorder) return launch_e8(L, s);
+    if (L.kind == SGB_BOX27 && L.edge == 8 && !L.use_tile && !L.grids) {
+        const unsigned nb = (unsigned)std::max<int64_t>(1, std::min<int64_t>(L.n, (int64_t)L.num_sms * 32));
+        k_box27_e8<<<nb, 64, 0, s>>>(L.fs.in[0][0], L.fs.out[0][0], L.mask, L.nn, L.keys, L.n, L.geo, L.prm,
+                                      L.g0.bck[0][0]);
+        SGB_CUDA(cudaGetLastError());
+        return SGB_OK;
+    }
     const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>(L.n, (int64_t)L.num_sms * 8));
 #define SGB_TILE(K, E) \
     k_stencil_tile<K, E><<<blocks, 256, 0, s>>>(L.fs, L.mask, L.nn, L.keys, L.gid, L.grids, L.g0, L.n, L.geo, L.prm, L.t)
