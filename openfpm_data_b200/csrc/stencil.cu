@@ -127,69 +127,99 @@ __global__ void __launch_bounds__(256) k_stencil_tile(FieldSet fs, const uint8_t
 }
 
 // ------------------------------------------------------------------ Conv3x3x3 on 8^3 chunks
-// One chunk per 64-thread CTA (grid-stride).  The 10^3 tile is built from
-// the chunk (16-byte loads of its rows) and its 26 NNFull neighbours (the six
-// faces, then the edges and corners); an absent neighbour gives the
-// background.  Thread t owns the column (x, y) = (t % 8, t / 8) and marches
-// z, holding the 3 x 3 x 3 window in registers: per point 9 shared loads
-// and the 27 FMAs in Conv3x3x3's order (x offset outermost, z innermost).
+// One chunk at a time per 64-thread CTA (grid-stride), software-pipelined:
+// while chunk i is computed from one 10^3 shared tile, the tile of chunk
+// i + 1 is being filled in the other by cp.async copies (16-byte copies of
+// the chunk's rows, 4-byte copies of the six faces, twelve edges and eight
+// corners from the 26 NNFull neighbours; an absent neighbour's cells get the
+// background with plain stores) and the chunk's mask bytes alongside.  Tile
+// cell (x, y, z), x, y, z in 0..9, sits at z * 240 + y * 24 + x + 3: rows of
+// 24 floats put the chunk's part of every row on a 16-byte boundary, and the
+// four rows a warp reads at once fall into disjoint banks.  The neighbour rows are read two chunks
+// ahead.  Thread t owns the column (x, y) = (t % 8, t / 8) and marches z
+// holding the 3 x 3 x 3 window in registers: per point 9 shared loads and
+// the 27 FMAs in Conv3x3x3's order (x offset outermost, z innermost).
 // Results equal the tile kernel's bit for bit (the background invariant
-// makes reading a stored non-existing point the same as substituting the
+// makes a stored non-existing point read the same as the substituted
 // background).
-__global__ void __launch_bounds__(64) k_box27_e8(const float* __restrict__ src, float* __restrict__ dst,
+constexpr int kB27Plane = 240, kB27Row = 24, kB27Tile = 10 * kB27Plane;
+
+__device__ __forceinline__ void box27_fill(float* tile, uint8_t* mt, const int32_t* nb, const float* __restrict__ src,
+                                           const uint8_t* __restrict__ mask, int64_t c, float bck, int t) {
+    if (t < 32) cp_async16(mt + t * 16, mask + c * 512 + t * 16);
+    // interior: row (y, z) = (t % 8, t / 8), two 16-byte copies
+    {
+        const float* row = src + c * 512 + t * 8;
+        float* d = &tile[((t >> 3) + 1) * kB27Plane + ((t & 7) + 1) * kB27Row + 4];
+        cp_async16(d, row);
+        cp_async16(d + 4, row + 4);
+    }
+    const int u = t & 7, v = t >> 3;
+    auto cell = [&](int ti, int32_t sc, int64_t off) {
+        if (sc >= 0) cp_async4(&tile[ti], src + (int64_t)sc * 512 + off);
+        else tile[ti] = bck;
+    };
+    // faces: cell (u, v) of each; slot = px + 3 py + 9 pz
+    auto at = [](int x, int y, int z) { return z * kB27Plane + y * kB27Row + x + 3; };
+    cell(at(0, u + 1, v + 1), nb[12], v * 64 + u * 8 + 7);
+    cell(at(9, u + 1, v + 1), nb[14], v * 64 + u * 8 + 0);
+    cell(at(u + 1, 0, v + 1), nb[10], v * 64 + 7 * 8 + u);
+    cell(at(u + 1, 9, v + 1), nb[16], v * 64 + 0 * 8 + u);
+    cell(at(u + 1, v + 1, 0), nb[4], 7 * 64 + v * 8 + u);
+    cell(at(u + 1, v + 1, 9), nb[22], 0 * 64 + v * 8 + u);
+    // edges (12 x 8 cells) and corners (8)
+    for (int e = t; e < 104; e += 64) {
+        int tx, ty, tz;
+        if (e < 96) {
+            const int k = e >> 3, w = (e & 7) + 1;  // edge k, position w along it
+            const int a = (k & 1) ? 9 : 0, b = (k & 2) ? 9 : 0;
+            if (k < 4) { tx = w; ty = a; tz = b; }          // edges along x
+            else if (k < 8) { tx = a; ty = w; tz = b; }     // along y
+            else { tx = a; ty = b; tz = w; }                // along z
+        } else {
+            const int k = e - 96;
+            tx = (k & 1) ? 9 : 0;
+            ty = (k & 2) ? 9 : 0;
+            tz = (k & 4) ? 9 : 0;
+        }
+        const int px = tx == 0 ? 0 : (tx == 9 ? 2 : 1), py = ty == 0 ? 0 : (ty == 9 ? 2 : 1),
+                  pz = tz == 0 ? 0 : (tz == 9 ? 2 : 1);
+        const int lx = (tx + 7) & 7, ly = (ty + 7) & 7, lz = (tz + 7) & 7;
+        cell(at(tx, ty, tz), nb[px + 3 * py + 9 * pz], lz * 64 + ly * 8 + lx);
+    }
+}
+
+__global__ void __launch_bounds__(64, 10) k_box27_e8(const float* __restrict__ src, float* __restrict__ dst,
                                                  const uint8_t* __restrict__ mask, const int32_t* __restrict__ nn,
                                                  const int64_t* __restrict__ keys, int64_t n, Geometry geo,
                                                  StencilParams prm, float bck) {
-    constexpr int T = 10;
-    __shared__ __align__(16) float tile[T * T * T];
-    __shared__ int32_t nb[27];
+    __shared__ __align__(16) float tile[2][kB27Tile];
+    __shared__ __align__(16) uint8_t mt[2][512];
+    __shared__ int32_t nbs[2][28];
     const int t = threadIdx.x;
     const int cx = t & 7, cy = t >> 3;
-    for (int64_t c = blockIdx.x; c < n; c += gridDim.x) {
-        if (t < 27) nb[t] = t == 13 ? (int32_t)c : nn[c * 27 + t];
-        // interior: row (y, z) = (t % 8, t / 8) of the chunk, two 16-byte loads
-        {
-            const float4* row = reinterpret_cast<const float4*>(src + c * 512 + t * 8);
-            const float4 a = __ldg(row), b = __ldg(row + 1);
-            float* d = &tile[((t >> 3) + 1) * 100 + ((t & 7) + 1) * 10 + 1];
-            d[0] = a.x; d[1] = a.y; d[2] = a.z; d[3] = a.w;
-            d[4] = b.x; d[5] = b.y; d[6] = b.z; d[7] = b.w;
-        }
-        __syncthreads();
-        // faces: thread t takes the cell (u, v) = (t % 8, t / 8) of each of the six faces
-        {
-            const int u = t & 7, v = t >> 3;
-            // slot = px + 3 py + 9 pz; (tile cell, neighbour point)
-            const int32_t sxm = nb[12], sxp = nb[14], sym = nb[10], syp = nb[16], szm = nb[4], szp = nb[22];
-            tile[(v + 1) * 100 + (u + 1) * 10 + 0] = sxm >= 0 ? src[(int64_t)sxm * 512 + v * 64 + u * 8 + 7] : bck;
-            tile[(v + 1) * 100 + (u + 1) * 10 + 9] = sxp >= 0 ? src[(int64_t)sxp * 512 + v * 64 + u * 8 + 0] : bck;
-            tile[(v + 1) * 100 + 0 * 10 + (u + 1)] = sym >= 0 ? src[(int64_t)sym * 512 + v * 64 + 7 * 8 + u] : bck;
-            tile[(v + 1) * 100 + 9 * 10 + (u + 1)] = syp >= 0 ? src[(int64_t)syp * 512 + v * 64 + 0 * 8 + u] : bck;
-            tile[0 * 100 + (v + 1) * 10 + (u + 1)] = szm >= 0 ? src[(int64_t)szm * 512 + 7 * 64 + v * 8 + u] : bck;
-            tile[9 * 100 + (v + 1) * 10 + (u + 1)] = szp >= 0 ? src[(int64_t)szp * 512 + 0 * 64 + v * 8 + u] : bck;
-        }
-        // edges (12 x 8 cells) and corners (8): cells 0..103 of the remaining halo
-        for (int e = t; e < 104; e += 64) {
-            int tx, ty, tz;
-            if (e < 96) {
-                const int k = e >> 3, w = (e & 7) + 1;  // edge k, position w along it
-                const int a = (k & 1) ? 9 : 0, b = (k & 2) ? 9 : 0;
-                if (k < 4) { tx = w; ty = a; tz = b; }          // edges along x
-                else if (k < 8) { tx = a; ty = w; tz = b; }     // along y
-                else { tx = a; ty = b; tz = w; }                // along z
-            } else {
-                const int k = e - 96;
-                tx = (k & 1) ? 9 : 0;
-                ty = (k & 2) ? 9 : 0;
-                tz = (k & 4) ? 9 : 0;
-            }
-            const int px = tx == 0 ? 0 : (tx == 9 ? 2 : 1), py = ty == 0 ? 0 : (ty == 9 ? 2 : 1),
-                      pz = tz == 0 ? 0 : (tz == 9 ? 2 : 1);
-            const int32_t sc = nb[px + 3 * py + 9 * pz];
-            const int lx = (tx + 7) & 7, ly = (ty + 7) & 7, lz = (tz + 7) & 7;
-            tile[tz * 100 + ty * 10 + tx] = sc >= 0 ? src[(int64_t)sc * 512 + lz * 64 + ly * 8 + lx] : bck;
-        }
-        __syncthreads();
+    const int64_t stride = gridDim.x;
+    int64_t c = blockIdx.x;
+    if (c >= n) return;
+    // neighbour rows: of the first chunk now, of the second in a register
+    if (t < 27) nbs[0][t] = t == 13 ? (int32_t)c : nn[c * 27 + t];
+    int32_t nb_next = -1;
+    if (t < 27 && c + stride < n) nb_next = t == 13 ? (int32_t)(c + stride) : nn[(c + stride) * 27 + t];
+    __syncthreads();
+    box27_fill(tile[0], mt[0], nbs[0], src, mask, c, bck, t);
+    cp_async_commit();
+    for (int it = 0; c < n; ++it, c += stride) {
+        const int cur = it & 1, nxt = cur ^ 1;
+        const int64_t c1 = c + stride;
+        // the next chunk's neighbour row to shared memory, the one after it to a register
+        if (t < 27) nbs[nxt][t] = nb_next;
+        if (t < 27 && c1 + stride < n) nb_next = t == 13 ? (int32_t)(c1 + stride) : nn[(c1 + stride) * 27 + t];
+        __syncthreads();  // nbs[nxt] visible; every thread is done with tile[nxt] (chunk it - 1)
+        if (c1 < n) box27_fill(tile[nxt], mt[nxt], nbs[nxt], src, mask, c1, bck, t);
+        cp_async_commit();
+        cp_async_wait_group<1>();  // this thread's copies of chunk c have landed
+        __syncthreads();           // and everyone's
+        const float* T0 = tile[cur];
         int64_t ox = 0, oy = 0, oz = 0;
         if (prm.has_box) {
             int64_t o[3];
@@ -204,17 +234,17 @@ __global__ void __launch_bounds__(64) k_box27_e8(const float* __restrict__ src, 
         for (int a = 0; a < 3; ++a)
 #pragma unroll
             for (int b = 0; b < 3; ++b) {
-                w[a][b][0] = tile[0 * 100 + (cy + b) * 10 + (cx + a)];
-                w[a][b][1] = tile[1 * 100 + (cy + b) * 10 + (cx + a)];
+                w[a][b][0] = T0[0 * kB27Plane + (cy + b) * kB27Row + (cx + a) + 3];
+                w[a][b][1] = T0[1 * kB27Plane + (cy + b) * kB27Row + (cx + a) + 3];
             }
 #pragma unroll
         for (int z = 0; z < 8; ++z) {
 #pragma unroll
             for (int a = 0; a < 3; ++a)
 #pragma unroll
-                for (int b = 0; b < 3; ++b) w[a][b][2] = tile[(z + 2) * 100 + (cy + b) * 10 + (cx + a)];
+                for (int b = 0; b < 3; ++b) w[a][b][2] = T0[(z + 2) * kB27Plane + (cy + b) * kB27Row + (cx + a) + 3];
             const int64_t gi = c * 512 + z * 64 + cy * 8 + cx;
-            const uint8_t m = mask[gi];
+            const uint8_t m = mt[cur][z * 64 + cy * 8 + cx];
             bool act = (m & 3) == 1;
             if (prm.has_box) act = act && in_box(prm, ox + cx, oy + cy, oz + z);
             if (act) {
@@ -235,8 +265,8 @@ __global__ void __launch_bounds__(64) k_box27_e8(const float* __restrict__ src, 
                     w[a][b][1] = w[a][b][2];
                 }
         }
-        __syncthreads();
     }
+    cp_async_wait_all();
 }
 
 int make_params(sgb_grid* g, int kind, const int* src, const int* dst, const float* params, int nparams,
@@ -311,7 +341,8 @@ int launch_fields(const LaunchDesc& L, cudaStream_t s) {
     // x neighbours only under the x-fastest chunk ids
     if (L.kind != SGB_BOX27 && L.edge == 8 && !L.use_tile && !L.geo.zorder) return launch_e8(L, s);
     if (L.kind == SGB_BOX27 && L.edge == 8 && !L.use_tile && !L.grids) {
-        const unsigned nb = (unsigned)std::max<int64_t>(1, std::min<int64_t>(L.n, (int64_t)L.num_sms * 32));
+        // 10 CTAs of 64 threads per SM are resident (20 KB of shared memory each)
+        const unsigned nb = (unsigned)std::max<int64_t>(1, std::min<int64_t>(L.n, (int64_t)L.num_sms * 10));
         k_box27_e8<<<nb, 64, 0, s>>>(L.fs.in[0][0], L.fs.out[0][0], L.mask, L.nn, L.keys, L.n, L.geo, L.prm,
                                       L.g0.bck[0][0]);
         SGB_CUDA(cudaGetLastError());
