@@ -52,7 +52,7 @@ __global__ void k_ep_emit(const uint8_t* __restrict__ mask, int64_t n, int bs, c
 int ensure_point_list(sgb_grid* g, cudaStream_t s) {
     if (g->epts_valid) return SGB_OK;
     const int64_t n = g->n, bs = g->geo.bs;
-    if (n * bs >= (int64_t(1) << 32)) {
+    if ((n + 1) * bs > (int64_t(1) << 32)) {  // ids and the background chunk's points fit 32 bits
         set_error("the existing-point list holds 32-bit point ids: at most 2^32 chunk points");
         return SGB_ERANGE;
     }
@@ -102,23 +102,38 @@ __global__ void __launch_bounds__(256) k_box27_points(const float* __restrict__ 
         act = act && in_box(prm, o[0] + x, o[1] + y, o[2] + z);
     }
     if (!act) return;
+    // per axis and offset -1 / 0 / +1: the neighbour chunk's component (0, 1, 2) and the local
+    // coordinate's contribution to the point offset; ids are below 2^32, so 32-bit arithmetic
+    const uint32_t cc = (uint32_t)c;
+    int sx[3], sy[3], sz[3];
+    uint32_t ox[3], oy[3], oz[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const int qx = x + k - 1, qy = y + k - 1, qz = z + k - 1;
+        const int px = qx < 0 ? 0 : (qx >= E ? 2 : 1), py = qy < 0 ? 0 : (qy >= E ? 2 : 1),
+                  pz = qz < 0 ? 0 : (qz >= E ? 2 : 1);
+        sx[k] = px;
+        sy[k] = 3 * py;
+        sz[k] = 9 * pz;
+        ox[k] = (uint32_t)(qx + (1 - px) * E);
+        oy[k] = (uint32_t)((qy + (1 - py) * E) * E);
+        oz[k] = (uint32_t)((qz + (1 - pz) * E) * E * E);
+    }
+    const int32_t* row = nn + (int64_t)c * 27;
     float tot = 0.0f;
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
-        const int qz = z + i - 1, pz = qz < 0 ? 0 : (qz >= E ? 2 : 1), lz = qz + (1 - pz) * E;
 #pragma unroll
         for (int j = 0; j < 3; ++j) {
-            const int qy = y + j - 1, py = qy < 0 ? 0 : (qy >= E ? 2 : 1), ly = qy + (1 - py) * E;
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
-                const int qx = x + k - 1, px = qx < 0 ? 0 : (qx >= E ? 2 : 1), lx = qx + (1 - px) * E;
-                const int slot = px + 3 * py + 9 * pz;
-                int64_t pos = c;
+                const int slot = sx[k] + sy[j] + sz[i];
+                uint32_t pos = cc;
                 if (slot != 13) {
-                    const int32_t v = nn[c * 27 + slot];
-                    pos = v < 0 ? n : v;
+                    const int32_t v = __ldg(row + slot);
+                    pos = v < 0 ? (uint32_t)n : (uint32_t)v;
                 }
-                tot = __fmaf_rn(src[pos * BS + lx + E * (ly + E * lz)], prm.coeff[i * 9 + j * 3 + k], tot);
+                tot = __fmaf_rn(__ldg(src + (pos * BS + ox[k] + oy[j] + oz[i])), prm.coeff[i * 9 + j * 3 + k], tot);
             }
         }
     }
