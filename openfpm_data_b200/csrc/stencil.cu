@@ -228,8 +228,9 @@ __global__ void __launch_bounds__(64, 10) k_box27_e8(const float* __restrict__ s
             oy = o[1];
             oz = o[2];
         }
-        // window w[a][b][d] = tile[z + d][y + b][x + a] (a, b, d in 0..2, tile coordinates)
-        float w[3][3][3];
+        // window w[a][b][d] = tile[z + d][y + b][x + a] (a, b in 0..2, d in 0..3, tile coordinates):
+        // two points (z, z + 1) per step, their two FMA chains interleaved
+        float w[3][3][4];
 #pragma unroll
         for (int a = 0; a < 3; ++a)
 #pragma unroll
@@ -238,31 +239,39 @@ __global__ void __launch_bounds__(64, 10) k_box27_e8(const float* __restrict__ s
                 w[a][b][1] = T0[1 * kB27Plane + (cy + b) * kB27Row + (cx + a) + 3];
             }
 #pragma unroll
-        for (int z = 0; z < 8; ++z) {
+        for (int z = 0; z < 8; z += 2) {
 #pragma unroll
             for (int a = 0; a < 3; ++a)
 #pragma unroll
-                for (int b = 0; b < 3; ++b) w[a][b][2] = T0[(z + 2) * kB27Plane + (cy + b) * kB27Row + (cx + a) + 3];
-            const int64_t gi = c * 512 + z * 64 + cy * 8 + cx;
-            const uint8_t m = mt[cur][z * 64 + cy * 8 + cx];
-            bool act = (m & 3) == 1;
-            if (prm.has_box) act = act && in_box(prm, ox + cx, oy + cy, oz + z);
-            if (act) {
-                float tot = 0.0f;
+                for (int b = 0; b < 3; ++b) {
+                    w[a][b][2] = T0[(z + 2) * kB27Plane + (cy + b) * kB27Row + (cx + a) + 3];
+                    w[a][b][3] = T0[(z + 3) * kB27Plane + (cy + b) * kB27Row + (cx + a) + 3];
+                }
+            float tot0 = 0.0f, tot1 = 0.0f;
 #pragma unroll
-                for (int a = 0; a < 3; ++a)
+            for (int a = 0; a < 3; ++a)
 #pragma unroll
-                    for (int b = 0; b < 3; ++b)
+                for (int b = 0; b < 3; ++b)
 #pragma unroll
-                        for (int d = 0; d < 3; ++d) tot = __fmaf_rn(w[a][b][d], prm.coeff[a * 9 + b * 3 + d], tot);
-                dst[gi] = tot;
+                    for (int d = 0; d < 3; ++d) {
+                        const float cf = prm.coeff[a * 9 + b * 3 + d];
+                        tot0 = __fmaf_rn(w[a][b][d], cf, tot0);
+                        tot1 = __fmaf_rn(w[a][b][d + 1], cf, tot1);
+                    }
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int zz = z + h;
+                const uint8_t m = mt[cur][zz * 64 + cy * 8 + cx];
+                bool act = (m & 3) == 1;
+                if (prm.has_box) act = act && in_box(prm, ox + cx, oy + cy, oz + zz);
+                if (act) dst[c * 512 + zz * 64 + cy * 8 + cx] = h ? tot1 : tot0;
             }
 #pragma unroll
             for (int a = 0; a < 3; ++a)
 #pragma unroll
                 for (int b = 0; b < 3; ++b) {
-                    w[a][b][0] = w[a][b][1];
-                    w[a][b][1] = w[a][b][2];
+                    w[a][b][0] = w[a][b][2];
+                    w[a][b][1] = w[a][b][3];
                 }
         }
     }
