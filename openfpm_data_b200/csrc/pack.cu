@@ -144,11 +144,12 @@ __global__ void k_pack_emit(const int64_t* __restrict__ keys, int64_t n, Geometr
         int64_t o[3];
         origin_of(geo, key, o);
         for (int k = 0; k < nb; ++k) {
+            const PackBox& P = pbs[k];
+            const Box6 bx = P.box;
+            if (!chunk_meets(bx, o, e)) continue;  // uniform over the warp; no scan read
             const int64_t r = (int64_t)k * (n + 1) + c;
             uint32_t base = scnt[r];
             if (scnt[r + 1] == base) continue;  // no packed point of box k here (uniform)
-            const PackBox& P = pbs[k];
-            const Box6 bx = P.box;
             unsigned char* b = out + P.base;
             base -= P.pnt0;
             const uint32_t slot = sflg[r] - P.cnk0;
