@@ -91,9 +91,15 @@ __global__ void k_pack_count(const int64_t* __restrict__ keys, int64_t n, Geomet
         for (int k = 0; k < nb; ++k) {
             const Box6 bx = boxes[k];
             if (!chunk_meets(bx, o, e)) continue;  // uniform over the warp
+            uint8_t mv[16];  // the lane's mask bytes, all loads in flight at once (bs <= 512)
+#pragma unroll
+            for (int i = 0; i < 16; ++i) mv[i] = lane + 32 * i < bs ? mask[c * bs + lane + 32 * i] : 0;
             uint32_t t = 0;
-            for (int pt = lane; pt < bs; pt += 32) {
-                const bool in = (mask[c * bs + pt] & 1) && inside6(bx, o[0] + pt % e, o[1] + (pt / e) % e, o[2] + pt / (e * e));
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+                if (32 * i >= bs) break;
+                const int pt = lane + 32 * i;
+                const bool in = (mv[i] & 1) && inside6(bx, o[0] + pt % e, o[1] + (pt / e) % e, o[2] + pt / (e * e));
                 t += __popc(__ballot_sync(0xffffffffu, in));
             }
             if (lane == 0 && t) {
@@ -159,8 +165,14 @@ __global__ void k_pack_emit(const int64_t* __restrict__ keys, int64_t n, Geometr
             }
             int16_t* offs = reinterpret_cast<int16_t*>(b + P.L.off_offs);
             uint8_t* msk = b + P.L.off_mask;
-            for (int pt = lane; pt < bs; pt += 32) {
-                const uint8_t m = mask[c * bs + pt];
+            uint8_t mv[16];  // the lane's mask bytes, all loads in flight at once (bs <= 512)
+#pragma unroll
+            for (int i = 0; i < 16; ++i) mv[i] = lane + 32 * i < bs ? mask[c * bs + lane + 32 * i] : 0;
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+                if (32 * i >= bs) break;
+                const int pt = lane + 32 * i;
+                const uint8_t m = mv[i];
                 const bool in = (m & 1) && inside6(bx, o[0] + pt % e, o[1] + (pt / e) % e, o[2] + pt / (e * e));
                 const unsigned bal = __ballot_sync(0xffffffffu, in);
                 if (in) {
