@@ -33,14 +33,36 @@ __device__ __forceinline__ int64_t block_lin_ref(const Geometry& geo, const int6
 // NNStar::getNNpos (SparseGridGpu_ker_util.hpp:91-112, slots -x,+x,-y,+y,-z,+z,
 // two unused) and NNFull::getNNpos (SparseGridGpu.hpp:266-287, slot
 // dx+3dy+9dz over {0,1,2}).  Output: data position, -1 when absent.
+//
+// The keys are distinct sorted integers, so the key bl of a neighbour lies
+// within |bl - key| positions of the chunk's own: the search is limited to
+// that window (one probe for an x neighbour under x-fastest ids).
+__device__ __forceinline__ int64_t find_near(const int64_t* keys, int64_t n, int64_t i, int64_t key, int64_t bl) {
+    int64_t lo, hi;
+    if (bl > key) {
+        lo = i + 1;
+        hi = bl - key < n - i ? i + 1 + (bl - key) : n;
+    } else {
+        hi = i;
+        lo = key - bl < i ? i - (key - bl) : 0;
+    }
+    while (lo < hi) {
+        const int64_t mid = (lo + hi) >> 1;
+        if (keys[mid] < bl) lo = mid + 1;
+        else hi = mid;
+    }
+    return (lo < n && keys[lo] == bl) ? lo : -1;
+}
+
 __global__ void k_find_nn(const int64_t* keys, int64_t n, Geometry geo, int kind, int32_t* out) {
     const int nnn = kind == SGB_NN_STAR ? 8 : 27;
     const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     const int64_t chunk = t / nnn;
     const int o = (int)(t - chunk * nnn);
     if (chunk >= n) return;
+    const int64_t key = keys[chunk];
     int64_t bc[3];
-    block_coords(geo, keys[chunk], bc);
+    block_coords(geo, key, bc);
     int64_t pos = -1;
     if (kind == SGB_NN_STAR) {
         if (o < 2 * geo.dim) {
@@ -49,7 +71,8 @@ __global__ void k_find_nn(const int64_t* keys, int64_t n, Geometry geo, int kind
             if (dpos >= 0) {
                 bc[d] = dpos;
                 const int64_t bl = block_lin_ref(geo, bc);
-                if (bl >= 0) pos = find_key(keys, n, bl);
+                if (bl >= 0 && bl != key) pos = find_near(keys, n, chunk, key, bl);
+                else if (bl == key) pos = chunk;
             }
         }
     } else if (o != nnn / 2) {
@@ -59,7 +82,8 @@ __global__ void k_find_nn(const int64_t* keys, int64_t n, Geometry geo, int kind
             cnt /= 3;
         }
         const int64_t bl = block_lin_ref(geo, bc);
-        if (bl >= 0) pos = find_key(keys, n, bl);
+        if (bl >= 0 && bl != key) pos = find_near(keys, n, chunk, key, bl);
+        else if (bl == key) pos = chunk;
     }
     out[t] = (int32_t)pos;
 }
