@@ -28,18 +28,21 @@ constexpr int kRsRounds = 16;
 constexpr int kRsThreads = kRsWarps * 32;
 constexpr int kRsTile = kRsThreads * kRsRounds;  // 4096 keys per CTA
 
+constexpr int kRsMaxBuckets = 1024;  // digits of up to 10 bits
+
 template <typename K>
-__global__ void k_rs_hist(const K* keys, int64_t n, int shift, uint32_t* hist, int ntiles) {
-    __shared__ uint32_t h[256];
-    for (int i = threadIdx.x; i < 256; i += blockDim.x) h[i] = 0;
+__global__ void k_rs_hist(const K* keys, int64_t n, int shift, unsigned dmask, int nbuckets, uint32_t* hist,
+                          int ntiles) {
+    __shared__ uint32_t h[kRsMaxBuckets];
+    for (int i = threadIdx.x; i < nbuckets; i += blockDim.x) h[i] = 0;
     __syncthreads();
     const int64_t base = (int64_t)blockIdx.x * kRsTile;
     for (int k = threadIdx.x; k < kRsTile; k += blockDim.x) {
         int64_t i = base + k;
-        if (i < n) atomicAdd(&h[(unsigned)(keys[i] >> shift) & 255u], 1u);
+        if (i < n) atomicAdd(&h[(unsigned)(keys[i] >> shift) & dmask], 1u);
     }
     __syncthreads();
-    for (int d = threadIdx.x; d < 256; d += blockDim.x) hist[(size_t)d * ntiles + blockIdx.x] = h[d];
+    for (int d = threadIdx.x; d < nbuckets; d += blockDim.x) hist[(size_t)d * ntiles + blockIdx.x] = h[d];
 }
 
 // Stable scatter: items keep their order inside each digit.  Tile order is
@@ -47,9 +50,10 @@ __global__ void k_rs_hist(const K* keys, int64_t n, int shift, uint32_t* hist, i
 // __match_any_sync peer groups, counts across warps from a shared prefix.
 template <typename K>
 __global__ void __launch_bounds__(kRsThreads) k_rs_scatter(const K* kin, const uint32_t* vin, K* kout, uint32_t* vout,
-                                                            int64_t n, int shift, const uint32_t* offs, int ntiles) {
-    __shared__ uint32_t wcnt[kRsWarps][256];
-    for (int i = threadIdx.x; i < kRsWarps * 256; i += blockDim.x) (&wcnt[0][0])[i] = 0;
+                                                            int64_t n, int shift, unsigned dmask, int nbuckets,
+                                                            const uint32_t* offs, int ntiles) {
+    __shared__ uint32_t wcnt[kRsWarps][kRsMaxBuckets];
+    for (int i = threadIdx.x; i < kRsWarps * kRsMaxBuckets; i += blockDim.x) (&wcnt[0][0])[i] = 0;
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int64_t base = (int64_t)blockIdx.x * kRsTile + warp * (32 * kRsRounds);
@@ -62,7 +66,7 @@ __global__ void __launch_bounds__(kRsThreads) k_rs_scatter(const K* kin, const u
         const bool valid = i < n;
         key[r] = valid ? kin[i] : K(0);
         val[r] = valid ? (vin ? vin[i] : (uint32_t)i) : 0u;
-        const unsigned d = valid ? ((unsigned)(key[r] >> shift) & 255u) : 0x10000u;
+        const unsigned d = valid ? ((unsigned)(key[r] >> shift) & dmask) : 0x10000u;
         const unsigned peers = __match_any_sync(0xffffffffu, d);
         uint32_t cnt = 0;
         if (valid) cnt = wcnt[warp][d];
@@ -72,7 +76,7 @@ __global__ void __launch_bounds__(kRsThreads) k_rs_scatter(const K* kin, const u
         __syncwarp();
     }
     __syncthreads();
-    for (int d = threadIdx.x; d < 256; d += blockDim.x) {
+    for (int d = threadIdx.x; d < nbuckets; d += blockDim.x) {
         uint32_t run = 0;
         for (int w = 0; w < kRsWarps; ++w) {
             uint32_t c = wcnt[w][d];
@@ -85,7 +89,7 @@ __global__ void __launch_bounds__(kRsThreads) k_rs_scatter(const K* kin, const u
     for (int r = 0; r < kRsRounds; ++r) {
         const int64_t i = base + r * 32 + lane;
         if (i < n) {
-            const unsigned d = (unsigned)(key[r] >> shift) & 255u;
+            const unsigned d = (unsigned)(key[r] >> shift) & dmask;
             const size_t pos = (size_t)offs[(size_t)d * ntiles + blockIdx.x] + wcnt[warp][d] + rank[r];
             kout[pos] = key[r];
             vout[pos] = val[r];
@@ -278,23 +282,28 @@ static int radix_sort(sgb_grid* g, int64_t n, int bits, K** keys_out, uint32_t**
     SGB_TRY(vA.ensure((size_t)n * 4));
     SGB_TRY(vB.ensure((size_t)n * 4));
     const int ntiles = (int)((n + kRsTile - 1) / kRsTile);
-    SGB_TRY(hist.ensure((size_t)ntiles * 256 * 4));
-    SGB_TRY(hoff.ensure((size_t)ntiles * 256 * 4));
+    // as few passes as digits of at most 10 bits allow, the digit width spread evenly over them
+    const int passes = bits <= 0 ? 1 : (bits + 9) / 10;
+    const int dbits = bits <= 0 ? 1 : (bits + passes - 1) / passes;
+    const int nbuckets = 1 << dbits;
+    const unsigned dmask = (unsigned)nbuckets - 1u;
+    SGB_TRY(hist.ensure((size_t)ntiles * nbuckets * 4));
+    SGB_TRY(hoff.ensure((size_t)ntiles * nbuckets * 4));
     k_make_keys<K><<<nblk(n), 256, 0, s>>>(g->pend_lin.as<int64_t>(), n, kA.as<K>());
     SGB_CUDA(cudaGetLastError());
     K* kin = kA.as<K>();
     K* kout = kB.as<K>();
     uint32_t* vbuf[2] = {vA.as<uint32_t>(), vB.as<uint32_t>()};
-    const int passes = bits <= 0 ? 1 : (bits + 7) / 8;
     for (int ps = 0; ps < passes; ++ps) {
-        const int shift = ps * 8;
+        const int shift = ps * dbits;
         const uint32_t* vin = ps == 0 ? nullptr : vbuf[ps & 1];  // pass 0 ranks the insertion index itself
         uint32_t* vout = vbuf[(ps + 1) & 1];
-        k_rs_hist<K><<<ntiles, 256, 0, s>>>(kin, n, shift, hist.as<uint32_t>(), ntiles);
+        k_rs_hist<K><<<ntiles, 256, 0, s>>>(kin, n, shift, dmask, nbuckets, hist.as<uint32_t>(), ntiles);
         SGB_CUDA(cudaGetLastError());
-        SGB_TRY(scan_exclusive_u32(hist.as<uint32_t>(), hoff.as<uint32_t>(), (int64_t)ntiles * 256, nullptr,
+        SGB_TRY(scan_exclusive_u32(hist.as<uint32_t>(), hoff.as<uint32_t>(), (int64_t)ntiles * nbuckets, nullptr,
                                    &g->scratch[6], s));
-        k_rs_scatter<K><<<ntiles, kRsThreads, 0, s>>>(kin, vin, kout, vout, n, shift, hoff.as<uint32_t>(), ntiles);
+        k_rs_scatter<K><<<ntiles, kRsThreads, 0, s>>>(kin, vin, kout, vout, n, shift, dmask, nbuckets,
+                                                      hoff.as<uint32_t>(), ntiles);
         SGB_CUDA(cudaGetLastError());
         K* kt = kin;
         kin = kout;
