@@ -22,7 +22,9 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <array>
+#include <cmath>
 #include <cstdint>
 #include <cstring>
 #include <fstream>
@@ -323,12 +325,15 @@ __global__ void conv_kernel(sgb_view v, int src0, int src1, int dst0, int dst1, 
                     f(r1, r2, u, w, i, j, k);
                     dst[0][g] = r1;
                     dst[1][g] = r2;
-                } else {  // conv2_b
+                } else if constexpr (MODE == 3) {  // conv2_b
                     float r1 = 0, r2 = 0;
                     data_block<8> blk{v.data, chunk, BS};
                     f(r1, r2, u, w, blk, pnt, i, j, k);
                     dst[0][g] = r1;
                     dst[1][g] = r2;
+                } else {  // conv_cross_b: the chunk's data block and the point's offset as well
+                    data_block<8> blk{v.data, chunk, BS};
+                    dst[0][g] = f(u, blk, pnt, i, j, k);
                 }
             }
         }
@@ -579,6 +584,15 @@ class SparseGridGpu {
     void conv(grid_key_dx<3> start, grid_key_dx<3> stop, F f) {
         launch_conv<1, 1>(p_src, p_src, p_dst, p_dst, start, stop, f);
     }
+    // conv_cross_b (SparseGridGpu.hpp:2606-2621): f(cp_block, data_block, offset, i, j, k) over the
+    // NNStar halo (edge and corner cells read the background), written at active points
+    template <unsigned p_src, unsigned p_dst, unsigned stencil_size, typename F>
+    void conv_cross_b(grid_key_dx<3> start, grid_key_dx<3> stop, F f) {
+        const int keep = nn_kind_;
+        nn_kind_ = SGB_NN_STAR;
+        launch_conv<1, 4>(p_src, p_src, p_dst, p_dst, start, stop, f);
+        nn_kind_ = keep;
+    }
     template <unsigned s1, unsigned s2, unsigned d1, unsigned d2, unsigned stencil_size, typename F>
     void conv2(grid_key_dx<3> start, grid_key_dx<3> stop, F f) {
         launch_conv<2, 2>(s1, s2, d1, d2, start, stop, f);
@@ -650,6 +664,78 @@ class SparseGridGpu {
     }
     bool write_with_spacing_offset(const std::string& output, Point<dim, double> spacing, Point<dim, double> offset) {
         return write_impl(output, spacing.x, offset.x);
+    }
+
+    // insertFlush<p>(coord) (SparseGridGpu.hpp:2779-2846): insert a point into the host copy
+    // made by deviceToHost (its chunk is created with background values if missing), mark it
+    // existing and return its value for the caller to fill; hostToDevice() uploads the copy
+    template <unsigned p, typename CoordT>
+    typename std::tuple_element<p, props>::type& insertFlush(const grid_key_dx<dim, CoordT>& c) {
+        using T = typename std::tuple_element<p, props>::type;
+        if (h_data_.size() != nprop || h_mask_.empty()) deviceToHost<>();  // no host copy yet
+        int64_t bsz[3];
+        for (int d = 0; d < 3; ++d) bsz[d] = ((int64_t)size_[d] + blockEdgeSize - 1) / blockEdgeSize;
+        const int64_t b = detail::block_key(linearizer::zorder, bsz, c.get(0) / blockEdgeSize, c.get(1) / blockEdgeSize,
+                                            c.get(2) / blockEdgeSize);
+        const int64_t l = ((c.get(2) % blockEdgeSize) * blockEdgeSize + c.get(1) % blockEdgeSize) * blockEdgeSize +
+                          c.get(0) % blockEdgeSize;
+        auto it = std::lower_bound(h_keys_.begin(), h_keys_.end(), b);
+        const int64_t pos = it - h_keys_.begin();
+        if (it == h_keys_.end() || *it != b) {
+            // a new chunk at pos: background values (the background chunk's, last), mask 0
+            const int64_t n = (int64_t)h_keys_.size();
+            h_keys_.insert(it, b);
+            h_mask_.insert(h_mask_.begin() + pos * bs, bs, (uint8_t)0);
+            for (unsigned q = 0; q < nprop; ++q) {
+                const size_t es = h_data_[q].size() / ((n + 1) * bs);
+                std::vector<unsigned char> bck(h_data_[q].end() - es * bs, h_data_[q].end());
+                h_data_[q].insert(h_data_[q].begin() + pos * bs * es, bck.begin(), bck.end());
+            }
+        }
+        h_mask_[pos * bs + l] = 1;
+        return reinterpret_cast<T*>(h_data_[p].data())[pos * bs + l];
+    }
+
+    // hostToDevice(): upload the host copy (deviceToHost, insertFlush) as the grid's block map
+    void hostToDevice() {
+        const int64_t n = (int64_t)h_keys_.size();
+        std::vector<const void*> ptrs(nprop);
+        for (unsigned q = 0; q < nprop; ++q) ptrs[q] = h_data_[q].data();
+        check(sgb_load_map(g_, n, h_keys_.data(), ptrs.data(), h_mask_.data(), nullptr), "hostToDevice");
+    }
+
+    // measureBlockOccupancy / measureBlockOccupancyMemory (SparseGridGpu.hpp:2485-2554): mean and
+    // sample standard deviation over the chunks of the fraction of active (existing and not
+    // padding) / existing points
+    void measureBlockOccupancy(double& mean, double& deviation) const { occupancy(true, mean, deviation); }
+    void measureBlockOccupancyMemory(double& mean, double& deviation) const { occupancy(false, mean, deviation); }
+
+    // swap (SparseGridGpu.hpp:3403-3408)
+    void swap(SparseGridGpu& o) {
+        std::swap(g_, o.g_);
+        for (int d = 0; d < 3; ++d) std::swap(size_[d], o.size_[d]);
+        std::swap(nn_kind_, o.nn_kind_);
+        std::swap(npools_, o.npools_);
+        std::swap(nslot_, o.nslot_);
+        std::swap(pool_lin_, o.pool_lin_);
+        for (int p = 0; p < 8; ++p) std::swap(pool_val_[p], o.pool_val_[p]);
+        std::swap(pool_cnt_, o.pool_cnt_);
+        h_keys_.swap(o.h_keys_);
+        h_data_.swap(o.h_data_);
+        h_mask_.swap(o.h_mask_);
+        rem_sects_.swap(o.rem_sects_);
+        pack_subs_.swap(o.pack_subs_);
+    }
+
+    // removeUnusedBuffers (SparseGridGpu.hpp:3739-3742)
+    void removeUnusedBuffers() { check(sgb_release_scratch(g_), "removeUnusedBuffers"); }
+
+    // private_get_neighborhood_array: the device neighbour table of the current NN type (int32,
+    // -1 absent), valid until the next flush
+    const int32_t* private_get_neighborhood_array() {
+        sgb_view v;
+        check(sgb_get_view(g_, nn_kind_, &v, nullptr), "private_get_neighborhood_array");
+        return v.nn;
     }
 
     // remove(box): queue a section whose points removePoints deletes (SparseGridGpu.hpp:3528-3531)
@@ -846,6 +932,28 @@ class SparseGridGpu {
         for (size_t i : sel) f.put((char)h_mask_[i]);
         f << "\n";
         return (bool)f;
+    }
+
+    void occupancy(bool active_only, double& mean, double& deviation) const {
+        int64_t n = 0;
+        sgb_nchunks(g_, &n);
+        std::vector<uint8_t> m((n + 1) * bs);
+        check(sgb_download_map(g_, nullptr, nullptr, m.data(), nullptr), "measureBlockOccupancy");
+        std::vector<double> occ((size_t)n);
+        for (int64_t c = 0; c < n; ++c) {
+            size_t k = 0;
+            for (unsigned i = 0; i < bs; ++i) {
+                const uint8_t b = m[c * bs + i];
+                k += active_only ? ((b & 1) && !(b & 2)) : (b & 1) != 0;
+            }
+            occ[c] = (double)k / bs;
+        }
+        mean = 0;
+        for (double x : occ) mean += x;
+        mean /= (double)n;
+        deviation = 0;
+        for (double x : occ) deviation += (x - mean) * (x - mean);
+        deviation = std::sqrt(deviation / (double)(n - 1));
     }
 
     sgb_links links(int up) const {

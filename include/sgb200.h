@@ -107,6 +107,13 @@ int sgb_destroy(sgb_grid* g);
 typedef enum { SGB_LIN_SMB = 0, SGB_LIN_ZMB = 1 } sgb_linearizer;
 int sgb_set_linearizer(sgb_grid* g, int kind);
 
+/* removeUnusedBuffers (SparseGridGpu.hpp:3739-3742): free the grid's
+ * temporary device buffers (flush and scan scratch, the second buffer set,
+ * existence bitmaps, the existing-point list; the staged inserts when none
+ * are pending).  They are allocated again when needed.  Synchronises the
+ * device. */
+int sgb_release_scratch(sgb_grid* g);
+
 /* setBackgroundValue<p> (SparseGridGpu.hpp:2878-2884); value host. */
 int sgb_set_background(sgb_grid* g, int prop, const void* value_host);
 

@@ -423,10 +423,37 @@ int sgb_destroy(sgb_grid* g) {
     g->nn[0].release();
     g->nn[1].release();
     g->bits.release();
+    g->epts.release();
+    for (auto& L : g->links) {
+        L.pad_pos.release();
+        L.pad_off.release();
+        L.scan.release();
+        L.pos.release();
+        L.off.release();
+    }
     for (auto& b : g->scratch) b.release();
     g->hscratch.release();
     g->err.release();
     delete g;
+    return SGB_OK;
+}
+
+int sgb_release_scratch(sgb_grid* g) {
+    if (!g) return SGB_EINVAL;
+    cudaSetDevice(g->device);
+    SGB_CUDA(cudaDeviceSynchronize());  // no kernel of this grid may still use the buffers
+    g->keys2.release();
+    g->mask2.release();
+    for (int p = 0; p < kMaxProps; ++p) {
+        g->data2[p].release();
+        if (g->npend == 0) g->pend_val[p].release();
+    }
+    if (g->npend == 0) g->pend_lin.release();
+    g->bits.release();
+    g->bits_valid = false;
+    g->epts.release();
+    g->epts_valid = false;
+    for (auto& b : g->scratch) b.release();
     return SGB_OK;
 }
 

@@ -479,6 +479,21 @@ class SparseGridGpu:
             ops[p] = L.OP_RIGHT
         self.flush(ops, stream)
 
+    def measureBlockOccupancy(self, memory: bool = False):
+        """(mean, sample standard deviation) over the chunks of the fraction of active points
+        (existing and not padding; existing points with memory=True) -- measureBlockOccupancy /
+        measureBlockOccupancyMemory (src/SparseGridGpu/SparseGridGpu.hpp:2485-2554)."""
+        keys, _, mask = self.deviceToHost()
+        n = len(keys)
+        m = mask[: n * self.bs].reshape(n, self.bs)
+        sel = (m & 1) != 0 if memory else (m & 3) == 1
+        occ = sel.sum(axis=1) / self.bs
+        return float(occ.mean()), float(occ.std(ddof=1)) if n > 1 else float("nan")
+
+    def removeUnusedBuffers(self) -> None:
+        """Free the temporary device buffers (removeUnusedBuffers)."""
+        L.check(self._lib.sgb_release_scratch(self._h), "sgb_release_scratch")
+
     def countExistingElements(self, stream=None) -> int:
         e = C.c_int64()
         L.check(self._lib.sgb_count_existing(self._h, C.byref(e), None, _stream(stream)), "sgb_count_existing")

@@ -10,6 +10,7 @@
 // device-side paths against the C ABI calls that the Python parity tests pin
 // to the CPU oracle.  Prints "ok <name>" per check; exit status 0 when all
 // pass.
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -382,6 +383,63 @@ int main() {
         CHECK(req > 0 && sts.getOffset() == req && ps.getOffset() == req && !s1.empty() && !s2.empty() && vals_ok &&
                   dst.countExistingElements() == s1.size() + s2.size(),
               "pack_unpack");
+    }
+
+    // ---------------------------------------------------------------- host-side API
+    {
+        // measureBlockOccupancy: mean over chunks of the active fraction
+        HostMap H = download(grid.handle(), 6);
+        size_t act_pts = 0;
+        for (size_t i = 0; i < H.keys.size() * 512; ++i) act_pts += active(H.mask[i]);
+        double mean = 0, dev = 0;
+        grid.measureBlockOccupancy(mean, dev);
+        const bool occ_ok = std::fabs(mean * (double)H.keys.size() * 512 - (double)act_pts) < 1e-6 && dev >= 0;
+        CHECK(occ_ok, "measureBlockOccupancy");
+
+        // conv_cross_b: the face stencil equals conv over NNStar; the data block reads other properties
+        grid.setNNType<NNStar<3>>();
+        grid.conv_cross_b<0, 4, 1>(lo, hi, [] __device__(cp_block<float, 8>& u, data_block<8>&, int, int i, int j,
+                                                         int k) {
+            return __fadd_rn(__fadd_rn(u(i - 1, j, k), u(i + 1, j, k)), __fadd_rn(u(i, j - 1, k), u(i, j, k + 1)));
+        });
+        grid.conv<0, 5, 1>(lo, hi, [] __device__(cp_block<float, 8>& u, int i, int j, int k) {
+            return __fadd_rn(__fadd_rn(u(i - 1, j, k), u(i + 1, j, k)), __fadd_rn(u(i, j - 1, k), u(i, j, k + 1)));
+        });
+        cudaDeviceSynchronize();
+        HostMap C1 = download(grid.handle(), 6);
+        const bool cb1 = same(C1, 4, C1, 5, active);
+        grid.conv_cross_b<0, 4, 1>(lo, hi, [] __device__(cp_block<float, 8>&, data_block<8>& blk, int off, int, int,
+                                                         int) { return blk.template get<1>()[off]; });
+        cudaDeviceSynchronize();
+        HostMap C2 = download(grid.handle(), 6);
+        CHECK(cb1 && same(C2, 4, C2, 1, active), "conv_cross_b");
+
+        // insertFlush on the host copy, then hostToDevice
+        Grid6 h(sz);
+        h.setBackgroundValue<0>(0.0f);
+        h.deviceToHost<>();
+        h.insertFlush<0>(grid_key_dx<3, int>({3, 4, 5})) = 7.5f;
+        h.insertFlush<0>(grid_key_dx<3, int>({60, 61, 62})) = -2.0f;
+        h.insertFlush<0>(grid_key_dx<3, int>({4, 4, 5})) = 1.25f;  // same chunk as the first point
+        h.hostToDevice();
+        h.deviceToHost<0>();
+        const bool ins_ok = h.countExistingElements() == 3 && h.nchunks() == 2 &&
+                            h.get<0>(grid_key_dx<3, int>({3, 4, 5})) == 7.5f &&
+                            h.get<0>(grid_key_dx<3, int>({60, 61, 62})) == -2.0f &&
+                            h.get<0>(grid_key_dx<3, int>({4, 4, 5})) == 1.25f &&
+                            h.get<0>(grid_key_dx<3, int>({5, 4, 5})) == 0.0f;
+        CHECK(ins_ok, "insertFlush_hostToDevice");
+
+        // swap and removeUnusedBuffers: the grids trade contents; a flush and a stencil still run
+        const size_t na = grid.countExistingElements(), nb = h.countExistingElements();
+        grid.swap(h);
+        const bool sw = grid.countExistingElements() == nb && h.countExistingElements() == na;
+        grid.swap(h);
+        grid.removeUnusedBuffers();
+        grid.applyStencils<HeatStencil<3, 0, 1>>(grid.getBox(), STENCIL_MODE_INPLACE, 0.1f);
+        cudaDeviceSynchronize();
+        CHECK(sw && grid.countExistingElements() == na && grid.private_get_neighborhood_array() != nullptr,
+              "swap_removeUnusedBuffers");
     }
 
     // ---------------------------------------------------------------- SparseGridGpu_z (Morton chunk ids)

@@ -129,3 +129,26 @@ def test_isolated_chunks_stencils(sgb):
         err[a == b] = 0
         assert err.max() <= 1e-6
     g.check_device_errors()
+
+
+def test_occupancy_and_release(sgb):
+    rng = np.random.default_rng(8)
+    size = (40, 40, 40)
+    pts = np.unique(rng.integers(0, size, size=(9000, 3)), axis=0).astype(np.int64)
+    g = sgb.SparseGridGpu(size, ["f32", "f32"], edge=8)
+    g.insert(torch.from_numpy(pts).cuda(), [torch.from_numpy(rng.random(len(pts)).astype(np.float32)).cuda(), None])
+    g.flush(["sRight_", None])
+    g.tagBoundaries(sgb.NN_STAR)
+    keys, _, mask = g.deviceToHost()
+    n = len(keys)
+    mean, dev = g.measureBlockOccupancy()
+    assert abs(mean * n * 512 - ((mask[: n * 512] & 3) == 1).sum()) < 1e-6 and dev > 0
+    mem_mean, _ = g.measureBlockOccupancy(memory=True)
+    assert abs(mem_mean * n * 512 - len(pts)) < 1e-6
+    g.removeUnusedBuffers()
+    g.applyStencils(sgb.HEAT7, [0], [1], [0.1])
+    more = rng.integers(0, size, size=(500, 3)).astype(np.int64)
+    g.insert(torch.from_numpy(more).cuda(), [torch.from_numpy(rng.random(500).astype(np.float32)).cuda(), None])
+    g.flush(["sRight_", None])
+    assert g.countExistingElements() == len(np.unique(np.concatenate([pts, more]), axis=0))
+    g.check_device_errors()
