@@ -358,7 +358,7 @@ def run_heat128(args, dist: Dist):
     ach = 9 * npts / (t / args.steps) / 1e9
     roof = {"bound": "hbm", "achieved": round(ach, 1), "peak": peak, "unit": "GB/s", "frac": round(ach / peak, 4),
             "traffic": None, "peak_kind": pk, "alg_bytes_per_launch": 9 * npts}
-    # e2e: one solve = upload, 100 steps (one graph), download
+    # e2e: one solve = upload, 100 steps (sgb_run_steps), download
     pin = lambda a: torch.from_numpy(a).pin_memory().numpy()  # noqa: E731
     hk, hu, hm = pin(keys), pin(data[0]), pin(mask)
     out = torch.empty((len(keys) + 1) * 512, dtype=torch.float32).pin_memory()
@@ -374,7 +374,7 @@ def run_heat128(args, dist: Dist):
     te = dist.max(e0.elapsed_time(e1) / 1e3)
     e2e = {"value": round(dist.world * npts * 100 * nsolve / te / 1e9, 3), "unit": "Gpts/s",
            "h2d_bytes_per_step": int(hk.nbytes + hu.nbytes + hm.nbytes), "d2h_bytes_per_step": int(out.numel() * 4),
-           "step": "one solve: upload, 100 heat steps in one CUDA graph, download"}
+           "step": "one solve: upload, 100 heat steps (sgb_run_steps: one cooperative launch on this small grid), download"}
     cpu = None
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
         from oracle import oracle as O

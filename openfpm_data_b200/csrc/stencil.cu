@@ -278,6 +278,134 @@ __global__ void __launch_bounds__(64, 10) k_box27_e8(const float* __restrict__ s
     cp_async_wait_all();
 }
 
+// ------------------------------------------------------------------ many steps of a small grid in one launch
+// A grid of a few hundred chunks runs each step in a few microseconds, less
+// than a launch costs.  Here every step of a run is done by one cooperative
+// launch (all CTAs resident): each CTA takes chunks blockIdx.x + k *
+// gridDim.x, gathers the (e+2)^3 tile as k_stencil_tile does, updates, and
+// the CTAs meet at a grid barrier (an arrival counter, a bounded wait)
+// before the next step reads what the last one wrote.  Field reads bypass
+// L1 (other SMs wrote them during the launch).  The arithmetic and the
+// written points are those of k_stencil_tile.
+template <int KIND, int E>
+__global__ void __launch_bounds__(256) k_steps_coop(FieldSet fs, const uint8_t* __restrict__ mask,
+                                                    const int32_t* __restrict__ nn, int64_t n, GridInfo gi, int nsteps,
+                                                    unsigned* bar, unsigned* err) {
+    constexpr int T = E + 2, TT = T * T * T, BS = E * E * E;
+    constexpr int NP = KIND == SGB_GS7 ? 2 : 1;
+    __shared__ float tile[NP][TT];
+    __shared__ int abort_run;
+    if (threadIdx.x == 0) abort_run = 0;
+    for (int t = 0; t < nsteps; ++t) {
+        const int par = t & 1;
+        const float* src[2] = {par ? fs.in[1][0] : fs.in[0][0], par ? fs.in[1][NP - 1] : fs.in[0][NP - 1]};
+        float* d0 = par ? fs.out[1][0] : fs.out[0][0];
+        float* d1 = par ? fs.out[1][NP - 1] : fs.out[0][NP - 1];
+        for (int64_t chunk = blockIdx.x; chunk < n; chunk += gridDim.x) {
+            for (int cell = threadIdx.x; cell < TT; cell += blockDim.x) {
+                const int tx = cell % T, ty = (cell / T) % T, tz = cell / (T * T);
+                const int dx = tx == 0 ? -1 : (tx == T - 1 ? 1 : 0);
+                const int dy = ty == 0 ? -1 : (ty == T - 1 ? 1 : 0);
+                const int dz = tz == 0 ? -1 : (tz == T - 1 ? 1 : 0);
+                if ((dx != 0) + (dy != 0) + (dz != 0) > 1) continue;  // edges / corners: unused by 7 points
+                int64_t sc = chunk;
+                if (dx || dy || dz) sc = nn[chunk * 8 + (dx ? (dx < 0 ? 0 : 1) : dy ? (dy < 0 ? 2 : 3) : (dz < 0 ? 4 : 5))];
+                const int lx = (tx - 1 + E) % E, ly = (ty - 1 + E) % E, lz = (tz - 1 + E) % E;
+                const int64_t idx = sc * BS + lx + E * (ly + E * lz);
+                const bool ex = sc >= 0 && mask[idx] != 0;
+#pragma unroll
+                for (int p = 0; p < NP; ++p)
+                    tile[p][cell] = ex ? __ldcg(src[p] + idx) : (par ? gi.bck[1][p] : gi.bck[0][p]);
+            }
+            __syncthreads();
+            for (int pnt = threadIdx.x; pnt < BS; pnt += blockDim.x) {
+                const int x = pnt % E, y = (pnt / E) % E, z = pnt / (E * E);
+                const uint8_t m = mask[chunk * BS + pnt];
+                const bool act = (m & 1) && !(m & 2);
+                const int c = (x + 1) + T * ((y + 1) + T * (z + 1));
+                const int64_t gidx = chunk * BS + pnt;
+                if (KIND == SGB_HEAT7) {
+                    const float cur = tile[0][c];
+                    d0[gidx] = act ? heat_update(cur, tile[0][c - 1], tile[0][c + 1], tile[0][c - T], tile[0][c + T],
+                                                 tile[0][c - T * T], tile[0][c + T * T], gi.dt)
+                                   : (m ? cur : (par ? gi.bck[0][0] : gi.bck[1][0]));
+                } else {
+                    if (!act) continue;
+                    const float u = tile[0][c], v = tile[1][c];
+                    const float lu = lap7(u, tile[0][c - 1], tile[0][c + 1], tile[0][c - T], tile[0][c + T],
+                                          tile[0][c - T * T], tile[0][c + T * T]);
+                    const float lv = lap7(v, tile[1][c - 1], tile[1][c + 1], tile[1][c - T], tile[1][c + T],
+                                          tile[1][c - T * T], tile[1][c + T * T]);
+                    float un, vn;
+                    gs_update(u, v, lu, lv, gi, un, vn);
+                    d0[gidx] = un;
+                    d1[gidx] = vn;
+                }
+            }
+            __syncthreads();
+        }
+        if (t + 1 < nsteps) {
+            // grid barrier: arrival t + 1 of every CTA; the counter only grows.  Every thread
+            // fences its stores of this step before the CTA arrives.
+            __threadfence();
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                __threadfence();
+                atomicAdd(bar, 1u);
+                const unsigned target = (unsigned)(t + 1) * gridDim.x;
+                const uint64_t t0 = global_timer_ns();
+                for (uint32_t it = 0;; ++it) {
+                    if (*reinterpret_cast<volatile unsigned*>(bar) >= target) break;
+                    if ((it & 63u) == 63u && global_timer_ns() - t0 > 2000000000ull) {
+                        atomicOr(err, kErrWaitTimeout);
+                        abort_run = 1;
+                        break;
+                    }
+                }
+                __threadfence();
+            }
+            __syncthreads();
+            if (abort_run) return;
+        }
+    }
+}
+
+// Runs nsteps of a HEAT7 / GS7 ping-pong on one grid as one cooperative launch; returns
+// SGB_ENOTSUP when the grid is too large for it (the caller then takes the per-step path).
+int run_steps_coop(sgb_grid* g, int kind, const int* src, const int* dst, const StencilParams& fwd, int nsteps,
+                   cudaStream_t s) {
+    if (kind != SGB_HEAT7 && kind != SGB_GS7) return SGB_ENOTSUP;
+    if (g->n > (int64_t)g->num_sms * 4 || nsteps < 2) return SGB_ENOTSUP;
+    if ((int64_t)nsteps * g->n >= (int64_t(1) << 31)) return SGB_ENOTSUP;  // arrival counter range
+    const int np = kind == SGB_GS7 ? 2 : 1;
+    FieldSet fs;
+    for (int j = 0; j < 2; ++j) {
+        fs.in[0][j] = g->data[src[j < np ? j : 0]].as<float>();
+        fs.out[0][j] = g->data[dst[j < np ? j : 0]].as<float>();
+        fs.in[1][j] = g->data[dst[j < np ? j : 0]].as<float>();
+        fs.out[1][j] = g->data[src[j < np ? j : 0]].as<float>();
+    }
+    GridInfo gi = grid_info_of(fwd);
+    const uint8_t* mask = g->mask.as<uint8_t>();
+    const int32_t* nnp = g->nn[SGB_NN_STAR].as<int32_t>();
+    int64_t n = g->n;
+    unsigned* err = g->err.as<unsigned>();
+    SGB_TRY(g->scratch[11].ensure(64));
+    unsigned* bar = g->scratch[11].as<unsigned>();
+    SGB_CUDA(cudaMemsetAsync(bar, 0, 4, s));
+    void* kern = nullptr;
+    const int e = g->geo.edge;
+    if (kind == SGB_HEAT7) kern = e == 8 ? (void*)k_steps_coop<SGB_HEAT7, 8> : (void*)k_steps_coop<SGB_HEAT7, 4>;
+    else kern = e == 8 ? (void*)k_steps_coop<SGB_GS7, 8> : (void*)k_steps_coop<SGB_GS7, 4>;
+    int per_sm = 0;
+    SGB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, 0));
+    if (per_sm < 1) return SGB_ENOTSUP;
+    const int64_t blocks = std::min<int64_t>(n, (int64_t)per_sm * g->num_sms);
+    void* args[] = {&fs, &mask, &nnp, &n, &gi, &nsteps, &bar, &err};
+    SGB_CUDA(cudaLaunchCooperativeKernel(kern, dim3((unsigned)blocks), dim3(256), args, 0, s));
+    return SGB_OK;
+}
+
 int make_params(sgb_grid* g, int kind, const int* src, const int* dst, const float* params, int nparams,
                 const int64_t* box, StencilParams& prm) {
     std::memset(&prm, 0, sizeof(prm));
@@ -457,6 +585,15 @@ int sgb_run_steps(sgb_grid* g, int kind, const int* src, const int* dst, const f
     for (int j = 0; j < (kind == SGB_GS7 ? 2 : 1); ++j) {
         SGB_TRY(ensure_clean(g, src[j], s));
         SGB_TRY(ensure_clean(g, dst[j], s));
+    }
+    // a small grid: all steps in one cooperative launch
+    {
+        const int st = run_steps_coop(g, kind, src, dst, fwd, nsteps, s);
+        if (st == SGB_OK) {
+            if (kind == SGB_HEAT7) g->clean[nsteps % 2 ? dst[0] : src[0]] = true;
+            return SGB_OK;
+        }
+        if (st != SGB_ENOTSUP) return st;
     }
     if (!use_graph) {
         for (int k = 0; k < nsteps; ++k) {

@@ -437,3 +437,41 @@ def test_existing_offsets_and_counts(sgb, edge):
     assert np.array_equal(g.existing_offsets().cpu().numpy(), exp)
     assert g.countExistingElements() == int(exp[-1]) == len(pts)
     assert g.countBoundaryElements() == int(((m & 3) == 3).sum())
+
+
+@pytest.mark.parametrize("edge", [8, 4])
+@pytest.mark.parametrize("kind", ["heat", "gs"])
+@pytest.mark.parametrize("nsteps", [2, 7])
+def test_run_steps_small_grid_one_launch(sgb, edge, kind, nsteps):
+    """A small grid runs all steps in one cooperative launch: the result equals the
+    step-by-step applyStencils path bit for bit (ping-pong, distinct backgrounds)."""
+    rng = np.random.default_rng(100 + edge + nsteps)
+    size = (40, 36, 44) if edge == 8 else (24, 20, 28)
+    pts = np.unique(rng.integers(0, size, size=(9000 if edge == 8 else 3000, 3)), axis=0).astype(np.int64)
+    bck = [0.3, -0.2, 0.7, 0.1]
+    grids = []
+    for _ in range(2):
+        g = sgb.SparseGridGpu(size, ["f32"] * 4, edge=edge)
+        for p, b in enumerate(bck):
+            g.setBackgroundValue(p, b)
+        vals = [np.random.default_rng(7).random(len(pts)).astype(np.float32) for _ in range(4)]
+        g.insert(torch.from_numpy(pts).cuda(), [torch.from_numpy(v).cuda() for v in vals])
+        g.flush(["sRight_"] * 4)
+        g.tagBoundaries(sgb.NN_STAR)
+        grids.append(g)
+    a, b = grids
+    assert a.nchunks <= 4 * torch.cuda.get_device_properties(0).multi_processor_count
+    if kind == "heat":
+        src, dst, prm, k = [0], [1], [0.1], sgb.HEAT7
+    else:
+        src, dst, prm, k = [0, 1], [2, 3], [0.16, 0.08, 0.035, 0.065, 1.0], sgb.GS7
+    fin = a.run_steps(k, src, dst, prm, nsteps, use_graph=False)
+    for s in range(nsteps):
+        b.applyStencils(k, src if s % 2 == 0 else dst, dst if s % 2 == 0 else src, prm)
+    assert fin == (nsteps % 2 == 1)
+    ka, da, ma = a.deviceToHost()
+    kb, db, mb = b.deviceToHost()
+    assert np.array_equal(ka, kb) and np.array_equal(ma, mb)
+    for p in range(4):
+        assert np.array_equal(da[p].view(np.uint32), db[p].view(np.uint32)), f"property {p}"
+    a.check_device_errors()
