@@ -481,7 +481,8 @@ def run_batched256(args, dist: Dist):
     value: solves/s of the batched form (one persistent launch per step over
     the concatenated block maps, each solve's 200 steps one CUDA graph) with
     the autotuned launch; beside it the same solves with per-grid plain
-    launches (one sgb_run_steps per grid, no graph)."""
+    launches (one applyStencils per grid per step), with the reference's
+    one-CTA-per-chunk execution model, and with one sgb_run_steps per grid."""
     import torch
 
     import openfpm_data_b200 as sgb
@@ -519,15 +520,26 @@ def run_batched256(args, dist: Dist):
         g.build_balls(sp.balls, sp.init, sp.seed, [0])
         grids.append(g)
     for g in grids[:4]:
-        g.run_steps(sgb.HEAT7, [0], [1], [W.HEAT_DT], 4, use_graph=False)
+        for k in range(4):
+            g.applyStencils(sgb.HEAT7, [k % 2], [1 - k % 2], [W.HEAT_DT])
     torch.cuda.synchronize()
+    # plain drop-in use: one applyStencils launch per grid per step (the pipelined kernel)
     p0, p1 = _events()
     p0.record()
     for g in grids:
-        g.run_steps(sgb.HEAT7, [0], [1], [W.HEAT_DT], steps_per_solve, use_graph=False)
+        for k in range(steps_per_solve):
+            g.applyStencils(sgb.HEAT7, [k % 2], [1 - k % 2], [W.HEAT_DT])
     p1.record()
     torch.cuda.synchronize()
     tp = dist.max(p0.elapsed_time(p1) / 1e3)
+    # per-grid sgb_run_steps (grids of at most 4 chunks per SM run all steps in one cooperative launch)
+    q0, q1 = _events()
+    q0.record()
+    for g in grids:
+        g.run_steps(sgb.HEAT7, [0], [1], [W.HEAT_DT], steps_per_solve, use_graph=False)
+    q1.record()
+    torch.cuda.synchronize()
+    tq = dist.max(q0.elapsed_time(q1) / 1e3)
     # the reference's execution model: one applyStencils launch per grid per step, one CTA per chunk
     # (the generic tile kernel, which gathers the halo per cell as loadGhostBlock does)
     r0, r1 = _events()
@@ -542,6 +554,7 @@ def run_batched256(args, dist: Dist):
         g.close()
     plain = dist.world * len(specs) / tp
     plain_ref = dist.world * len(specs) / tr
+    per_grid_runs = dist.world * len(specs) / tq
     peak, pk = _peak_hbm()
     ach = 9 * pts * steps_per_solve * nsolves / (t / dist.world) / 1e9 if dist.world == 1 else None
     roof = {"bound": "hbm", "achieved": round(ach, 1) if ach else None, "peak": peak, "unit": "GB/s",
@@ -556,6 +569,8 @@ def run_batched256(args, dist: Dist):
                               "plain_solves_per_s": round(plain, 3), "batched_over_plain": round(batched / plain, 2),
                               "plain_one_cta_per_chunk_solves_per_s": round(plain_ref, 3),
                               "batched_over_plain_one_cta_per_chunk": round(batched / plain_ref, 2),
+                              "per_grid_run_steps_solves_per_s": round(per_grid_runs, 3),
+                              "batched_over_per_grid_run_steps": round(batched / per_grid_runs, 2),
                               "l2": "resident fields >> L2"},
                  roofline=roof, cpu_baseline=None, e2e=None, gpu_launches=steps_per_solve * nsolves, clocks=clk)
 
