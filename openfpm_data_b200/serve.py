@@ -211,7 +211,13 @@ def solve_alone(req: W.Request, device: int = 0, use_graph: bool = False):
             g.setBackgroundValue(p, b)
     g.build_balls(balls_of(req), 0 if req.kind == "heat" else 1, req.vseed, list(range(nf)))
     prm = HEAT_PARAMS if req.kind == "heat" else GS_PARAMS
-    fin = g.run_steps(KIND[req.kind], list(range(nf)), list(range(nf, 2 * nf)), prm, req.steps, use_graph=use_graph)
+    a, b = list(range(nf)), list(range(nf, 2 * nf))
+    if use_graph:
+        fin = g.run_steps(KIND[req.kind], a, b, prm, req.steps, use_graph=True)
+    else:  # one applyStencils launch per step
+        for k in range(req.steps):
+            g.applyStencils(KIND[req.kind], a if k % 2 == 0 else b, b if k % 2 == 0 else a, prm)
+        fin = req.steps % 2 == 1
     keys, data, mask = g.deviceToHost()
     n = len(keys)
     off = nf if fin else 0
