@@ -288,7 +288,7 @@ __global__ void __launch_bounds__(64, 10) k_box27_e8(const float* __restrict__ s
 // L1 (other SMs wrote them during the launch).  The arithmetic and the
 // written points are those of k_stencil_tile.
 template <int KIND, int E>
-__global__ void __launch_bounds__(256) k_steps_coop(FieldSet fs, const uint8_t* __restrict__ mask,
+__global__ void __launch_bounds__(E * E * E < 256 ? 256 : E * E * E) k_steps_coop(FieldSet fs, const uint8_t* __restrict__ mask,
                                                     const int32_t* __restrict__ nn, int64_t n, GridInfo gi, int nsteps,
                                                     unsigned* bar, unsigned* err) {
     constexpr int T = E + 2, TT = T * T * T, BS = E * E * E;
@@ -302,7 +302,16 @@ __global__ void __launch_bounds__(256) k_steps_coop(FieldSet fs, const uint8_t* 
         float* d0 = par ? fs.out[1][0] : fs.out[0][0];
         float* d1 = par ? fs.out[1][NP - 1] : fs.out[0][NP - 1];
         for (int64_t chunk = blockIdx.x; chunk < n; chunk += gridDim.x) {
-            for (int cell = threadIdx.x; cell < TT; cell += blockDim.x) {
+            constexpr int THREADS = BS < 256 ? 256 : BS;
+            constexpr int ROUNDS = (TT + THREADS - 1) / THREADS;
+            // all of the thread's tile cells are loaded before any is stored (the loads overlap)
+            float v[ROUNDS][NP];
+            int cells[ROUNDS];
+#pragma unroll
+            for (int r = 0; r < ROUNDS; ++r) {
+                const int cell = threadIdx.x + r * THREADS;
+                cells[r] = -1;
+                if (cell >= TT) continue;
                 const int tx = cell % T, ty = (cell / T) % T, tz = cell / (T * T);
                 const int dx = tx == 0 ? -1 : (tx == T - 1 ? 1 : 0);
                 const int dy = ty == 0 ? -1 : (ty == T - 1 ? 1 : 0);
@@ -313,10 +322,15 @@ __global__ void __launch_bounds__(256) k_steps_coop(FieldSet fs, const uint8_t* 
                 const int lx = (tx - 1 + E) % E, ly = (ty - 1 + E) % E, lz = (tz - 1 + E) % E;
                 const int64_t idx = sc * BS + lx + E * (ly + E * lz);
                 const bool ex = sc >= 0 && mask[idx] != 0;
+                cells[r] = cell;
 #pragma unroll
-                for (int p = 0; p < NP; ++p)
-                    tile[p][cell] = ex ? __ldcg(src[p] + idx) : (par ? gi.bck[1][p] : gi.bck[0][p]);
+                for (int p = 0; p < NP; ++p) v[r][p] = ex ? __ldcg(src[p] + idx) : (par ? gi.bck[1][p] : gi.bck[0][p]);
             }
+#pragma unroll
+            for (int r = 0; r < ROUNDS; ++r)
+                if (cells[r] >= 0)
+#pragma unroll
+                    for (int p = 0; p < NP; ++p) tile[p][cells[r]] = v[r][p];
             __syncthreads();
             for (int pnt = threadIdx.x; pnt < BS; pnt += blockDim.x) {
                 const int x = pnt % E, y = (pnt / E) % E, z = pnt / (E * E);
@@ -397,12 +411,13 @@ int run_steps_coop(sgb_grid* g, int kind, const int* src, const int* dst, const 
     const int e = g->geo.edge;
     if (kind == SGB_HEAT7) kern = e == 8 ? (void*)k_steps_coop<SGB_HEAT7, 8> : (void*)k_steps_coop<SGB_HEAT7, 4>;
     else kern = e == 8 ? (void*)k_steps_coop<SGB_GS7, 8> : (void*)k_steps_coop<SGB_GS7, 4>;
+    const int threads = e == 8 ? 512 : 256;  // one thread per chunk point (8^3), 256 for 4^3
     int per_sm = 0;
-    SGB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, 0));
+    SGB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, 0));
     if (per_sm < 1) return SGB_ENOTSUP;
     const int64_t blocks = std::min<int64_t>(n, (int64_t)per_sm * g->num_sms);
     void* args[] = {&fs, &mask, &nnp, &n, &gi, &nsteps, &bar, &err};
-    SGB_CUDA(cudaLaunchCooperativeKernel(kern, dim3((unsigned)blocks), dim3(256), args, 0, s));
+    SGB_CUDA(cudaLaunchCooperativeKernel(kern, dim3((unsigned)blocks), dim3(threads), args, 0, s));
     return SGB_OK;
 }
 
