@@ -248,6 +248,8 @@ int ensure_bits(sgb_grid* g, cudaStream_t s);
 // points.cu
 int ensure_point_list(sgb_grid* g, cudaStream_t s);
 int launch_points_box27(sgb_grid* g, const int* src, const int* dst, const StencilParams& prm, cudaStream_t s);
+int launch_points_box27_sparse(sgb_grid* g, const int* src, const int* dst, const StencilParams& prm,
+                               cudaStream_t s);
 
 // stencil.cu
 int launch_stencil(sgb_grid* g, int kind, const int* src, const int* dst, const StencilParams& prm,

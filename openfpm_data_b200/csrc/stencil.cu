@@ -522,6 +522,10 @@ int launch_stencil_impl(sgb_grid* g, int kind, const int* src, const int* dst, c
                         cudaStream_t s, bool use_tile) {
     if (g->n == 0) return SGB_OK;
     if (kind == SGB_BOX27_NS) return launch_points_box27(g, src, dst, prm, s);
+    if (kind == SGB_BOX27 && !use_tile) {  // sparse chunks: the point list
+        const int st = launch_points_box27_sparse(g, src, dst, prm, s);
+        if (st != SGB_ENOTSUP) return st;
+    }
     const int nnk = kind == SGB_BOX27 ? SGB_NN_FULL : SGB_NN_STAR;
     SGB_TRY(ensure_neighbours(g, nnk, s));
     const int np = kind == SGB_GS7 ? 2 : 1;
@@ -595,7 +599,7 @@ int sgb_run_steps(sgb_grid* g, int kind, const int* src, const int* dst, const f
     if (final_is_dst) *final_is_dst = nsteps % 2;
     if (nsteps == 0 || g->n == 0) return SGB_OK;
     SGB_TRY(ensure_neighbours(g, kind == SGB_BOX27 || kind == SGB_BOX27_NS ? SGB_NN_FULL : SGB_NN_STAR, s));
-    if (kind == SGB_BOX27_NS) SGB_TRY(ensure_point_list(g, s));  // built outside the capture
+    if (kind == SGB_BOX27_NS || kind == SGB_BOX27) SGB_TRY(ensure_point_list(g, s));  // built outside the capture
     // both halves of the ping-pong are read as sources; no sanitising inside a capture
     for (int j = 0; j < (kind == SGB_GS7 ? 2 : 1); ++j) {
         SGB_TRY(ensure_clean(g, src[j], s));

@@ -475,3 +475,42 @@ def test_run_steps_small_grid_one_launch(sgb, edge, kind, nsteps):
     for p in range(4):
         assert np.array_equal(da[p].view(np.uint32), db[p].view(np.uint32)), f"property {p}"
     a.check_device_errors()
+
+
+@pytest.mark.parametrize("edge", [8, 4])
+@pytest.mark.parametrize("boxed", [False, True])
+def test_box27_sparse_chunks_point_path(sgb, edge, boxed):
+    """Conv3x3x3 on sparse chunks (fewer than an eighth of their points exist) runs over
+    the existing-point list; the result equals the shared-tile kernel's bit for bit and
+    the oracle's."""
+    rng = np.random.default_rng(200 + edge)
+    size = (96, 80, 88)
+    pts = np.unique(rng.integers(0, size, size=(12000, 3)), axis=0).astype(np.int64)
+    v = (rng.random(len(pts)).astype(np.float32) - 0.5) * 3
+    coeff = (rng.random(27).astype(np.float32) - 0.4).tolist()
+    box = ((4, 3, 5), (80, 70, 77)) if boxed else None
+    out = []
+    for tiled in (False, True):
+        g = sgb.SparseGridGpu(size, ["f32", "f32"], edge=edge)
+        g.setBackgroundValue(0, 0.4)
+        g.setBackgroundValue(1, -0.6)
+        g.insert(torch.from_numpy(pts).cuda(), [torch.from_numpy(v).cuda(), None])
+        g.flush(["sRight_", None])
+        g.tagBoundaries(sgb.NN_FULL)
+        assert g.countExistingElements() * 8 < g.nchunks * g.bs  # sparse: the point path is taken
+        g.applyStencils(sgb.BOX27, [0], [1], coeff, box=box, tiled=tiled)
+        out.append(g.deviceToHost())
+        g.check_device_errors()
+    (ka, da, ma), (kb, db, mb) = out
+    assert np.array_equal(ka, kb) and np.array_equal(ma, mb)
+    act = (ma[: len(ka) * (edge ** 3)] & 3) == 1
+    n = len(ka) * edge ** 3
+    assert np.array_equal(da[1][:n][act].view(np.uint32), db[1][:n][act].view(np.uint32))
+    o = O.OracleGrid(size, edge=edge, ptypes=[O.T_F32, O.T_F32])
+    o.set_background(0, 0.4)
+    o.set_background(1, -0.6)
+    o.insert_flush(pts, [v, np.zeros(len(v), np.float32)], [O.OP_RIGHT, O.OP_NONE])
+    o.tag_boundaries(O.NN_FULL)
+    o.box27(0, 1, np.asarray(coeff, np.float32), box)
+    ok_, od, om = o.export()
+    assert np.array_equal(da[1][:n][act].view(np.uint32), od[1][:n][act].view(np.uint32))
