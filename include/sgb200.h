@@ -114,6 +114,13 @@ int sgb_set_linearizer(sgb_grid* g, int kind);
  * device. */
 int sgb_release_scratch(sgb_grid* g);
 
+/* Self-check of failure detection (no reference counterpart): runs the
+ * library's two kinds of bounded wait -- on an mbarrier phase and on an
+ * arrival counter -- on conditions nothing satisfies, with a limit of
+ * limit_ns (at most 1 s).  Returns SGB_ETIMEOUT when both gave up as they
+ * should, with the device still usable. */
+int sgb_probe_bounded_waits(int64_t limit_ns, int device, sgb_stream s);
+
 /* setBackgroundValue<p> (SparseGridGpu.hpp:2878-2884); value host. */
 int sgb_set_background(sgb_grid* g, int prop, const void* value_host);
 

@@ -152,3 +152,20 @@ def test_occupancy_and_release(sgb):
     g.flush(["sRight_", None])
     assert g.countExistingElements() == len(np.unique(np.concatenate([pts, more]), axis=0))
     g.check_device_errors()
+
+
+def test_bounded_waits_give_up_and_the_device_stays_usable(sgb):
+    """Failure detection without a GPU fault: a wait on an mbarrier phase nobody completes
+    and one on a counter nobody increments each give up after 20 ms; the host reads
+    SGB_ETIMEOUT and the device keeps working."""
+    from openfpm_data_b200 import _lib as L
+    lib = L.load()
+    st = lib.sgb_probe_bounded_waits(20_000_000, 0, None)
+    assert st == 6  # SGB_ETIMEOUT
+    g = sgb.SparseGridGpu((32, 32, 32), ["f32", "f32"], edge=8)
+    pts = np.array([[1, 2, 3], [4, 5, 6], [30, 30, 30]], dtype=np.int64)
+    g.insert(torch.from_numpy(pts).cuda(), [torch.ones(3, device="cuda"), None])
+    g.flush(["sRight_", None])
+    g.applyStencils(sgb.HEAT7, [0], [1], [0.1])
+    g.check_device_errors()
+    assert g.countExistingElements() == 3
