@@ -385,12 +385,19 @@ static int flush_impl(sgb_grid* g, const int* ops, int bits, cudaStream_t s) {
         const int64_t nold = g->n, nn_ = nold + NB;
         k_compact_new<<<nblk(B), 256, 0, s>>>(ublk_key, B, isnew, rank, newkeys);
         SGB_CUDA(cudaGetLastError());
-        // second buffer set sized for the new map (contents are rebuilt)
-        const int64_t cap2 = std::max<int64_t>(nn_ + nn_ / 2, 16);
-        SGB_TRY(g->keys2.ensure((size_t)cap2 * 8));
-        SGB_TRY(g->mask2.ensure((size_t)(cap2 + 1) * bs));
+        // second buffer set for the new map (contents are rebuilt): kept while it holds the map,
+        // otherwise allocated for twice the map, so that a growing map reallocates rarely (each
+        // reallocation frees and maps gigabytes and stalls the device)
+        int64_t cap2 = std::min<int64_t>((int64_t)(g->keys2.bytes / 8), (int64_t)(g->mask2.bytes / bs) - 1);
         for (int p = 0; p < g->nprop; ++p)
-            SGB_TRY(g->data2[p].ensure((size_t)(cap2 + 1) * bs * elem_size(g->ptype[p])));
+            cap2 = std::min<int64_t>(cap2, (int64_t)(g->data2[p].bytes / ((size_t)bs * elem_size(g->ptype[p]))) - 1);
+        if (cap2 < nn_) {
+            cap2 = std::max<int64_t>(2 * nn_, 16);
+            SGB_TRY(g->keys2.ensure((size_t)cap2 * 8));
+            SGB_TRY(g->mask2.ensure((size_t)(cap2 + 1) * bs));
+            for (int p = 0; p < g->nprop; ++p)
+                SGB_TRY(g->data2[p].ensure((size_t)(cap2 + 1) * bs * elem_size(g->ptype[p])));
+        }
         DevBuf& posbuf = g->scratch[5];  // histogram offsets are no longer needed
         SGB_TRY(posbuf.ensure((size_t)(nold + NB) * 8 + 64));
         int64_t* oldpos = posbuf.as<int64_t>();

@@ -43,6 +43,8 @@ int DevBuf::reserve(size_t need) {
     return SGB_OK;
 }
 
+int DevBuf::grow(size_t need) { return need <= bytes ? SGB_OK : ensure(2 * need); }
+
 int DevBuf::ensure(size_t need) {
     if (need <= bytes) return SGB_OK;
     if (p) cudaFree(p);

@@ -43,6 +43,7 @@ struct DevBuf {
     size_t bytes = 0;
     int reserve(size_t need);   // keeps contents
     int ensure(size_t need);    // may drop contents
+    int grow(size_t need);      // may drop contents; grows to twice the need (for tables that follow a growing map)
     void release();
     template <typename T>
     T* as() const { return static_cast<T*>(p); }

@@ -202,7 +202,7 @@ __global__ void k_tag_generic(const uint64_t* bits, const int32_t* nn, int64_t n
 int ensure_neighbours(sgb_grid* g, int nn, cudaStream_t s) {
     if (g->nn_valid[nn]) return SGB_OK;
     const int nnn = nn == SGB_NN_STAR ? 8 : 27;
-    SGB_TRY(g->nn[nn].ensure((size_t)(g->n + 1) * nnn * 4));
+    SGB_TRY(g->nn[nn].grow((size_t)(g->n + 1) * nnn * 4));
     if (g->n > 0) {
         const int64_t total = g->n * nnn;
         k_find_nn<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(g->keys.as<int64_t>(), g->n, g->geo, nn,
@@ -216,7 +216,7 @@ int ensure_neighbours(sgb_grid* g, int nn, cudaStream_t s) {
 int ensure_bits(sgb_grid* g, cudaStream_t s) {
     if (g->bits_valid) return SGB_OK;
     const int words = g->geo.bs / 64;
-    SGB_TRY(g->bits.ensure((size_t)(g->n + 1) * words * 8));
+    SGB_TRY(g->bits.grow((size_t)(g->n + 1) * words * 8));
     if (g->n > 0) {
         const int64_t threads = g->n * 32;
         k_bits<<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(g->mask.as<uint8_t>(), g->n, g->geo.bs,

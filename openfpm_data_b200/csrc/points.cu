@@ -70,7 +70,7 @@ int ensure_point_list(sgb_grid* g, cudaStream_t s) {
         SGB_CUDA(cudaMemcpyAsync(g->hscratch.p, offs + n, 4, cudaMemcpyDeviceToHost, s));
         SGB_CUDA(cudaStreamSynchronize(s));
         g->nepts = *(uint32_t*)g->hscratch.p;
-        SGB_TRY(g->epts.ensure((size_t)g->nepts * 4 + 16));
+        SGB_TRY(g->epts.grow((size_t)g->nepts * 4 + 16));
         k_ep_emit<<<blocks, 256, 0, s>>>(g->mask.as<uint8_t>(), n, (int)bs, offs, g->epts.as<uint32_t>());
         SGB_CUDA(cudaGetLastError());
     }
