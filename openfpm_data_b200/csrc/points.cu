@@ -23,28 +23,47 @@
 
 namespace sgb {
 
-// Existing points per chunk: one warp per chunk, ballot counts.
-__global__ void k_ep_count(const uint8_t* __restrict__ mask, int64_t n, int bs, uint32_t* counts) {
+// The list is read off the existence bitmaps (one bit per point, kept for
+// tagBoundaries): 64 bytes per 8^3 chunk instead of its 512 mask bytes.
+// Warp per chunk; lane l owns points [l * P, l * P + P) with P = bs / 32.
+__device__ __forceinline__ uint32_t lane_bits(const uint64_t* __restrict__ bits, int64_t c, int bs, int lane) {
+    const int P = bs >> 5, words = bs >> 6;
+    const int first = lane * P;
+    const uint64_t w = bits[c * words + (first >> 6)];
+    return (uint32_t)(w >> (first & 63)) & ((P == 32 ? 0u : (1u << P)) - 1u);
+}
+
+__global__ void k_ep_count(const uint64_t* __restrict__ bits, int64_t n, int bs, uint32_t* counts) {
     const int lane = threadIdx.x & 31;
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
     for (int64_t c = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; c < n; c += nw) {
-        uint32_t t = 0;
-        for (int pt = lane; pt < bs; pt += 32) t += __popc(__ballot_sync(0xffffffffu, mask[c * bs + pt] & 1));
+        uint32_t t = __popc(lane_bits(bits, c, bs, lane));
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
         if (lane == 0) counts[c] = t;
     }
 }
 
-__global__ void k_ep_emit(const uint8_t* __restrict__ mask, int64_t n, int bs, const uint32_t* __restrict__ offs,
+__global__ void k_ep_emit(const uint64_t* __restrict__ bits, int64_t n, int bs, const uint32_t* __restrict__ offs,
                           uint32_t* out) {
     const int lane = threadIdx.x & 31;
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const int P = bs >> 5;
     for (int64_t c = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; c < n; c += nw) {
-        uint32_t base = offs[c];
-        for (int pt = lane; pt < bs; pt += 32) {
-            const bool ex = mask[c * bs + pt] & 1;
-            const unsigned bal = __ballot_sync(0xffffffffu, ex);
-            if (ex) out[base + __popc(bal & lanemask_lt())] = (uint32_t)(c * bs + pt);
-            base += __popc(bal);
+        uint32_t m = lane_bits(bits, c, bs, lane);
+        const uint32_t cnt = __popc(m);
+        uint32_t pre = cnt;  // inclusive prefix over the lanes
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t v = __shfl_up_sync(0xffffffffu, pre, o);
+            if (lane >= o) pre += v;
+        }
+        uint32_t pos = offs[c] + pre - cnt;
+        const uint32_t base = (uint32_t)(c * bs) + (uint32_t)(lane * P);
+        while (m) {
+            const int b = __ffs(m) - 1;
+            out[pos++] = base + (uint32_t)b;
+            m &= m - 1;
         }
     }
 }
@@ -63,7 +82,8 @@ int ensure_point_list(sgb_grid* g, cudaStream_t s) {
         uint32_t* counts = g->scratch[1].as<uint32_t>();
         uint32_t* offs = g->scratch[2].as<uint32_t>();
         const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>((int64_t)g->num_sms * 8, (n + 7) / 8));
-        k_ep_count<<<blocks, 256, 0, s>>>(g->mask.as<uint8_t>(), n, (int)bs, counts);
+        SGB_TRY(ensure_bits(g, s));
+        k_ep_count<<<blocks, 256, 0, s>>>(g->bits.as<uint64_t>(), n, (int)bs, counts);
         SGB_CUDA(cudaGetLastError());
         SGB_TRY(scan_exclusive_u32(counts, offs, n, offs + n, &g->scratch[6], s));
         SGB_TRY(g->hscratch.ensure(64));
@@ -71,7 +91,7 @@ int ensure_point_list(sgb_grid* g, cudaStream_t s) {
         SGB_CUDA(cudaStreamSynchronize(s));
         g->nepts = *(uint32_t*)g->hscratch.p;
         SGB_TRY(g->epts.grow((size_t)g->nepts * 4 + 16));
-        k_ep_emit<<<blocks, 256, 0, s>>>(g->mask.as<uint8_t>(), n, (int)bs, offs, g->epts.as<uint32_t>());
+        k_ep_emit<<<blocks, 256, 0, s>>>(g->bits.as<uint64_t>(), n, (int)bs, offs, g->epts.as<uint32_t>());
         SGB_CUDA(cudaGetLastError());
     }
     g->epts_valid = true;
