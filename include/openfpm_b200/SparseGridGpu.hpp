@@ -347,6 +347,7 @@ __global__ void conv_kernel(sgb_view v, int src0, int src1, int dst0, int dst1, 
 template <typename AggregateT, unsigned E>
 struct SparseGridGpu_ker {
     sgb_view v;
+    unsigned long long bck[8];  // background of every property, as raw bytes (device remove)
     int64_t* pool_lin;
     void* pool_val[8];
     int32_t* pool_cnt;
@@ -393,6 +394,30 @@ struct SparseGridGpu_ker {
     }
 
     // get<p>(coord): value, or the background when the point does not exist
+    // remove(coord) (SparseGridGpu_ker.cuh:664-668 -> BlockMapGpu_ker::remove, BlockMapGpu_ker.cuh:
+    // 310-331): the point's mask byte is cleared (no effect if its chunk is absent); its properties
+    // get their backgrounds, which the grid keeps in every non-existing point
+    template <typename CoordT>
+    __device__ void remove(const grid_key_dx<3, CoordT>& coord) const {
+        const int64_t lin = getLinId(coord), bs = E * E * E;
+        const int64_t pos = detail::find_key(v.keys, v.n, lin / bs);
+        if (pos < 0) return;
+        const int64_t idx = pos * bs + lin % bs;
+        const_cast<uint8_t*>(v.mask)[idx] = 0;
+        clear_props(idx, std::make_index_sequence<std::tuple_size<props>::value>{});
+    }
+    template <size_t... I>
+    __device__ void clear_props(int64_t idx, std::index_sequence<I...>) const {
+        (clear_prop<I>(idx), ...);
+    }
+    template <size_t I>
+    __device__ void clear_prop(int64_t idx) const {
+        using T = typename std::tuple_element<I, props>::type;
+        T b;
+        memcpy(&b, &bck[I], sizeof(T));
+        static_cast<T*>(v.data[I])[idx] = b;
+    }
+
     template <unsigned p, typename CoordT>
     __device__ typename std::tuple_element<p, props>::type get(const grid_key_dx<3, CoordT>& coord) const {
         using T = typename std::tuple_element<p, props>::type;
@@ -437,6 +462,7 @@ class SparseGridGpu {
 
     sgb_grid* g_ = nullptr;
     size_t size_[3];
+    unsigned long long bck_raw_[8] = {};  // backgrounds as raw bytes, for the view's device remove
     int nn_kind_ = SGB_NN_STAR;  // setNNType
     // device insert pools
     int64_t npools_ = 0, nslot_ = 0;
@@ -494,6 +520,8 @@ class SparseGridGpu {
     template <unsigned p>
     void setBackgroundValue(typename std::tuple_element<p, props>::type v) {
         check(sgb_set_background(g_, p, &v), "setBackgroundValue");
+        bck_raw_[p] = 0;
+        std::memcpy(&bck_raw_[p], &v, sizeof(v));
     }
 
     // setGPUInsertBuffer(nBlock, nSlot) (SparseGridGpu.hpp:2270-2277)
@@ -518,6 +546,9 @@ class SparseGridGpu {
     device_grid_type toKernel() {
         device_grid_type k{};
         check(sgb_get_view(g_, nn_kind_, &k.v, nullptr), "toKernel");
+        // the kernel may remove points: cached existence data is rebuilt when next needed
+        check(sgb_existence_changed(g_), "toKernel");
+        for (unsigned p = 0; p < nprop && p < 8; ++p) k.bck[p] = bck_raw_[p];
         k.pool_lin = pool_lin_;
         for (int p = 0; p < 8; ++p) k.pool_val[p] = pool_val_[p];
         k.pool_cnt = pool_cnt_;
@@ -715,6 +746,7 @@ class SparseGridGpu {
         std::swap(g_, o.g_);
         for (int d = 0; d < 3; ++d) std::swap(size_[d], o.size_[d]);
         std::swap(nn_kind_, o.nn_kind_);
+        for (int p = 0; p < 8; ++p) std::swap(bck_raw_[p], o.bck_raw_[p]);
         std::swap(npools_, o.npools_);
         std::swap(nslot_, o.nslot_);
         std::swap(pool_lin_, o.pool_lin_);

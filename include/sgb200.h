@@ -121,6 +121,13 @@ int sgb_release_scratch(sgb_grid* g);
  * should, with the device still usable. */
 int sgb_probe_bounded_waits(int64_t limit_ns, int device, sgb_stream s);
 
+/* Tell the grid that a user kernel may have changed which points exist
+ * (device-side remove through the view): the cached existence bitmaps and
+ * existing-point list are rebuilt when next needed.  A kernel that clears a
+ * mask byte must also store the properties' backgrounds at that point (the
+ * C++ header's device remove does). */
+int sgb_existence_changed(sgb_grid* g);
+
 /* setBackgroundValue<p> (SparseGridGpu.hpp:2878-2884); value host. */
 int sgb_set_background(sgb_grid* g, int prop, const void* value_host);
 

@@ -44,6 +44,7 @@ SIGNATURES = {
     "sgb_existing_point_list": (_i32, [_vp, _vp, _vp, _vp]),
     "sgb_set_linearizer": (_i32, [_vp, _i32]),
     "sgb_release_scratch": (_i32, [_vp]),
+    "sgb_existence_changed": (_i32, [_vp]),
     "sgb_probe_bounded_waits": (_i32, [_i64, _i32, _vp]),
     "sgb_construct_link_dw": (_i32, [_vp, _vp, _vp, _vp, _vp]),
     "sgb_construct_link_up": (_i32, [_vp, _vp, _vp, _vp, _vp]),

@@ -440,6 +440,13 @@ int sgb_destroy(sgb_grid* g) {
     return SGB_OK;
 }
 
+int sgb_existence_changed(sgb_grid* g) {
+    if (!g) return SGB_EINVAL;
+    g->bits_valid = false;
+    g->epts_valid = false;
+    return SGB_OK;
+}
+
 int sgb_release_scratch(sgb_grid* g) {
     if (!g) return SGB_EINVAL;
     cudaSetDevice(g->device);

@@ -130,6 +130,15 @@ static void insert_via_abi(sgb_grid* g) {
     cudaFree(dv);
 }
 
+// remove<>(coord) from a device kernel: the points of the shape with an even coordinate sum
+// (SparseGridGpu_testKernels.cuh:318-357 removeSphere3D_even_radiusV)
+template <typename Ker>
+__global__ void remove_even(Ker g) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y,
+              z = blockIdx.z * blockDim.z + threadIdx.z;
+    if (in_shape(x, y, z) && (x + y + z) % 2 == 0) g.remove(grid_key_dx<3, int>({x, y, z}));
+}
+
 int main() {
     const size_t sz[3] = {N, N, N};
     gpu::ofp_context_t ctx;
@@ -440,6 +449,59 @@ int main() {
         cudaDeviceSynchronize();
         CHECK(sw && grid.countExistingElements() == na && grid.private_get_neighborhood_array() != nullptr,
               "swap_removeUnusedBuffers");
+    }
+
+    // ---------------------------------------------------------------- device remove
+    {
+        // remove from a kernel, then the heat stencil: equal to a grid that never had those points
+        Grid6 rg(sz), og(sz);
+        rg.setBackgroundValue<0>(0.25f);
+        og.setBackgroundValue<0>(0.25f);
+        rg.setGPUInsertBuffer(dim3(N / 8, N / 8, N / 8), dim3(1024, 1, 1));
+        insert_shape<0><<<dim3(N / 8, N / 8, N / 8), dim3(8, 8, 8)>>>(rg.toKernel());
+        rg.flush<smax_<0>>(ctx, FLUSH_ON_DEVICE);
+        remove_even<<<dim3(N / 8, N / 8, N / 8), dim3(8, 8, 8)>>>(rg.toKernel());
+        std::vector<int32_t> oc;
+        std::vector<float> ov;
+        size_t odd = 0;
+        for (int z = 0; z < N; ++z)
+            for (int y = 0; y < N; ++y)
+                for (int x = 0; x < N; ++x)
+                    if (in_shape(x, y, z) && (x + y + z) % 2 == 1) {
+                        oc.insert(oc.end(), {x, y, z});
+                        ov.push_back(val_a(x, y, z));
+                        ++odd;
+                    }
+        int32_t* dc;
+        float* dv;
+        cudaMalloc(&dc, oc.size() * 4);
+        cudaMalloc(&dv, ov.size() * 4);
+        cudaMemcpy(dc, oc.data(), oc.size() * 4, cudaMemcpyHostToDevice);
+        cudaMemcpy(dv, ov.data(), ov.size() * 4, cudaMemcpyHostToDevice);
+        const void* vals[6] = {dv, nullptr, nullptr, nullptr, nullptr, nullptr};
+        check(sgb_insert(og.handle(), (int64_t)odd, dc, vals, nullptr), "sgb_insert");
+        int ops[6] = {SGB_OP_MAX, SGB_OP_NONE, SGB_OP_NONE, SGB_OP_NONE, SGB_OP_NONE, SGB_OP_NONE};
+        check(sgb_flush(og.handle(), ops, nullptr), "sgb_flush");
+        cudaDeviceSynchronize();
+        cudaFree(dc);
+        cudaFree(dv);
+        const bool cnt_ok = rg.countExistingElements() == odd && og.countExistingElements() == odd;
+        rg.tagBoundaries<NNStar<3>>(ctx);
+        og.tagBoundaries<NNStar<3>>(ctx);
+        rg.applyStencils<HeatStencil<3, 0, 1>>(rg.getBox(), STENCIL_MODE_INPLACE, 0.1f);
+        og.applyStencils<HeatStencil<3, 0, 1>>(og.getBox(), STENCIL_MODE_INPLACE, 0.1f);
+        cudaDeviceSynchronize();
+        rg.deviceToHost<0, 1>();
+        og.deviceToHost<0, 1>();
+        bool eq = cnt_ok && rg.countBoundaryElements() == og.countBoundaryElements();
+        for (int z = 0; z < N && eq; ++z)
+            for (int y = 0; y < N; ++y)
+                for (int x = 0; x < N; ++x) {
+                    const grid_key_dx<3, int> k({x, y, z});
+                    const float a = rg.get<1>(k), b = og.get<1>(k);
+                    eq = eq && std::memcmp(&a, &b, 4) == 0;
+                }
+        CHECK(eq, "device_remove_then_heat");
     }
 
     // ---------------------------------------------------------------- SparseGridGpu_z (Morton chunk ids)
