@@ -77,6 +77,10 @@ __global__ void __launch_bounds__(kThreads8, KIND == SGB_GS7 ? 6 : 8)
                   const GridInfo* __restrict__ grids, GridInfo g0, int64_t n, Geometry geo, StencilParams prm,
                   int64_t t, int R, int64_t nwarps, unsigned* err) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
+    // Programmatic dependent launch: the next step's launch may begin while this one drains; no
+    // field is read or written before the previous launch on the stream has completed.
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    asm volatile("griddepcontrol.wait;" ::: "memory");
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     Stage8<NP>* ring = reinterpret_cast<Stage8<NP>*>(smem_raw) + (size_t)warp * R;
     uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + (size_t)kWarps * R * sizeof(Stage8<NP>)) + warp * R;
@@ -374,9 +378,19 @@ static int launch_kind(const LaunchDesc& L, cudaStream_t s) {
     const unsigned blocks = (unsigned)((nwarps + kWarps - 1) / kWarps);
     auto kern = k_stencil7_e8<KIND, NP, BOX>;
     SGB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    kern<<<blocks, kThreads8, smem, s>>>(L.fs, L.mask, L.nn, L.keys, L.gid, L.grids, L.g0, L.n, L.geo, L.prm, L.t, R,
-                                         nwarps, L.err);
-    SGB_CUDA(cudaGetLastError());
+    // consecutive steps overlap one launch's ramp-up with the previous one's tail
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(blocks);
+    cfg.blockDim = dim3(kThreads8);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    SGB_CUDA(cudaLaunchKernelEx(&cfg, kern, L.fs, L.mask, L.nn, L.keys, L.gid, L.grids, L.g0, L.n, L.geo, L.prm, L.t, R,
+                                nwarps, L.err));
     return SGB_OK;
 }
 
