@@ -174,9 +174,9 @@ def _peak_hbm():
         return 6650.0, "fallback"
 
 
-def _profile_traffic():
-    """DRAM bytes per launch of the stencil kernel from the committed ncu summary."""
-    p = os.path.join(ROOT, "profiles", "stencil7_gs7_512.md")
+def _profile_traffic(name="stencil7_gs7_512.md"):
+    """DRAM bytes per launch of a kernel from its committed ncu summary under profiles/."""
+    p = os.path.join(ROOT, "profiles", name)
     try:
         m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", open(p).read())
         return float(m.group(1)) if m else None
@@ -847,8 +847,9 @@ def run_conv1000(args, dist: Dist):
     head = res["smb_shared"]
     t_one = head["us_per_application"] / 1e6
     ach = 9 * nelem / t_one / 1e9
-    roof = {"bound": "hbm", "kernel": "k_stencil_tile<BOX27,8> (Conv3x3x3, one CTA per chunk)",
-            "achieved": round(ach, 1), "peak": peak, "unit": "GB/s", "frac": round(ach / peak, 4), "traffic": None,
+    roof = {"bound": "hbm", "kernel": "k_box27_e8 (Conv3x3x3, one warp per chunk)",
+            "achieved": round(ach, 1), "peak": peak, "unit": "GB/s", "frac": round(ach / peak, 4),
+            "traffic": _profile_traffic("box27_e8_conv1000.md"),
             "peak_kind": pk, "alg_bytes_per_launch": 9 * nelem}
     cpu = None
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
@@ -867,7 +868,7 @@ def run_conv1000(args, dist: Dist):
                  {"workload": "conv3x3x3_1000^3_shell_r56_r128_chunk8", "elements": nelem, "chunks": nchunks,
                   "variants": res, "l2": "256 MiB L2-flushing write before every timed application "
                                          "(the grid fits in L2); events around each application"},
-                 roofline=roof, cpu_baseline=cpu, e2e=None, gpu_launches=None, clocks=clk)
+                 roofline=roof, cpu_baseline=cpu, e2e=None, gpu_launches=nsteps, clocks=clk)
 
 
 def run_reference(args, dist: Dist):

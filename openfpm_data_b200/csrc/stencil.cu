@@ -127,99 +127,130 @@ __global__ void __launch_bounds__(256) k_stencil_tile(FieldSet fs, const uint8_t
 }
 
 // ------------------------------------------------------------------ Conv3x3x3 on 8^3 chunks
-// One chunk at a time per 64-thread CTA (grid-stride), software-pipelined:
-// while chunk i is computed from one 10^3 shared tile, the tile of chunk
-// i + 1 is being filled in the other by cp.async copies (16-byte copies of
-// the chunk's rows, 4-byte copies of the six faces, twelve edges and eight
-// corners from the 26 NNFull neighbours; an absent neighbour's cells get the
-// background with plain stores) and the chunk's mask bytes alongside.  Tile
-// cell (x, y, z), x, y, z in 0..9, sits at z * 240 + y * 24 + x + 3: rows of
-// 24 floats put the chunk's part of every row on a 16-byte boundary, and the
-// four rows a warp reads at once fall into disjoint banks.  The neighbour rows are read two chunks
-// ahead.  Thread t owns the column (x, y) = (t % 8, t / 8) and marches z
-// holding the 3 x 3 x 3 window in registers: per point 9 shared loads and
-// the 27 FMAs in Conv3x3x3's order (x offset outermost, z innermost).
-// Results equal the tile kernel's bit for bit (the background invariant
-// makes a stored non-existing point read the same as the substituted
-// background).
-constexpr int kB27Plane = 240, kB27Row = 24, kB27Tile = 10 * kB27Plane;
+// One warp per chunk at a time (grid-stride over chunks, four independent warps per CTA, no CTA
+// barriers), software-pipelined: while chunk i is computed from one 10^3 shared tile, cp.async
+// copies fill the warp's other tile with chunk i + 1 (16-byte copies of the chunk's rows, of the z
+// and y faces and of the four edges along x; 4-byte copies of the x faces, the other eight edges
+// and the corners, from the 26 NNFull neighbours; an absent neighbour's cells get the background
+// with plain stores) and its mask bytes.  Tile cell (x, y, z), x, y, z in 0..9, sits at
+// z * 120 + y * 12 + x + 3: rows of 12 floats put the chunk's part of every row on a 16-byte
+// boundary and spread eight consecutive rows over all 32 banks.
+// Lane l owns the x quad q = l % 2 (chunk x = 4q .. 4q + 3) of row y (lanes 0..7 of each half
+// take the even rows, 8..15 the odd ones, so the 16-byte row loads of a quarter warp hit
+// distinct banks) and the z half l / 16 (z = 0..3 or 4..7).  It marches z holding a 3 x 3 x 6
+// window in registers (each row: one 16-byte load, the halo cell, and the partner quad's edge
+// cell by a shuffle) and runs the 27 FMAs of each of its four points in Conv3x3x3's order (x
+// offset outermost, z innermost), four independent chains.  Results equal the tile kernel's bit
+// for bit (the background invariant makes a stored non-existing point read the same as the
+// substituted background).
+constexpr int kW27Row = 12, kW27Plane = 120, kW27Tile = 1204, kW27Warps = 4;
 
-__device__ __forceinline__ void box27_fill(float* tile, uint8_t* mt, const int32_t* nb, const float* __restrict__ src,
-                                           const uint8_t* __restrict__ mask, int64_t c, float bck, int t) {
-    if (t < 32) cp_async16(mt + t * 16, mask + c * 512 + t * 16);
-    // interior: row (y, z) = (t % 8, t / 8), two 16-byte copies
-    {
-        const float* row = src + c * 512 + t * 8;
-        float* d = &tile[((t >> 3) + 1) * kB27Plane + ((t & 7) + 1) * kB27Row + 4];
-        cp_async16(d, row);
-        cp_async16(d + 4, row + 4);
+struct W27Stage {
+    float tile[2][kW27Tile];
+    uint8_t mt[2][512];
+};
+
+// Fill one tile with chunk c (warp-wide; lane l < 27 holds NNFull slot l of chunk c in nbr).
+__device__ __noinline__ void w27_fill(float* T, uint8_t* mt, int32_t nbr, const float* __restrict__ src,
+                                         const uint8_t* __restrict__ mask, int64_t c, float bck, int l) {
+    constexpr unsigned kAll = 0xffffffffu;
+    cp_async16(mt + l * 16, mask + c * 512 + l * 16);
+    // the chunk's rows: 128 pieces of 16 bytes, piece p = (x half, y, z)
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int p = l + 32 * k, h = p & 1, y = (p >> 1) & 7, z = p >> 4;
+        cp_async16(T + (z + 1) * kW27Plane + (y + 1) * kW27Row + 4 + 4 * h, src + c * 512 + p * 4);
     }
-    const int u = t & 7, v = t >> 3;
-    auto cell = [&](int ti, int32_t sc, int64_t off) {
-        if (sc >= 0) cp_async4(&tile[ti], src + (int64_t)sc * 512 + off);
-        else tile[ti] = bck;
+    auto piece = [&](float* d, int32_t nb, int off) {
+        if (nb >= 0) cp_async16(d, src + (int64_t)nb * 512 + off);
+        else *reinterpret_cast<float4*>(d) = make_float4(bck, bck, bck, bck);
     };
-    // faces: cell (u, v) of each; slot = px + 3 py + 9 pz
-    auto at = [](int x, int y, int z) { return z * kB27Plane + y * kB27Row + x + 3; };
-    cell(at(0, u + 1, v + 1), nb[12], v * 64 + u * 8 + 7);
-    cell(at(9, u + 1, v + 1), nb[14], v * 64 + u * 8 + 0);
-    cell(at(u + 1, 0, v + 1), nb[10], v * 64 + 7 * 8 + u);
-    cell(at(u + 1, 9, v + 1), nb[16], v * 64 + 0 * 8 + u);
-    cell(at(u + 1, v + 1, 0), nb[4], 7 * 64 + v * 8 + u);
-    cell(at(u + 1, v + 1, 9), nb[22], 0 * 64 + v * 8 + u);
-    // edges (12 x 8 cells) and corners (8)
-    for (int e = t; e < 104; e += 64) {
-        int tx, ty, tz;
-        if (e < 96) {
-            const int k = e >> 3, w = (e & 7) + 1;  // edge k, position w along it
-            const int a = (k & 1) ? 9 : 0, b = (k & 2) ? 9 : 0;
-            if (k < 4) { tx = w; ty = a; tz = b; }          // edges along x
-            else if (k < 8) { tx = a; ty = w; tz = b; }     // along y
-            else { tx = a; ty = b; tz = w; }                // along z
-        } else {
-            const int k = e - 96;
-            tx = (k & 1) ? 9 : 0;
-            ty = (k & 2) ? 9 : 0;
-            tz = (k & 4) ? 9 : 0;
+    auto cell = [&](float* d, int32_t nb, int off) {
+        if (nb >= 0) cp_async4(d, src + (int64_t)nb * 512 + off);
+        else *d = bck;
+    };
+    // z faces and y faces: lanes 0..15 the lower side, 16..31 the upper, one 16-byte piece each
+    {
+        const int f = l >> 4, h = l & 1, a = (l >> 1) & 7;
+        const int32_t nz = __shfl_sync(kAll, nbr, f ? 22 : 4);
+        const int32_t ny = __shfl_sync(kAll, nbr, f ? 16 : 10);
+        piece(T + (f ? 9 : 0) * kW27Plane + (a + 1) * kW27Row + 4 + 4 * h, nz, (f ? 0 : 7) * 64 + a * 8 + 4 * h);
+        piece(T + (a + 1) * kW27Plane + (f ? 9 : 0) * kW27Row + 4 + 4 * h, ny, a * 64 + (f ? 0 : 7) * 8 + 4 * h);
+    }
+    // x faces: 128 cells, four per lane; odd lanes take the upper face so that one copy
+    // instruction writes two bank residues
+    {
+        const int f = l & 1;
+        const int32_t nx = __shfl_sync(kAll, nbr, f ? 14 : 12);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int e = (l >> 1) + 16 * k, y = e & 7, z = e >> 3;
+            cell(T + (z + 1) * kW27Plane + (y + 1) * kW27Row + (f ? 12 : 3), nx, z * 64 + y * 8 + (f ? 0 : 7));
         }
-        const int px = tx == 0 ? 0 : (tx == 9 ? 2 : 1), py = ty == 0 ? 0 : (ty == 9 ? 2 : 1),
-                  pz = tz == 0 ? 0 : (tz == 9 ? 2 : 1);
-        const int lx = (tx + 7) & 7, ly = (ty + 7) & 7, lz = (tz + 7) & 7;
-        cell(at(tx, ty, tz), nb[px + 3 * py + 9 * pz], lz * 64 + ly * 8 + lx);
+    }
+    // edges along y (k = 0) and along z (k = 1): x side s & 1, other side s >> 1, position w
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        const int w = l & 7, s = l >> 3, sx = s & 1, so = s >> 1;
+        const int lx = sx ? 0 : 7, lo = so ? 0 : 7;
+        int slot, ty, tz, off;
+        if (k == 0) {
+            slot = (sx ? 2 : 0) + 3 + 9 * (so ? 2 : 0);
+            ty = w + 1;
+            tz = so ? 9 : 0;
+            off = lo * 64 + w * 8 + lx;
+        } else {
+            slot = (sx ? 2 : 0) + 3 * (so ? 2 : 0) + 9;
+            ty = so ? 9 : 0;
+            tz = w + 1;
+            off = w * 64 + lo * 8 + lx;
+        }
+        const int32_t nb = __shfl_sync(kAll, nbr, slot);
+        cell(T + tz * kW27Plane + ty * kW27Row + (sx ? 12 : 3), nb, off);
+    }
+    // edges along x (lanes 0..7, two 16-byte pieces each) and the corners (lanes 8..15)
+    {
+        const int k = (l >> 1) & 3, h = l & 1, sy = k & 1, sz = k >> 1;
+        const int32_t ne = __shfl_sync(kAll, nbr, 1 + 3 * (sy ? 2 : 0) + 9 * (sz ? 2 : 0));
+        const int r = l & 7, rx = r & 1, ry = (r >> 1) & 1, rz = r >> 2;
+        const int32_t nc = __shfl_sync(kAll, nbr, (rx ? 2 : 0) + 3 * (ry ? 2 : 0) + 9 * (rz ? 2 : 0));
+        if (l < 8)
+            piece(T + (sz ? 9 : 0) * kW27Plane + (sy ? 9 : 0) * kW27Row + 4 + 4 * h, ne,
+                  (sz ? 0 : 7) * 64 + (sy ? 0 : 7) * 8 + 4 * h);
+        else if (l < 16)
+            cell(T + (rz ? 9 : 0) * kW27Plane + (ry ? 9 : 0) * kW27Row + (rx ? 12 : 3), nc,
+                 (rz ? 0 : 7) * 64 + (ry ? 0 : 7) * 8 + (rx ? 0 : 7));
     }
 }
 
-__global__ void __launch_bounds__(64, 10) k_box27_e8(const float* __restrict__ src, float* __restrict__ dst,
-                                                 const uint8_t* __restrict__ mask, const int32_t* __restrict__ nn,
-                                                 const int64_t* __restrict__ keys, int64_t n, Geometry geo,
-                                                 StencilParams prm, float bck) {
-    __shared__ __align__(16) float tile[2][kB27Tile];
-    __shared__ __align__(16) uint8_t mt[2][512];
-    __shared__ int32_t nbs[2][28];
-    const int t = threadIdx.x;
-    const int cx = t & 7, cy = t >> 3;
-    const int64_t stride = gridDim.x;
-    int64_t c = blockIdx.x;
-    if (c >= n) return;
-    // neighbour rows: of the first chunk now, of the second in a register
-    if (t < 27) nbs[0][t] = t == 13 ? (int32_t)c : nn[c * 27 + t];
-    int32_t nb_next = -1;
-    if (t < 27 && c + stride < n) nb_next = t == 13 ? (int32_t)(c + stride) : nn[(c + stride) * 27 + t];
-    __syncthreads();
-    box27_fill(tile[0], mt[0], nbs[0], src, mask, c, bck, t);
+__global__ void __launch_bounds__(32 * kW27Warps, 4) k_box27_e8(const float* __restrict__ src, float* __restrict__ dst,
+                                                              const uint8_t* __restrict__ mask,
+                                                              const int32_t* __restrict__ nn,
+                                                              const int64_t* __restrict__ keys, int64_t n,
+                                                              Geometry geo, StencilParams prm, float bck) {
+    __shared__ __align__(16) W27Stage stage[kW27Warps];
+    constexpr unsigned kAll = 0xffffffffu;
+    const int warp = threadIdx.x >> 5, l = threadIdx.x & 31;
+    W27Stage& S = stage[warp];
+    const int64_t stride = (int64_t)gridDim.x * kW27Warps;
+    int64_t c = (int64_t)blockIdx.x * kW27Warps + warp;
+    if (c >= n) return;  // whole warp
+    int32_t nbr = l < 27 ? nn[c * 27 + l] : -1;
+    w27_fill(S.tile[0], S.mt[0], nbr, src, mask, c, bck, l);
     cp_async_commit();
+    nbr = (l < 27 && c + stride < n) ? nn[(c + stride) * 27 + l] : -1;
+    const int q = l & 1, j = (l >> 1) & 7, z0 = (l >> 4) * 4;
+    const int y = ((j & 3) << 1) | (j >> 2);
+    const int hoff = q ? 12 : 3;
     for (int it = 0; c < n; ++it, c += stride) {
-        const int cur = it & 1, nxt = cur ^ 1;
+        const int cur = it & 1;
         const int64_t c1 = c + stride;
-        // the next chunk's neighbour row to shared memory, the one after it to a register
-        if (t < 27) nbs[nxt][t] = nb_next;
-        if (t < 27 && c1 + stride < n) nb_next = t == 13 ? (int32_t)(c1 + stride) : nn[(c1 + stride) * 27 + t];
-        __syncthreads();  // nbs[nxt] visible; every thread is done with tile[nxt] (chunk it - 1)
-        if (c1 < n) box27_fill(tile[nxt], mt[nxt], nbs[nxt], src, mask, c1, bck, t);
+        if (c1 < n) w27_fill(S.tile[cur ^ 1], S.mt[cur ^ 1], nbr, src, mask, c1, bck, l);
         cp_async_commit();
-        cp_async_wait_group<1>();  // this thread's copies of chunk c have landed
-        __syncthreads();           // and everyone's
-        const float* T0 = tile[cur];
+        nbr = (l < 27 && c1 + stride < n) ? nn[(c1 + stride) * 27 + l] : -1;
+        cp_async_wait_group<1>();  // this lane's copies of chunk c have landed
+        __syncwarp();              // and every lane's
+        const float* T = S.tile[cur];
         int64_t ox = 0, oy = 0, oz = 0;
         if (prm.has_box) {
             int64_t o[3];
@@ -228,26 +259,29 @@ __global__ void __launch_bounds__(64, 10) k_box27_e8(const float* __restrict__ s
             oy = o[1];
             oz = o[2];
         }
-        // window w[a][b][d] = tile[z + d][y + b][x + a] (a, b in 0..2, d in 0..3, tile coordinates):
-        // two points (z, z + 1) per step, their two FMA chains interleaved
-        float w[3][3][4];
-#pragma unroll
-        for (int a = 0; a < 3; ++a)
+        // win[p][b][e] = tile cell (4q + e, y + b, plane p of the rolling window)
+        float win[3][3][6];
+        auto load_plane = [&](int tp, float(&pl)[3][6]) {
 #pragma unroll
             for (int b = 0; b < 3; ++b) {
-                w[a][b][0] = T0[0 * kB27Plane + (cy + b) * kB27Row + (cx + a) + 3];
-                w[a][b][1] = T0[1 * kB27Plane + (cy + b) * kB27Row + (cx + a) + 3];
+                const float* rb = T + tp * kW27Plane + (y + b) * kW27Row;
+                const float4 v = *reinterpret_cast<const float4*>(rb + 4 + 4 * q);
+                const float hv = rb[hoff];
+                const float got = __shfl_xor_sync(kAll, q ? v.x : v.w, 1);
+                pl[b][0] = q ? got : hv;
+                pl[b][1] = v.x;
+                pl[b][2] = v.y;
+                pl[b][3] = v.z;
+                pl[b][4] = v.w;
+                pl[b][5] = q ? hv : got;
             }
+        };
+        load_plane(z0, win[0]);
+        load_plane(z0 + 1, win[1]);
 #pragma unroll
-        for (int z = 0; z < 8; z += 2) {
-#pragma unroll
-            for (int a = 0; a < 3; ++a)
-#pragma unroll
-                for (int b = 0; b < 3; ++b) {
-                    w[a][b][2] = T0[(z + 2) * kB27Plane + (cy + b) * kB27Row + (cx + a) + 3];
-                    w[a][b][3] = T0[(z + 3) * kB27Plane + (cy + b) * kB27Row + (cx + a) + 3];
-                }
-            float tot0 = 0.0f, tot1 = 0.0f;
+        for (int zz = 0; zz < 4; ++zz) {
+            load_plane(z0 + zz + 2, win[(zz + 2) % 3]);
+            float acc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
 #pragma unroll
             for (int a = 0; a < 3; ++a)
 #pragma unroll
@@ -255,25 +289,24 @@ __global__ void __launch_bounds__(64, 10) k_box27_e8(const float* __restrict__ s
 #pragma unroll
                     for (int d = 0; d < 3; ++d) {
                         const float cf = prm.coeff[a * 9 + b * 3 + d];
-                        tot0 = __fmaf_rn(w[a][b][d], cf, tot0);
-                        tot1 = __fmaf_rn(w[a][b][d + 1], cf, tot1);
+#pragma unroll
+                        for (int i = 0; i < 4; ++i) acc[i] = __fmaf_rn(win[(zz + d) % 3][b][i + a], cf, acc[i]);
                     }
+            const int z = z0 + zz, po = z * 64 + y * 8 + 4 * q;
+            const uint32_t m4 = *reinterpret_cast<const uint32_t*>(S.mt[cur] + po);
+            float* d = dst + c * 512 + po;
+            if (!prm.has_box && (m4 & 0x03030303u) == 0x01010101u) {
+                *reinterpret_cast<float4*>(d) = make_float4(acc[0], acc[1], acc[2], acc[3]);
+            } else {
 #pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const int zz = z + h;
-                const uint8_t m = mt[cur][zz * 64 + cy * 8 + cx];
-                bool act = (m & 3) == 1;
-                if (prm.has_box) act = act && in_box(prm, ox + cx, oy + cy, oz + zz);
-                if (act) dst[c * 512 + zz * 64 + cy * 8 + cx] = h ? tot1 : tot0;
-            }
-#pragma unroll
-            for (int a = 0; a < 3; ++a)
-#pragma unroll
-                for (int b = 0; b < 3; ++b) {
-                    w[a][b][0] = w[a][b][2];
-                    w[a][b][1] = w[a][b][3];
+                for (int i = 0; i < 4; ++i) {
+                    bool act = ((m4 >> (8 * i)) & 3u) == 1u;
+                    if (prm.has_box) act = act && in_box(prm, ox + 4 * q + i, oy + y, oz + z);
+                    if (act) d[i] = acc[i];
                 }
+            }
         }
+        __syncwarp();  // every lane is done with tile[cur] before it is refilled
     }
     cp_async_wait_all();
 }
@@ -493,9 +526,10 @@ int launch_fields(const LaunchDesc& L, cudaStream_t s) {
     // x neighbours only under the x-fastest chunk ids
     if (L.kind != SGB_BOX27 && L.edge == 8 && !L.use_tile && !L.geo.zorder) return launch_e8(L, s);
     if (L.kind == SGB_BOX27 && L.edge == 8 && !L.use_tile && !L.grids) {
-        // 10 CTAs of 64 threads per SM are resident (20 KB of shared memory each)
-        const unsigned nb = (unsigned)std::max<int64_t>(1, std::min<int64_t>(L.n, (int64_t)L.num_sms * 10));
-        k_box27_e8<<<nb, 64, 0, s>>>(L.fs.in[0][0], L.fs.out[0][0], L.mask, L.nn, L.keys, L.n, L.geo, L.prm,
+        // 4 CTAs of four warps per SM are resident (128 registers a thread)
+        const int64_t want = (L.n + kW27Warps - 1) / kW27Warps;
+        const unsigned nb = (unsigned)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)L.num_sms * 4));
+        k_box27_e8<<<nb, 32 * kW27Warps, 0, s>>>(L.fs.in[0][0], L.fs.out[0][0], L.mask, L.nn, L.keys, L.n, L.geo, L.prm,
                                       L.g0.bck[0][0]);
         SGB_CUDA(cudaGetLastError());
         return SGB_OK;
