@@ -481,6 +481,7 @@ extern "C" int sgb_flush(sgb_grid* g, const int* ops, sgb_stream stream) {
     else st = flush_impl<uint64_t>(g, ops, bits, s);
     g->npend = 0;
     g->nn_valid[0] = g->nn_valid[1] = false;
+    g->nnhash_ok = false;
     g->bits_valid = false;
     g->epts_valid = false;
     return st;

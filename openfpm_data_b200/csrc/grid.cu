@@ -142,6 +142,7 @@ int grid_reserve(sgb_grid* g, int64_t chunks, bool keep) {
 
 static void invalidate_derived(sgb_grid* g) {
     g->nn_valid[0] = g->nn_valid[1] = false;
+    g->nnhash_ok = false;
     g->bits_valid = false;
     g->epts_valid = false;
 }
@@ -424,6 +425,7 @@ int sgb_destroy(sgb_grid* g) {
     g->pend_lin.release();
     g->nn[0].release();
     g->nn[1].release();
+    g->nnhash.release();
     g->bits.release();
     g->epts.release();
     for (auto& L : g->links) {
@@ -462,6 +464,8 @@ int sgb_release_scratch(sgb_grid* g) {
     g->bits_valid = false;
     g->epts.release();
     g->epts_valid = false;
+    g->nnhash.release();
+    g->nnhash_ok = false;
     for (auto& b : g->scratch) b.release();
     return SGB_OK;
 }
@@ -557,6 +561,7 @@ int sgb_set_linearizer(sgb_grid* g, int kind) {
     }
     g->geo.zorder = kind == SGB_LIN_ZMB;
     g->nn_valid[0] = g->nn_valid[1] = false;
+    g->nnhash_ok = false;
     return SGB_OK;
 }
 

@@ -103,6 +103,15 @@ __host__ __device__ inline void block_coords(const Geometry& g, int64_t key, int
         bc[2] = (int64_t)morton_compact3((uint64_t)key >> 2);
         return;
     }
+    if (key >= 0 && key <= 0xffffffffLL && g.bsz[0] <= 0xffffffffLL && g.bsz[1] <= 0xffffffffLL) {
+        // the same quotients in 32-bit arithmetic (a 64-bit division is several times dearer)
+        const uint32_t k = (uint32_t)key, b0 = (uint32_t)g.bsz[0], b1 = (uint32_t)g.bsz[1];
+        const uint32_t q = k / b0;
+        bc[0] = (int64_t)(k - q * b0);
+        bc[1] = (int64_t)(q % b1);
+        bc[2] = (int64_t)(q / b1);
+        return;
+    }
     bc[0] = key % g.bsz[0];
     bc[1] = (key / g.bsz[0]) % g.bsz[1];
     bc[2] = key / (g.bsz[0] * g.bsz[1]);
@@ -214,6 +223,8 @@ struct sgb_grid {
     // neighbour tables (int32, -1 = absent); index 0 NNStar (8/chunk), 1 NNFull (27/chunk)
     sgb::DevBuf nn[2];
     bool nn_valid[2] = {false, false};
+    sgb::DevBuf nnhash;   // open-addressing hash of the chunk keys used by the neighbour search
+    bool nnhash_ok = false;  // built for the current keys (any key change invalidates both nn tables)
     sgb::DevBuf bits;     // uint64 existence bitmaps, bs/64 words per chunk
     bool bits_valid = false;
     // existing-point list (e_points): uint32 chunk position * bs + offset

@@ -35,8 +35,9 @@ __device__ __forceinline__ int64_t block_lin_ref(const Geometry& geo, const int6
 // dx+3dy+9dz over {0,1,2}).  Output: data position, -1 when absent.
 //
 // The keys are distinct sorted integers, so the key bl of a neighbour lies
-// within |bl - key| positions of the chunk's own: the search is limited to
-// that window (one probe for an x neighbour under x-fastest ids).
+// within |bl - key| positions of the chunk's own: a near key (an x neighbour
+// under x-fastest ids) is searched in that window, one or two probes of
+// neighbouring positions; a far one is looked up in a hash of the keys.
 __device__ __forceinline__ int64_t find_near(const int64_t* keys, int64_t n, int64_t i, int64_t key, int64_t bl) {
     int64_t lo, hi;
     if (bl > key) {
@@ -54,7 +55,55 @@ __device__ __forceinline__ int64_t find_near(const int64_t* keys, int64_t n, int
     return (lo < n && keys[lo] == bl) ? lo : -1;
 }
 
-__global__ void k_find_nn(const int64_t* keys, int64_t n, Geometry geo, int kind, int32_t* out) {
+// Open-addressing hash of the chunk keys: linear probing, Fibonacci hashing (the key times
+// 2^64 divided by the golden ratio, top bits), at most half full, so every probe sequence ends
+// at an empty slot (key -1) within a few steps.  A lookup costs one or two L2 reads where a
+// binary search for a y or z neighbour costs up to log2(n) dependent ones.
+struct KeyHash {
+    int64_t* keys;
+    int32_t* pos;
+    uint64_t mask;
+    int shift;
+};
+
+__device__ __forceinline__ uint64_t kh_slot(const KeyHash& h, int64_t key) {
+    return ((uint64_t)key * 0x9E3779B97F4A7C15ull) >> h.shift;
+}
+
+__global__ void k_kh_build(const int64_t* __restrict__ keys, int64_t n, KeyHash h) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int64_t key = keys[i];
+    uint64_t s = kh_slot(h, key);
+    for (uint64_t probe = 0; probe <= h.mask; ++probe) {  // keys are distinct: the first empty slot is ours
+        const unsigned long long prev =
+            atomicCAS(reinterpret_cast<unsigned long long*>(h.keys + s), ~0ull, (unsigned long long)key);
+        if (prev == ~0ull) {
+            h.pos[s] = (int32_t)i;
+            return;
+        }
+        s = (s + 1) & h.mask;
+    }
+}
+
+__device__ __forceinline__ int64_t kh_find(const KeyHash& h, int64_t key) {
+    uint64_t s = kh_slot(h, key);
+    for (uint64_t probe = 0; probe <= h.mask; ++probe) {
+        const int64_t k = h.keys[s];
+        if (k == key) return h.pos[s];
+        if (k == -1) return -1;
+        s = (s + 1) & h.mask;
+    }
+    return -1;
+}
+
+__device__ __forceinline__ int64_t locate(const int64_t* keys, int64_t n, int64_t i, int64_t key, int64_t bl,
+                                          const KeyHash& h) {
+    const int64_t d = bl > key ? bl - key : key - bl;
+    return d <= 4 ? find_near(keys, n, i, key, bl) : kh_find(h, bl);
+}
+
+__global__ void k_find_nn(const int64_t* keys, int64_t n, Geometry geo, int kind, KeyHash h, int32_t* out) {
     const int nnn = kind == SGB_NN_STAR ? 8 : 27;
     const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     const int64_t chunk = t / nnn;
@@ -71,7 +120,7 @@ __global__ void k_find_nn(const int64_t* keys, int64_t n, Geometry geo, int kind
             if (dpos >= 0) {
                 bc[d] = dpos;
                 const int64_t bl = block_lin_ref(geo, bc);
-                if (bl >= 0 && bl != key) pos = find_near(keys, n, chunk, key, bl);
+                if (bl >= 0 && bl != key) pos = locate(keys, n, chunk, key, bl, h);
                 else if (bl == key) pos = chunk;
             }
         }
@@ -82,7 +131,7 @@ __global__ void k_find_nn(const int64_t* keys, int64_t n, Geometry geo, int kind
             cnt /= 3;
         }
         const int64_t bl = block_lin_ref(geo, bc);
-        if (bl >= 0 && bl != key) pos = find_near(keys, n, chunk, key, bl);
+        if (bl >= 0 && bl != key) pos = locate(keys, n, chunk, key, bl, h);
         else if (bl == key) pos = chunk;
     }
     out[t] = (int32_t)pos;
@@ -204,8 +253,22 @@ int ensure_neighbours(sgb_grid* g, int nn, cudaStream_t s) {
     const int nnn = nn == SGB_NN_STAR ? 8 : 27;
     SGB_TRY(g->nn[nn].grow((size_t)(g->n + 1) * nnn * 4));
     if (g->n > 0) {
+        int b = 10;
+        while ((int64_t(1) << b) < 2 * g->n) ++b;
+        const int64_t cap = int64_t(1) << b;
+        // the other table valid means the keys are those the hash was built from
+        const bool reuse = g->nnhash_ok && g->nn_valid[1 - nn] && g->nnhash.bytes >= (size_t)cap * 12;
+        SGB_TRY(g->nnhash.grow((size_t)cap * 12));
+        KeyHash h{g->nnhash.as<int64_t>(), reinterpret_cast<int32_t*>(g->nnhash.as<int64_t>() + cap),
+                  (uint64_t)cap - 1, 64 - b};
+        if (!reuse) {
+            SGB_CUDA(cudaMemsetAsync(h.keys, 0xff, (size_t)cap * 8, s));
+            k_kh_build<<<(unsigned)((g->n + 255) / 256), 256, 0, s>>>(g->keys.as<int64_t>(), g->n, h);
+            SGB_CUDA(cudaGetLastError());
+            g->nnhash_ok = true;
+        }
         const int64_t total = g->n * nnn;
-        k_find_nn<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(g->keys.as<int64_t>(), g->n, g->geo, nn,
+        k_find_nn<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(g->keys.as<int64_t>(), g->n, g->geo, nn, h,
                                                                    g->nn[nn].as<int32_t>());
         SGB_CUDA(cudaGetLastError());
     }

@@ -25,46 +25,53 @@ namespace sgb {
 
 // The list is read off the existence bitmaps (one bit per point, kept for
 // tagBoundaries): 64 bytes per 8^3 chunk instead of its 512 mask bytes.
-// Warp per chunk; lane l owns points [l * P, l * P + P) with P = bs / 32.
-__device__ __forceinline__ uint32_t lane_bits(const uint64_t* __restrict__ bits, int64_t c, int bs, int lane) {
-    const int P = bs >> 5, words = bs >> 6;
-    const int first = lane * P;
-    const uint64_t w = bits[c * words + (first >> 6)];
-    return (uint32_t)(w >> (first & 63)) & ((P == 32 ? 0u : (1u << P)) - 1u);
-}
-
+// Counting: one thread per chunk, the popcount of its bs / 64 words.
 __global__ void k_ep_count(const uint64_t* __restrict__ bits, int64_t n, int bs, uint32_t* counts) {
-    const int lane = threadIdx.x & 31;
-    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t c = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; c < n; c += nw) {
-        uint32_t t = __popc(lane_bits(bits, c, bs, lane));
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
-        if (lane == 0) counts[c] = t;
+    const int words = bs >> 6;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n; c += stride) {
+        uint32_t t = 0;
+        for (int k = 0; k < words; ++k) t += (uint32_t)__popcll(__ldg(bits + c * words + k));
+        counts[c] = t;
     }
 }
 
+// Emission: warp per chunk, the chunk's points in rounds of 32 (round r: points 32r .. 32r + 31,
+// lane l tests point 32r + l), so that each round's ids go out as one contiguous run; empty
+// rounds are skipped.  The next chunk's bitmap word and offset are loaded before the current
+// chunk is written out.
 __global__ void k_ep_emit(const uint64_t* __restrict__ bits, int64_t n, int bs, const uint32_t* __restrict__ offs,
                           uint32_t* out) {
+    constexpr unsigned kAll = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    const int P = bs >> 5;
-    for (int64_t c = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; c < n; c += nw) {
-        uint32_t m = lane_bits(bits, c, bs, lane);
-        const uint32_t cnt = __popc(m);
-        uint32_t pre = cnt;  // inclusive prefix over the lanes
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t v = __shfl_up_sync(0xffffffffu, pre, o);
-            if (lane >= o) pre += v;
+    const int words = bs >> 6, rounds = bs >> 5;
+    const uint32_t below = (1u << lane) - 1u;
+    int64_t c = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    uint64_t w = 0;
+    uint32_t pos = 0;
+    if (c < n) {
+        if (lane < words) w = __ldg(bits + c * words + lane);
+        pos = __ldg(offs + c);
+    }
+    for (; c < n; c += nw) {
+        const int64_t cn = c + nw;
+        uint64_t wn = 0;
+        uint32_t posn = 0;
+        if (cn < n) {
+            if (lane < words) wn = __ldg(bits + cn * words + lane);
+            posn = __ldg(offs + cn);
         }
-        uint32_t pos = offs[c] + pre - cnt;
-        const uint32_t base = (uint32_t)(c * bs) + (uint32_t)(lane * P);
-        while (m) {
-            const int b = __ffs(m) - 1;
-            out[pos++] = base + (uint32_t)b;
-            m &= m - 1;
+        const uint32_t base = (uint32_t)(c * bs) + (uint32_t)lane;
+        for (int r = 0; r < rounds; ++r) {
+            const uint64_t ww = __shfl_sync(kAll, w, r >> 1);
+            const uint32_t half = (uint32_t)(ww >> ((r & 1) << 5));
+            if (half == 0) continue;  // the same for every lane
+            if ((half >> lane) & 1u) out[pos + __popc(half & below)] = base + (uint32_t)(r << 5);
+            pos += (uint32_t)__popc(half);
         }
+        w = wn;
+        pos = posn;
     }
 }
 
@@ -83,7 +90,8 @@ int ensure_point_list(sgb_grid* g, cudaStream_t s) {
         uint32_t* offs = g->scratch[2].as<uint32_t>();
         const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>((int64_t)g->num_sms * 8, (n + 7) / 8));
         SGB_TRY(ensure_bits(g, s));
-        k_ep_count<<<blocks, 256, 0, s>>>(g->bits.as<uint64_t>(), n, (int)bs, counts);
+        const unsigned cblocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>((int64_t)g->num_sms * 16, (n + 255) / 256));
+        k_ep_count<<<cblocks, 256, 0, s>>>(g->bits.as<uint64_t>(), n, (int)bs, counts);
         SGB_CUDA(cudaGetLastError());
         SGB_TRY(scan_exclusive_u32(counts, offs, n, offs + n, &g->scratch[6], s));
         SGB_TRY(g->hscratch.ensure(64));
