@@ -19,14 +19,17 @@ __device__ __forceinline__ int64_t block_lin_ref(const Geometry& geo, const int6
         if (bc[0] < 0 || bc[1] < 0 || bc[2] < 0) return -1;
         return block_key(geo, bc[0], bc[1], bc[2]);
     }
-    int64_t lin = bc[geo.dim - 1];
-    if (lin >= geo.bsz[geo.dim - 1]) return -1;
-    for (int d = geo.dim - 2; d >= 0; --d) {
-        lin *= geo.bsz[d];
-        if (bc[d] >= geo.bsz[d]) return -1;
-        lin += bc[d];
+    // static indices only (a dynamic one would put the coordinates in local memory)
+    int64_t lin = 0;
+    bool past = false;
+#pragma unroll
+    for (int d = 2; d >= 0; --d) {
+        if (d < geo.dim) {
+            past |= bc[d] >= geo.bsz[d];
+            lin = lin * geo.bsz[d] + bc[d];
+        }
     }
-    return lin;
+    return past ? -1 : lin;
 }
 
 // findNeighbours (src/SparseGridGpu/SparseGridGpu_kernels.cuh:1014-1035) with
@@ -116,9 +119,14 @@ __global__ void k_find_nn(const int64_t* keys, int64_t n, Geometry geo, int kind
     if (kind == SGB_NN_STAR) {
         if (o < 2 * geo.dim) {
             const int d = o / 2;
-            const int64_t dpos = bc[d] + (o % 2) * 2 - 1;
+            int64_t dpos = 0;
+#pragma unroll
+            for (int e = 0; e < 3; ++e)
+                if (e == d) {
+                    dpos = bc[e] + (o % 2) * 2 - 1;
+                    bc[e] = dpos;
+                }
             if (dpos >= 0) {
-                bc[d] = dpos;
                 const int64_t bl = block_lin_ref(geo, bc);
                 if (bl >= 0 && bl != key) pos = locate(keys, n, chunk, key, bl, h);
                 else if (bl == key) pos = chunk;
@@ -126,8 +134,9 @@ __global__ void k_find_nn(const int64_t* keys, int64_t n, Geometry geo, int kind
         }
     } else if (o != nnn / 2) {
         int cnt = o;
-        for (int d = 0; d < geo.dim; ++d) {
-            bc[d] += cnt % 3 - 1;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            if (d < geo.dim) bc[d] += cnt % 3 - 1;
             cnt /= 3;
         }
         const int64_t bl = block_lin_ref(geo, bc);

@@ -36,41 +36,44 @@ __global__ void k_ep_count(const uint64_t* __restrict__ bits, int64_t n, int bs,
     }
 }
 
-// Emission: warp per chunk, the chunk's points in rounds of 32 (round r: points 32r .. 32r + 31,
-// lane l tests point 32r + l), so that each round's ids go out as one contiguous run; empty
-// rounds are skipped.  The next chunk's bitmap word and offset are loaded before the current
-// chunk is written out.
+// Emission: warp per chunk, lane l owns points [l * P, l * P + P) with P = bs / 32; a warp
+// scan of the lanes' counts places each lane's ids, written in point order.  The next chunk's
+// bitmap slice and offset are loaded before the current chunk is written out.
 __global__ void k_ep_emit(const uint64_t* __restrict__ bits, int64_t n, int bs, const uint32_t* __restrict__ offs,
                           uint32_t* out) {
     constexpr unsigned kAll = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    const int words = bs >> 6, rounds = bs >> 5;
-    const uint32_t below = (1u << lane) - 1u;
+    const int P = bs >> 5, words = bs >> 6;
+    const int first = lane * P, wi = first >> 6, sh = first & 63;
+    const uint32_t pmask = P >= 32 ? ~0u : (1u << P) - 1u;
     int64_t c = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-    uint64_t w = 0;
-    uint32_t pos = 0;
+    uint32_t m = 0, pos = 0;
     if (c < n) {
-        if (lane < words) w = __ldg(bits + c * words + lane);
+        m = (uint32_t)(__ldg(bits + c * words + wi) >> sh) & pmask;
         pos = __ldg(offs + c);
     }
     for (; c < n; c += nw) {
         const int64_t cn = c + nw;
-        uint64_t wn = 0;
-        uint32_t posn = 0;
+        uint32_t mn = 0, posn = 0;
         if (cn < n) {
-            if (lane < words) wn = __ldg(bits + cn * words + lane);
+            mn = (uint32_t)(__ldg(bits + cn * words + wi) >> sh) & pmask;
             posn = __ldg(offs + cn);
         }
-        const uint32_t base = (uint32_t)(c * bs) + (uint32_t)lane;
-        for (int r = 0; r < rounds; ++r) {
-            const uint64_t ww = __shfl_sync(kAll, w, r >> 1);
-            const uint32_t half = (uint32_t)(ww >> ((r & 1) << 5));
-            if (half == 0) continue;  // the same for every lane
-            if ((half >> lane) & 1u) out[pos + __popc(half & below)] = base + (uint32_t)(r << 5);
-            pos += (uint32_t)__popc(half);
+        const uint32_t cnt = __popc(m);
+        uint32_t pre = cnt;  // inclusive prefix over the lanes
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t v = __shfl_up_sync(kAll, pre, o);
+            if (lane >= o) pre += v;
         }
-        w = wn;
+        uint32_t p = pos + pre - cnt;
+        const uint32_t base = (uint32_t)(c * bs) + (uint32_t)first;
+        while (m) {
+            out[p++] = base + (uint32_t)(__ffs(m) - 1);
+            m &= m - 1;
+        }
+        m = mn;
         pos = posn;
     }
 }
