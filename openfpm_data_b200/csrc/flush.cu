@@ -48,15 +48,35 @@ __global__ void k_rs_hist(const K* keys, int64_t n, int shift, unsigned dmask, i
 // Stable scatter: items keep their order inside each digit.  Tile order is
 // (warp, round, lane) == index order; ranks inside a warp come from
 // __match_any_sync peer groups, counts across warps from a shared prefix.
+// The tile is then staged in shared memory in digit order and written out
+// run by run, so that consecutive threads store consecutive positions of a
+// digit's output range instead of one scattered 4-byte store per item.
+template <typename K>
+__host__ __device__ constexpr size_t rs_union_bytes() {
+    return (size_t)kRsWarps * kRsMaxBuckets * 4 > (size_t)kRsTile * (sizeof(K) + 4)
+               ? (size_t)kRsWarps * kRsMaxBuckets * 4
+               : (size_t)kRsTile * (sizeof(K) + 4);
+}
+template <typename K>
+__host__ __device__ constexpr size_t rs_scatter_smem() {
+    return rs_union_bytes<K>() + (size_t)kRsMaxBuckets * 4 + kRsWarps * 4;
+}
+
 template <typename K>
 __global__ void __launch_bounds__(kRsThreads) k_rs_scatter(const K* kin, const uint32_t* vin, K* kout, uint32_t* vout,
                                                             int64_t n, int shift, unsigned dmask, int nbuckets,
                                                             const uint32_t* offs, int ntiles) {
-    __shared__ uint32_t wcnt[kRsWarps][kRsMaxBuckets];
+    extern __shared__ __align__(16) unsigned char rs_smem[];
+    auto wcnt = reinterpret_cast<uint32_t(*)[kRsMaxBuckets]>(rs_smem);  // [kRsWarps][kRsMaxBuckets]
+    K* sk = reinterpret_cast<K*>(rs_smem);                              // the same bytes, once wcnt is done
+    uint32_t* sv = reinterpret_cast<uint32_t*>(rs_smem + (size_t)kRsTile * sizeof(K));
+    uint32_t* dstart = reinterpret_cast<uint32_t*>(rs_smem + rs_union_bytes<K>());
+    uint32_t* wsum = dstart + kRsMaxBuckets;
     for (int i = threadIdx.x; i < kRsWarps * kRsMaxBuckets; i += blockDim.x) (&wcnt[0][0])[i] = 0;
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int64_t base = (int64_t)blockIdx.x * kRsTile + warp * (32 * kRsRounds);
+    const int64_t tbase = (int64_t)blockIdx.x * kRsTile;
+    const int64_t base = tbase + warp * (32 * kRsRounds);
     K key[kRsRounds];
     uint32_t val[kRsRounds], rank[kRsRounds];
     const unsigned lt = lanemask_lt();
@@ -76,24 +96,63 @@ __global__ void __launch_bounds__(kRsThreads) k_rs_scatter(const K* kin, const u
         __syncwarp();
     }
     __syncthreads();
-    for (int d = threadIdx.x; d < nbuckets; d += blockDim.x) {
+    // per digit: the warps' counts become prefixes; thread t owns digits kPer t .. kPer t + kPer - 1
+    constexpr int kPer = kRsMaxBuckets / kRsThreads;
+    uint32_t tot[kPer], tsum = 0;
+#pragma unroll
+    for (int k = 0; k < kPer; ++k) {
+        const int d = threadIdx.x * kPer + k;
         uint32_t run = 0;
-        for (int w = 0; w < kRsWarps; ++w) {
-            uint32_t c = wcnt[w][d];
-            wcnt[w][d] = run;
-            run += c;
-        }
+        if (d < nbuckets)
+            for (int w = 0; w < kRsWarps; ++w) {
+                const uint32_t c = wcnt[w][d];
+                wcnt[w][d] = run;
+                run += c;
+            }
+        tot[k] = run;
+        tsum += run;
+    }
+    // the digits' first positions in the tile: an exclusive scan of the threads' sums
+    uint32_t incl = tsum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+    }
+    if (lane == 31) wsum[warp] = incl;
+    __syncthreads();
+    uint32_t run = incl - tsum;
+    for (int w = 0; w < warp; ++w) run += wsum[w];
+#pragma unroll
+    for (int k = 0; k < kPer; ++k) {
+        const int d = threadIdx.x * kPer + k;
+        if (d < nbuckets) dstart[d] = run;
+        run += tot[k];
     }
     __syncthreads();
 #pragma unroll
     for (int r = 0; r < kRsRounds; ++r) {
-        const int64_t i = base + r * 32 + lane;
-        if (i < n) {
+        if (base + r * 32 + lane < n) {
             const unsigned d = (unsigned)(key[r] >> shift) & dmask;
-            const size_t pos = (size_t)offs[(size_t)d * ntiles + blockIdx.x] + wcnt[warp][d] + rank[r];
-            kout[pos] = key[r];
-            vout[pos] = val[r];
+            rank[r] += dstart[d] + wcnt[warp][d];  // position in the tile, digit order
         }
+    }
+    __syncthreads();  // wcnt is read no more: its bytes take the staged tile
+#pragma unroll
+    for (int r = 0; r < kRsRounds; ++r) {
+        if (base + r * 32 + lane < n) {
+            sk[rank[r]] = key[r];
+            sv[rank[r]] = val[r];
+        }
+    }
+    __syncthreads();
+    const int tn = (int)(n - tbase < kRsTile ? n - tbase : kRsTile);
+    for (int j = threadIdx.x; j < tn; j += kRsThreads) {
+        const K k = sk[j];
+        const unsigned d = (unsigned)(k >> shift) & dmask;
+        const size_t pos = (size_t)offs[(size_t)d * ntiles + blockIdx.x] + (uint32_t)(j - dstart[d]);
+        kout[pos] = k;
+        vout[pos] = sv[j];
     }
 }
 
@@ -302,8 +361,10 @@ static int radix_sort(sgb_grid* g, int64_t n, int bits, K** keys_out, uint32_t**
         SGB_CUDA(cudaGetLastError());
         SGB_TRY(scan_exclusive_u32(hist.as<uint32_t>(), hoff.as<uint32_t>(), (int64_t)ntiles * nbuckets, nullptr,
                                    &g->scratch[6], s));
-        k_rs_scatter<K><<<ntiles, kRsThreads, 0, s>>>(kin, vin, kout, vout, n, shift, dmask, nbuckets,
-                                                      hoff.as<uint32_t>(), ntiles);
+        constexpr size_t smem = rs_scatter_smem<K>();
+        SGB_CUDA(cudaFuncSetAttribute(k_rs_scatter<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_rs_scatter<K><<<ntiles, kRsThreads, smem, s>>>(kin, vin, kout, vout, n, shift, dmask, nbuckets,
+                                                         hoff.as<uint32_t>(), ntiles);
         SGB_CUDA(cudaGetLastError());
         K* kt = kin;
         kin = kout;
