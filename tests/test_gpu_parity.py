@@ -441,7 +441,7 @@ def test_existing_offsets_and_counts(sgb, edge):
 
 @pytest.mark.parametrize("edge", [8, 4])
 @pytest.mark.parametrize("kind", ["heat", "gs"])
-@pytest.mark.parametrize("nsteps", [2, 7])
+@pytest.mark.parametrize("nsteps", [2, 7, 64])
 def test_run_steps_small_grid_one_launch(sgb, edge, kind, nsteps):
     """A small grid runs all steps in one cooperative launch: the result equals the
     step-by-step applyStencils path bit for bit (ping-pong, distinct backgrounds)."""
