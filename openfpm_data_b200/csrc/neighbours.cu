@@ -147,22 +147,20 @@ __global__ void k_find_nn(const int64_t* keys, int64_t n, Geometry geo, int kind
 }
 
 // Existence bitmap of every chunk: point p of a chunk is bit (p & 63) of
-// word (p >> 6).  One warp per chunk, one ballot per 32 mask bytes.
-__global__ void k_bits(const uint8_t* mask, int64_t n, int bs, uint64_t* bits) {
-    const int64_t chunk = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (chunk >= n) return;
-    const uint8_t* m = mask + (size_t)chunk * bs;
-    uint64_t word = 0;
-    for (int r = 0; r < bs / 32; ++r) {
-        const unsigned b = __ballot_sync(0xffffffffu, m[r * 32 + lane] & 1);
-        if (r & 1) {
-            word |= (uint64_t)b << 32;
-            if (lane == 0) bits[(size_t)chunk * (bs / 64) + (r >> 1)] = word;
-        } else {
-            word = b;
-        }
-    }
+// word (p >> 6).  The chunk size is a multiple of 64, so the points of mask
+// bytes [16k, 16k + 16) of the whole map are the 16-bit field k % 4 of bitmap
+// word k / 4: one thread per 16 mask bytes, one 16-byte load, one 2-byte store.
+__global__ void k_bits(const uint8_t* __restrict__ mask, int64_t n, int bs, uint64_t* bits) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= n * (bs >> 4)) return;
+    const uint4 v = __ldg(reinterpret_cast<const uint4*>(mask) + t);
+    // bit 0 of each of the four bytes of w, as four bits
+    auto four = [](unsigned w) {
+        const unsigned x = w & 0x01010101u;
+        return (x | x >> 7 | x >> 14 | x >> 21) & 0xfu;
+    };
+    const unsigned b = four(v.x) | four(v.y) << 4 | four(v.z) << 8 | four(v.w) << 12;
+    reinterpret_cast<uint16_t*>(bits)[t] = (uint16_t)b;
 }
 
 // tagBoundaries (src/SparseGridGpu/SparseGridGpu_kernels.cuh:676-737) with
@@ -290,7 +288,7 @@ int ensure_bits(sgb_grid* g, cudaStream_t s) {
     const int words = g->geo.bs / 64;
     SGB_TRY(g->bits.grow((size_t)(g->n + 1) * words * 8));
     if (g->n > 0) {
-        const int64_t threads = g->n * 32;
+        const int64_t threads = g->n * (g->geo.bs / 16);
         k_bits<<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(g->mask.as<uint8_t>(), g->n, g->geo.bs,
                                                                   g->bits.as<uint64_t>());
         SGB_CUDA(cudaGetLastError());
