@@ -267,30 +267,38 @@ __global__ void k_new_pos(const int64_t* newkeys, int64_t nnew, const int64_t* k
     keys_out[pos] = k;
 }
 
-// Move whole chunks (chunk_words 16-byte words each) to their new position:
-// one warp per chunk (no per-word index division), 16-byte loads and stores.
-__global__ void k_move_chunks(const uint4* __restrict__ src, uint4* __restrict__ dst, int64_t nchunks, int chunk_words,
+// Chunk moves as a flat stream of 16-byte words: word i of the old map (of
+// chunk i >> cw_shift; a chunk holds 2^cw_shift words) goes to the same word
+// of the chunk's merged position.  Four independent copies are in flight per
+// thread and the loads are coalesced, whatever a chunk's size.
+__global__ void k_move_chunks(const uint4* __restrict__ src, uint4* __restrict__ dst, int64_t nchunks, int cw_shift,
                               const int64_t* __restrict__ newpos) {
-    const int lane = threadIdx.x & 31;
-    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t c = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; c < nchunks; c += nw) {
-        const uint4* sp = src + c * chunk_words;
-        uint4* dp = dst + newpos[c] * chunk_words;
-#pragma unroll 4
-        for (int o = lane; o < chunk_words; o += 32) dp[o] = sp[o];
+    const int64_t total = nchunks << cw_shift, wmask = (int64_t(1) << cw_shift) - 1;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    for (; i + 3 * stride < total; i += 4 * stride) {
+        uint4 v[4];
+        int64_t d[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int64_t j = i + k * stride;
+            v[k] = __ldcs(src + j);  // the old map is read once
+            d[k] = (__ldg(newpos + (j >> cw_shift)) << cw_shift) | (j & wmask);
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) dst[d[k]] = v[k];
     }
+    for (; i < total; i += stride) dst[(__ldg(newpos + (i >> cw_shift)) << cw_shift) | (i & wmask)] = __ldcs(src + i);
 }
 
-// Fill new chunks with one element pattern (background) / zero mask: one
-// warp per chunk, the pattern replicated into 16-byte words.
-__global__ void k_fill_chunks(uint4* __restrict__ dst, int64_t nnew, int chunk_words, uint4 word,
+// New chunks get the background pattern (or a zero mask), the same flat word stream.
+__global__ void k_fill_chunks(uint4* __restrict__ dst, int64_t nnew, int cw_shift, uint4 word,
                               const int64_t* __restrict__ newpos) {
-    const int lane = threadIdx.x & 31;
-    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t c = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; c < nnew; c += nw) {
-        uint4* dp = dst + newpos[c] * chunk_words;
-        for (int o = lane; o < chunk_words; o += 32) dp[o] = word;
-    }
+    const int64_t total = nnew << cw_shift, wmask = (int64_t(1) << cw_shift) - 1;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+#pragma unroll 4
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += stride)
+        dst[(__ldg(newpos + (i >> cw_shift)) << cw_shift) | (i & wmask)] = word;
 }
 
 // The element pattern of es bytes repeated over a 16-byte word.
@@ -470,29 +478,41 @@ static int flush_impl(sgb_grid* g, const int* ops, int bits, cudaStream_t s) {
         }
         k_new_pos<<<nblk(NB), 256, 0, s>>>(newkeys, NB, g->keys.as<int64_t>(), nold, g->keys2.as<int64_t>(), npos);
         SGB_CUDA(cudaGetLastError());
-        // one warp per chunk: at most 8 CTAs of 8 warps per SM, no more warps than chunks
-        auto warp_grid = [&](int64_t chunks) {
-            return (unsigned)std::max<int64_t>(1, std::min<int64_t>((int64_t)g->num_sms * 8, (chunks + 7) / 8));
+        // flat word streams: at most 16 CTAs of 256 threads per SM, no more threads than words
+        auto word_grid = [&](int64_t chunks, int cw_shift) {
+            const int64_t words = chunks << cw_shift;
+            return (unsigned)std::max<int64_t>(1, std::min<int64_t>((int64_t)g->num_sms * 16, (words + 255) / 256));
         };
+        auto shift_of = [](int words) {  // chunk sizes in 16-byte words are powers of two
+            int sh = 0;
+            while ((1 << sh) < words) ++sh;
+            return sh;
+        };
+        const int msh = shift_of(bs / 16);
+        if ((1 << msh) != bs / 16) {  // chunk edges are powers of two, so every chunk is 2^k words
+            set_error("chunk size is not a power of two 16-byte words");
+            return SGB_ENOTSUP;
+        }
         for (int p = 0; p < g->nprop; ++p) {
             const int es = elem_size(g->ptype[p]);
+            const int sh = shift_of(bs * es / 16);
             if (nold > 0) {
-                k_move_chunks<<<warp_grid(nold), 256, 0, s>>>(g->data[p].as<uint4>(), g->data2[p].as<uint4>(), nold,
-                                                              bs * es / 16, oldpos);
+                k_move_chunks<<<word_grid(nold, sh), 256, 0, s>>>(g->data[p].as<uint4>(), g->data2[p].as<uint4>(),
+                                                                  nold, sh, oldpos);
                 SGB_CUDA(cudaGetLastError());
             }
             uint64_t pat = 0;
             std::memcpy(&pat, g->bck[p], es);
-            k_fill_chunks<<<warp_grid(NB), 256, 0, s>>>(g->data2[p].as<uint4>(), NB, bs * es / 16,
-                                                        replicate16(pat, es), npos);
+            k_fill_chunks<<<word_grid(NB, sh), 256, 0, s>>>(g->data2[p].as<uint4>(), NB, sh, replicate16(pat, es),
+                                                            npos);
             SGB_CUDA(cudaGetLastError());
         }
         if (nold > 0) {
-            k_move_chunks<<<warp_grid(nold), 256, 0, s>>>(g->mask.as<uint4>(), g->mask2.as<uint4>(), nold, bs / 16,
-                                                          oldpos);
+            k_move_chunks<<<word_grid(nold, msh), 256, 0, s>>>(g->mask.as<uint4>(), g->mask2.as<uint4>(), nold, msh,
+                                                               oldpos);
             SGB_CUDA(cudaGetLastError());
         }
-        k_fill_chunks<<<warp_grid(NB), 256, 0, s>>>(g->mask2.as<uint4>(), NB, bs / 16, make_uint4(0, 0, 0, 0), npos);
+        k_fill_chunks<<<word_grid(NB, msh), 256, 0, s>>>(g->mask2.as<uint4>(), NB, msh, make_uint4(0, 0, 0, 0), npos);
         SGB_CUDA(cudaGetLastError());
         // swap buffer sets
         std::swap(g->keys, g->keys2);
