@@ -75,6 +75,32 @@ __device__ __forceinline__ bool chunk_meets(const Box6& bx, const int64_t* o, in
            o[2] <= bx.b[5] && o[2] + e - 1 >= bx.b[2];
 }
 
+// Chunk-coordinate bounds of a box: the chunk at block coordinate c (origin c * e) meets the box
+// exactly when lo <= c <= hi in every dimension, lo = floor(low / e), hi = floor(high / e) --
+// the same test as chunk_meets, without the origin.  Each CTA stages the bounds of the first
+// kStageBoxes boxes in shared memory.
+constexpr int kStageBoxes = 64;
+struct CBounds {
+    int64_t lo[3], hi[3];
+};
+__device__ __forceinline__ int64_t floor_div(int64_t a, int64_t b) {  // b > 0
+    const int64_t q = a / b;
+    return (a % b != 0 && a < 0) ? q - 1 : q;
+}
+__device__ __forceinline__ CBounds cbounds_of(const Box6& bx, int e) {
+    CBounds cb;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        cb.lo[d] = floor_div(bx.b[d], e);
+        cb.hi[d] = floor_div(bx.b[d + 3], e);
+    }
+    return cb;
+}
+__device__ __forceinline__ bool meets_cb(const CBounds& cb, const int64_t* bc) {
+    return bc[0] >= cb.lo[0] && bc[0] <= cb.hi[0] && bc[1] >= cb.lo[1] && bc[1] <= cb.hi[1] && bc[2] >= cb.lo[2] &&
+           bc[2] <= cb.hi[2];
+}
+
 // Counts for all boxes in one pass: cnt[k * (n + 1) + c] = existing points of
 // chunk c inside box k, flg[...] = (cnt != 0).  Both arrays are zeroed by the
 // caller (row entries c = n stay 0 so that one scan over all rows gives every
@@ -85,12 +111,16 @@ __global__ void k_pack_count(const int64_t* __restrict__ keys, int64_t n, Geomet
     const int lane = threadIdx.x & 31;
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
     const int bs = geo.bs, e = geo.edge;
+    __shared__ CBounds sb[kStageBoxes];
+    for (int k = threadIdx.x; k < nb && k < kStageBoxes; k += blockDim.x) sb[k] = cbounds_of(boxes[k], e);
+    __syncthreads();
     for (int64_t c = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; c < n; c += nw) {
-        int64_t o[3];
-        origin_of(geo, keys[c], o);
+        int64_t bc[3], o[3];
+        block_coords(geo, keys[c], bc);
+        for (int d = 0; d < 3; ++d) o[d] = bc[d] * e;
         for (int k = 0; k < nb; ++k) {
+            if (k < kStageBoxes ? !meets_cb(sb[k], bc) : !chunk_meets(boxes[k], o, e)) continue;  // uniform
             const Box6 bx = boxes[k];
-            if (!chunk_meets(bx, o, e)) continue;  // uniform over the warp
             uint8_t mv[16];  // the lane's mask bytes, all loads in flight at once (bs <= 512)
 #pragma unroll
             for (int i = 0; i < 16; ++i) mv[i] = lane + 32 * i < bs ? mask[c * bs + lane + 32 * i] : 0;
@@ -145,14 +175,19 @@ __global__ void k_pack_emit(const int64_t* __restrict__ keys, int64_t n, Geometr
     const int lane = threadIdx.x & 31;
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
     const int bs = geo.bs, e = geo.edge;
+    __shared__ CBounds sb[kStageBoxes];
+    for (int k = threadIdx.x; k < nb && k < kStageBoxes; k += blockDim.x) sb[k] = cbounds_of(pbs[k].box, e);
+    __syncthreads();
     for (int64_t c = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; c < n; c += nw) {
         const int64_t key = keys[c];
-        int64_t o[3];
-        origin_of(geo, key, o);
+        int64_t bc[3], o[3];
+        block_coords(geo, key, bc);
+        for (int d = 0; d < 3; ++d) o[d] = bc[d] * e;
         for (int k = 0; k < nb; ++k) {
+            // uniform over the warp; no scan read for a box the chunk misses
+            if (k < kStageBoxes ? !meets_cb(sb[k], bc) : !chunk_meets(pbs[k].box, o, e)) continue;
             const PackBox& P = pbs[k];
             const Box6 bx = P.box;
-            if (!chunk_meets(bx, o, e)) continue;  // uniform over the warp; no scan read
             const int64_t r = (int64_t)k * (n + 1) + c;
             uint32_t base = scnt[r];
             if (scnt[r + 1] == base) continue;  // no packed point of box k here (uniform)
