@@ -101,6 +101,14 @@ class Dist:
         self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
         return float(t.item())
 
+    def gather(self, obj) -> list:
+        """Every rank's `obj` (a small picklable summary), in rank order."""
+        if not self.pg:
+            return [obj]
+        out = [None] * self.world
+        self.pg.all_gather_object(out, obj)
+        return out
+
     def close(self):
         if self.pg:
             self.pg.destroy_process_group()
@@ -209,6 +217,14 @@ def cpu_baseline(ps, keys_unused, threads: int, max_steps: int, budget_s: float 
     return len(ps.coords) * steps / dt / 1e9, steps, dt
 
 
+def gs512_config(npts: int, nchunks: int, world: int) -> dict:
+    """The workload description both arms print (the same dict, so the lines compare)."""
+    footprint = nchunks * 512 * (4 * 4 + 1)
+    return {"workload": "gray_scott_512^3_chunk8^3_40balls_seed1", "active_points_per_gpu": npts,
+            "chunks": nchunks, "fields": "u,v float32 + ping-pong", "parallelism": f"replicas x{world}",
+            "l2": f"inputs {footprint / 2**20:.0f} MiB > L2 {L2_BYTES / 2**20:.0f} MiB, no flush"}
+
+
 # ---------------------------------------------------------------- arms
 def run_ours(args, dist: Dist):
     import torch
@@ -229,7 +245,6 @@ def run_ours(args, dist: Dist):
     g.load_map(keys, data + [d.copy() for d in data], mask)
     prm = gs_params()
     stream = torch.cuda.current_stream()
-    footprint = g.nchunks * 512 * (4 * 4 + 1)
 
     # warm-up (W steps), then exactly K timed steps continuing the ping-pong
     g.run_steps(sgb.GS7, [0, 1], [2, 3], prm, args.warmup, use_graph=False)
@@ -318,11 +333,8 @@ def run_ours(args, dist: Dist):
         "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": dist.world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(t_max / args.steps * 1e3, 5), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded, workloads.gray_scott)",
-        "config": {"workload": "gray_scott_512^3_chunk8^3_40balls_seed1", "active_points_per_gpu": npts,
-                   "chunks": g.nchunks, "fields": "u,v float32 + ping-pong", "parallelism": f"replicas x{dist.world}",
-                   "l2": f"inputs {footprint / 2**20:.0f} MiB > L2 {L2_BYTES / 2**20:.0f} MiB, no flush",
-                   "launch": {"ctas_per_sm": args.ctas_per_sm or DEFAULT_CTAS_PER_SM,
-                              "stages": args.stages or DEFAULT_STAGES}},
+        "config": gs512_config(npts, g.nchunks, dist.world),
+        "launch": {"ctas_per_sm": args.ctas_per_sm or DEFAULT_CTAS_PER_SM, "stages": args.stages or DEFAULT_STAGES},
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": args.steps,
         "clocks": clk,
     }
@@ -502,6 +514,27 @@ def _batched_specs(n=256):
             for e, r, s in zip(edges, radii, seeds)]
 
 
+def _spec_weights(specs):
+    """Estimated active points of each batched grid (the ball's volume)."""
+    return [4.0 / 3.0 * np.pi * float(sp.balls[0, 3]) ** 3 for sp in specs]
+
+
+def batched_shard(rank: int, world: int):
+    """(all 256 batched grid specs, indices of this rank's grids): the grids are dealt largest-first
+    by estimated active points, so every rank computes the same split without talking."""
+    from openfpm_data_b200 import shard
+    all_specs = _batched_specs()
+    return all_specs, shard.shard_weighted(_spec_weights(all_specs), rank, world)
+
+
+def served_shard(rate: float, seconds: float, rank: int, world: int):
+    """(the whole seed-4 request stream, this rank's requests): round-robin by request id."""
+    from openfpm_data_b200 import shard
+    from openfpm_data_b200 import workloads as W
+    all_reqs = W.requests(rate=rate, duration=seconds, seed=4)
+    return all_reqs, shard.shard_requests(all_reqs, rank, world)
+
+
 def run_batched256(args, dist: Dist):
     """256 heat grids of uneven size (edges log-uniform in [32, 384], one
     centred ball of radius 0.25-0.5 edge, seed 3), 200 steps per solve.
@@ -516,7 +549,9 @@ def run_batched256(args, dist: Dist):
     from openfpm_data_b200 import autotune as A
     from openfpm_data_b200 import workloads as W
     torch.cuda.set_device(dist.local)
-    specs = _batched_specs()
+    # ranks split the 256 grids without any exchange
+    all_specs, mine = batched_shard(dist.rank, dist.world)
+    specs = [all_specs[i] for i in mine]
     steps_per_solve = 200
     tune = A.autotune(specs[::8], sgb.HEAT7, [W.HEAT_DT], steps=10, device=dist.local)
     nsolves = max(1, min(args.steps, 20))
@@ -539,7 +574,7 @@ def run_batched256(args, dist: Dist):
     t = dist.max(e0.elapsed_time(e1) / 1e3)
     ngr, nch, nbytes = b.info()
     b.close()
-    batched = dist.world * len(specs) * nsolves / t
+    batched = len(all_specs) * nsolves / t
     # per-grid plain launches, the same grids and steps (8^3 chunks, default launch)
     grids = []
     for sp in specs:
@@ -579,16 +614,17 @@ def run_batched256(args, dist: Dist):
     tr = dist.max(r0.elapsed_time(r1) / 1e3)
     for g in grids:
         g.close()
-    plain = dist.world * len(specs) / tp
-    plain_ref = dist.world * len(specs) / tr
-    per_grid_runs = dist.world * len(specs) / tq
+    plain = len(all_specs) / tp
+    plain_ref = len(all_specs) / tr
+    per_grid_runs = len(all_specs) / tq
     peak, pk = _peak_hbm()
-    ach = 9 * pts * steps_per_solve * nsolves / (t / dist.world) / 1e9 if dist.world == 1 else None
+    ach = 9 * pts * steps_per_solve * nsolves / t / 1e9 if dist.world == 1 else None
     roof = {"bound": "hbm", "achieved": round(ach, 1) if ach else None, "peak": peak, "unit": "GB/s",
             "frac": round(ach / peak, 4) if ach else None, "traffic": None, "peak_kind": pk,
             "alg_bytes_per_launch": 9 * pts}
     return _line("batched solves/s (256 heat grids, 200 steps each)", round(batched, 3), "solves/s", dist, args,
                  nsolves, t, {"workload": "batched_256_heat_grids_edge32-384_logu_seed3", "active_points": pts,
+                              "grids_this_rank": len(specs), "split": "grids dealt to ranks by active points",
                               "chunks": nch, "resident_bytes": nbytes,
                               "autotune": {"chunk_edge": tune.chunk_edge, "ctas_per_sm": tune.ctas_per_sm,
                                            "stages": tune.stages, "threads_per_chunk": tune.threads_per_chunk,
@@ -614,7 +650,8 @@ def run_served(args, dist: Dist):
     from openfpm_data_b200 import serve as S
     from openfpm_data_b200 import workloads as W
     torch.cuda.set_device(dist.local)
-    reqs = W.requests(rate=args.serve_rate, duration=args.serve_seconds, seed=4 + 1000 * dist.rank)
+    # one seed-4 stream dealt round-robin to the ranks: each rank serves its share, no exchange
+    all_reqs, reqs = served_shard(args.serve_rate, args.serve_seconds, dist.rank, dist.world)
     warm = W.requests(duration=0.05, seed=99)
     srv = S.Server(budget_bytes=150e9, device=dist.local)
     srv.run(warm, realtime=False)
@@ -627,19 +664,32 @@ def run_served(args, dist: Dist):
     clk = clocks.stop()
     srv.close()
     summ = st.summary()
+    if dist.world > 1:
+        # merged latency percentiles and the aggregate over all ranks' requests
+        parts = dist.gather({"lat": [d.latency for d in st.done], "wall": st.wall,
+                             "pts": sum(d.points * d.steps for d in st.done)})
+        lat = np.concatenate([np.asarray(p["lat"], dtype=np.float64) for p in parts]) if parts else np.zeros(1)
+        wall = max(p["wall"] for p in parts)
+        summ.update({"completed": int(lat.size), "wall_s": round(wall, 3),
+                     "solves_per_s": round(lat.size / max(wall, 1e-9), 2),
+                     "p50_latency_ms": round(float(np.percentile(lat, 50)) * 1e3, 2) if lat.size else None,
+                     "p99_latency_ms": round(float(np.percentile(lat, 99)) * 1e3, 2) if lat.size else None,
+                     "gpts_per_s": round(sum(p["pts"] for p in parts) / max(wall, 1e-9) / 1e9, 3),
+                     "merged_over_ranks": dist.world})
     sample = reqs[: args.plain_sample]
     t0 = time.perf_counter()
     for r in sample:
         S.solve_alone(r, device=dist.local)
     torch.cuda.synchronize()
-    tp = time.perf_counter() - t0
-    plain = len(sample) / tp
-    served = dist.world * summ["completed"] / st.wall
+    tp = dist.max(time.perf_counter() - t0)
+    plain = dist.world * len(sample) / tp  # every rank solves its own sample alone
+    served = summ["completed"] / summ["wall_s"] if summ["wall_s"] else 0.0
     return _line(f"served solves/s (heat + Gray-Scott requests, Poisson {args.serve_rate:g}/s)", round(served, 2),
                  "solves/s",
-                 dist, args, summ["completed"], st.wall,
+                 dist, args, summ["completed"], summ["wall_s"],
                  {"workload": f"served_poisson{args.serve_rate:g}_{args.serve_seconds:g}s_edge32-256_seed4",
-                  "requests": len(reqs),
+                  "requests": len(all_reqs), "requests_this_rank": len(reqs),
+                  "split": "one seed-4 stream dealt round-robin by request id",
                   "serve": summ, "plain_sample": len(sample), "plain_solves_per_s": round(plain, 3),
                   "served_over_plain": round(served / plain, 2), "budget_bytes": 150e9},
                  roofline=None, cpu_baseline=None,
@@ -880,6 +930,7 @@ def run_reference(args, dist: Dist):
         return None
     threads = os.cpu_count() or 1
     ps = W.gray_scott()
+    nchunks = len(np.unique(((ps.coords[:, 2] // 8) * 64 + ps.coords[:, 1] // 8) * 64 + ps.coords[:, 0] // 8))
     wu = max(1, args.warmup)
     v, st, dt = cpu_baseline(ps, None, threads, max(1, args.steps), budget_s=90.0, warmup=wu)
     cpu = {"value": round(v, 5), "unit": UNIT, "cores": threads, "kind": "port",
@@ -887,7 +938,7 @@ def run_reference(args, dist: Dist):
     return {"metric": METRIC, "value": round(v, 5), "unit": UNIT, "n_gpus": dist.world, "steps": st,
             "warmup": wu, "ms_per_step": round(dt / st * 1e3, 3), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded, workloads.gray_scott)",
-            "config": {"workload": "gray_scott_512^3_chunk8^3_40balls_seed1", "active_points": len(ps.coords)},
+            "config": gs512_config(len(ps.coords), nchunks, dist.world),
             "impl": "reference", "cpu_baseline": cpu,
             "e2e": {"value": round(v, 5), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 

@@ -9,6 +9,15 @@
  * "host".  Handles are not thread safe; one handle is used by one host thread
  * at a time.
  *
+ * Devices: a grid lives on the device it was created for.  The entry points
+ * that take a device or only free or look up memory (sgb_create,
+ * sgb_destroy, sgb_release_scratch, sgb_batch_create, sgb_batch_destroy,
+ * sgb_existing_offsets_noalloc, sgb_probe_bounded_waits) switch to that
+ * device themselves and give the caller's current device back before they
+ * return; every other entry point runs on the calling thread's current
+ * device, which must be the grid's (as every call of the reference runs on
+ * the current device).
+ *
  * Block-map layout (identical to the reference's memory_traits_inte layout):
  *   index[n]                int64 chunk ids, sorted ascending
  *   data_p[(n+1) * bs]      one array per property, chunk major; position n
@@ -343,7 +352,9 @@ int sgb_count_existing(sgb_grid* g, int64_t* existing, int64_t* padding, sgb_str
  * points in chunks 0..i-1, offsets_dev[n] = total (int64, n + 1 entries).
  * The calc_exist_points + scan step of tagBoundaries(...,
  * CALCULATE_EXISTING_POINTS) (SparseGridGpu.hpp:2355-2387,
- * SparseGridGpu_kernels.cuh:1194-1225); totals below 2^32 points. */
+ * SparseGridGpu_kernels.cuh:1194-1225).  Grids of 2^32 or more chunk points
+ * (chunks x edge^3) are rejected with SGB_ERANGE: the counts are scanned in
+ * 32-bit words. */
 int sgb_existing_offsets(sgb_grid* g, int64_t* offsets_dev, sgb_stream s);
 
 /* The same offsets without allocating device memory (no counterpart in the

@@ -37,12 +37,37 @@ def _stale() -> bool:
     return any(os.path.getmtime(d) > t for d in deps)
 
 
+OBJ_DIR = os.path.join(HERE, "_build")
+
+
 def build(force: bool = False, verbose: bool = False) -> str:
+    """Compile every csrc/*.cu to an object in parallel, then link the shared library."""
     if not force and not _stale():
         return LIB
+    from concurrent.futures import ThreadPoolExecutor
     nvcc = os.environ.get("NVCC", "nvcc")
+    os.makedirs(OBJ_DIR, exist_ok=True)
+    compile_flags = [f for f in NVCC_FLAGS if f != "-shared"]
+
+    def compile_one(src):
+        obj = os.path.join(OBJ_DIR, os.path.basename(src)[:-3] + ".o")
+        cmd = [nvcc] + compile_flags + ["-I", os.path.join(ROOT, "include"), "-c", "-o", obj, src]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        return obj, r
+
+    srcs = sources()
+    with ThreadPoolExecutor(max_workers=max(1, min(len(srcs), os.cpu_count() or 1))) as ex:
+        results = list(ex.map(compile_one, srcs))
+    for obj, r in results:
+        sys.stdout.write(r.stdout)
+        sys.stderr.write(r.stderr)
+        if r.returncode != 0:
+            raise subprocess.CalledProcessError(r.returncode, r.args)
     tmp = LIB + ".tmp"
-    cmd = [nvcc] + NVCC_FLAGS + ["-I", os.path.join(ROOT, "include"), "-o", tmp] + sources()
+    cmd = [nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-Xcompiler", "-fPIC", "-o", tmp]
+    cmd += [obj for obj, _ in results]
     if verbose:
         print(" ".join(cmd), flush=True)
     subprocess.run(cmd, check=True)

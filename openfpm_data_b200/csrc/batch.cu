@@ -169,7 +169,8 @@ extern "C" {
 
 int sgb_batch_create(sgb_batch** out, int device) {
     if (!out) return SGB_EINVAL;
-    SGB_CUDA(cudaSetDevice(device));
+    DeviceGuard dg(device);
+    SGB_CUDA(dg.status);
     sgb_batch* b = new sgb_batch();
     b->device = device;
     cudaDeviceGetAttribute(&b->num_sms, cudaDevAttrMultiProcessorCount, device);
@@ -183,7 +184,7 @@ int sgb_batch_create(sgb_batch** out, int device) {
 
 int sgb_batch_destroy(sgb_batch* b) {
     if (!b) return SGB_EINVAL;
-    cudaSetDevice(b->device);
+    DeviceGuard dg(b->device);
     for (DevBuf* d : {&b->keys, &b->mask, &b->nn, &b->gid, &b->grids, &b->keys2, &b->mask2, &b->nn2, &b->gid2, &b->err})
         d->release();
     for (int k = 0; k < 2; ++k)

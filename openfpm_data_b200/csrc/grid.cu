@@ -384,7 +384,8 @@ int sgb_create(sgb_grid** out, int dim, int edge, const int64_t* size, int nprop
         if (prop_types[p] < SGB_F32 || prop_types[p] > SGB_U8) return SGB_EINVAL;
     for (int d = 0; d < dim; ++d)
         if (size[d] <= 0) return SGB_EINVAL;
-    SGB_CUDA(cudaSetDevice(device));
+    DeviceGuard dg(device);
+    SGB_CUDA(dg.status);
     sgb_grid* g = new sgb_grid();
     g->device = device;
     g->geo.dim = dim;
@@ -412,7 +413,7 @@ int sgb_create(sgb_grid** out, int dim, int edge, const int64_t* size, int nprop
 
 int sgb_destroy(sgb_grid* g) {
     if (!g) return SGB_EINVAL;
-    cudaSetDevice(g->device);
+    DeviceGuard dg(g->device);
     g->keys.release();
     g->keys2.release();
     g->mask.release();
@@ -451,7 +452,8 @@ int sgb_existence_changed(sgb_grid* g) {
 
 int sgb_release_scratch(sgb_grid* g) {
     if (!g) return SGB_EINVAL;
-    cudaSetDevice(g->device);
+    DeviceGuard dg(g->device);
+    SGB_CUDA(dg.status);
     SGB_CUDA(cudaDeviceSynchronize());  // no kernel of this grid may still use the buffers
     g->keys2.release();
     g->mask2.release();
@@ -688,6 +690,11 @@ int sgb_existing_offsets(sgb_grid* g, int64_t* offsets, sgb_stream stream) {
     if (!g || !offsets) return SGB_EINVAL;
     cudaStream_t s = (cudaStream_t)stream;
     const int64_t n = g->n;
+    if (n * (int64_t)g->geo.bs >= (int64_t(1) << 32)) {
+        // the counts are scanned in 32-bit words: larger totals would wrap
+        set_error("sgb_existing_offsets scans 32-bit counts: at most 2^32 - 1 chunk points");
+        return SGB_ERANGE;
+    }
     DevBuf& counts = g->scratch[7];
     DevBuf& scanned = g->scratch[8];
     SGB_TRY(counts.ensure((size_t)(n + 1) * 4));

@@ -37,6 +37,24 @@ int cuda_status(cudaError_t e, const char* what);
         if (s_ != SGB_OK) return s_;  \
     } while (0)
 
+// Makes `dev` the current device for the lifetime of the guard and gives the
+// caller's current device back on every return path, so an entry point that
+// works on a grid of another GPU leaves the caller's CUDA state as it was.
+struct DeviceGuard {
+    int prev = -1;
+    cudaError_t status = cudaSuccess;
+    explicit DeviceGuard(int dev) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != dev) status = cudaSetDevice(dev);
+        else prev = -1;  // nothing to restore
+    }
+    ~DeviceGuard() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+    DeviceGuard(const DeviceGuard&) = delete;
+    DeviceGuard& operator=(const DeviceGuard&) = delete;
+};
+
 // Grow-only device buffer.
 struct DevBuf {
     void* p = nullptr;

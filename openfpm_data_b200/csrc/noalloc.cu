@@ -134,7 +134,8 @@ extern "C" int sgb_existing_offsets_noalloc(const sgb_grid* g, int64_t* offsets_
         set_error("sgb_existing_offsets_noalloc handles at most 1048576 chunks; use sgb_existing_offsets");
         return SGB_ERANGE;
     }
-    SGB_CUDA(cudaSetDevice(g->device));
+    DeviceGuard dg(g->device);
+    SGB_CUDA(dg.status);
     long long* scratch = nullptr;
     SGB_TRY(scratch_for_device(g->device, &scratch));
     cudaStream_t s = (cudaStream_t)stream;

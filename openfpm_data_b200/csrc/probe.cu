@@ -37,7 +37,8 @@ using namespace sgb;
 
 extern "C" int sgb_probe_bounded_waits(int64_t limit_ns, int device, sgb_stream stream) {
     if (limit_ns <= 0 || limit_ns > 1000000000ll) return SGB_EINVAL;
-    SGB_CUDA(cudaSetDevice(device));
+    DeviceGuard dg(device);
+    SGB_CUDA(dg.status);
     cudaStream_t s = (cudaStream_t)stream;
     unsigned* d = nullptr;
     SGB_CUDA(cudaMalloc(&d, 8));

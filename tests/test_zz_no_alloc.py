@@ -58,3 +58,23 @@ def test_noalloc_rejects_grids_above_its_maximum():
     assert b"1048576" in lib.sgb_last_error_string()
     st, ref = _offsets(lib, g, noalloc=False)  # the allocating entry point has no such limit
     assert st == 0 and ref[-1] == n * 64
+
+
+def test_noalloc_offsets_at_the_maximum_size():
+    """Exactly 1,048,576 chunks: all 512 scan tiles and the full one-CTA scan of
+    the tile sums run; the result must equal the allocating entry point's."""
+    import openfpm_data_b200 as sgb
+    from openfpm_data_b200 import _lib
+    lib = _lib.load()
+    n = 1_048_576
+    g = sgb.SparseGridGpu((1024, 1024, 1024), ["u8"], edge=4)
+    keys = torch.arange(n, dtype=torch.int64, device="cuda")
+    gen = torch.Generator(device="cuda").manual_seed(5)
+    mask = (torch.rand(n * 64, device="cuda", generator=gen) < 0.37).to(torch.uint8)
+    g.load_map_dev(keys, [torch.zeros(n * 64, dtype=torch.uint8, device="cuda")], mask)
+    for _ in range(2):  # two calls in a row on the shared scratch
+        st_a, ref = _offsets(lib, g, noalloc=False)
+        st_b, got = _offsets(lib, g, noalloc=True)
+        assert st_a == 0 and st_b == 0
+        assert np.array_equal(got, ref)
+    assert got[-1] == int(mask.sum().item())
