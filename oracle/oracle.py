@@ -66,6 +66,8 @@ def _load():
         f = C.c_float
         _lib.sgo_heat7.argtypes = [vp, i32, i32, f, vp]
         _lib.sgo_gs7.argtypes = [vp, i32, i32, i32, i32, f, f, f, f, f, vp]
+        _lib.sgo_gs7_steps.argtypes = [vp, i32, i32, i32, i32, f, f, f, f, f, i32, i32]
+        _lib.sgo_heat7_steps.argtypes = [vp, i32, i32, f, i32, i32]
         _lib.sgo_box27.argtypes = [vp, i32, i32, vp, vp]
         _lib.sgo_box27_ns.argtypes = [vp, i32, i32, vp, vp]
         _lib.sgo_set_zorder.argtypes = [vp, i32]
@@ -380,6 +382,16 @@ class OracleGrid:
     def gs7(self, pu, pv, pu2, pv2, Du, Dv, F, k, dt, box=None):
         b = self._box(box)
         _lib.sgo_gs7(self._h, pu, pv, pu2, pv2, Du, Dv, F, k, dt, None if b is None else _ptr(b))
+
+    def gs7_steps(self, pu, pv, pu2, pv2, Du, Dv, F, k, dt, steps, threads=None):
+        """`steps` gs7 calls ping-ponging (pu, pv) <-> (pu2, pv2), the chunks of each step shared
+        out over host threads (the same bits as the serial calls)."""
+        _lib.sgo_gs7_steps(self._h, pu, pv, pu2, pv2, Du, Dv, F, k, dt, steps, threads or (os.cpu_count() or 1))
+
+    def heat7_steps(self, src, dst, dt, steps, threads=None):
+        """`steps` heat7 calls ping-ponging src <-> dst over host threads (the same bits as the
+        serial calls)."""
+        _lib.sgo_heat7_steps(self._h, src, dst, dt, steps, threads or (os.cpu_count() or 1))
 
     def box27(self, src, dst, coeff, box=None):
         c = np.ascontiguousarray(coeff, dtype=np.float32).reshape(27)

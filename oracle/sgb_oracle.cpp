@@ -26,6 +26,7 @@
 #include <cstdint>
 #include <cstring>
 #include <numeric>
+#include <thread>
 #include <vector>
 #include <xmmintrin.h>
 
@@ -361,6 +362,81 @@ void relayout(Grid& g, const std::vector<int64_t>& merged, const std::vector<int
     g.mask.swap(nm);
 }
 
+// One chunk of a HeatStencil step into `out` (the destination array's bytes).
+void heat7_chunk(const Grid& g, const std::vector<int64_t>& nn, int64_t i, int src, float dt, const int64_t* box,
+                 std::vector<float>& tile, std::vector<uint8_t>& out) {
+    load_tile(g, nn, NN_STAR, i, src, tile);
+    for (int o = 0; o < g.bs; ++o) {
+        int lc[3] = {0, 0, 0}, tc[3] = {0, 0, 0};
+        local_coord(g, o, lc);
+        for (int d = 0; d < g.dim; ++d) tc[d] = lc[d] + 1;
+        float cur = tile[tile_index(g, tc)];
+        float res = cur;
+        if (active(cur_mask(g, i, o, box))) {
+            float lap = (float)(-2.0 * g.dim * (double)cur);
+            for (int d = 0; d < g.dim; ++d) {
+                int a[3] = {tc[0], tc[1], tc[2]}, b[3] = {tc[0], tc[1], tc[2]};
+                a[d] -= 1;
+                b[d] += 1;
+                lap = lap + (tile[tile_index(g, a)] + tile[tile_index(g, b)]);
+            }
+            res = std::fmaf(dt, lap, cur);
+        }
+        std::memcpy(&out[((size_t)i * g.bs + o) * 4], &res, 4);
+    }
+}
+
+// One chunk of a Gray-Scott step into `ou` / `ov` (the destination arrays' bytes).
+void gs7_chunk(const Grid& g, const std::vector<int64_t>& nn, int64_t i, int pu, int pv, float Du, float Dv, float F,
+               float nfk, float dt, const int64_t* box, std::vector<float>& tu, std::vector<float>& tv,
+               std::vector<uint8_t>& ou, std::vector<uint8_t>& ov) {
+    load_tile(g, nn, NN_STAR, i, pu, tu);
+    load_tile(g, nn, NN_STAR, i, pv, tv);
+    for (int o = 0; o < g.bs; ++o) {
+        if (!active(cur_mask(g, i, o, box))) continue;
+        int lc[3] = {0, 0, 0}, tc[3] = {0, 0, 0};
+        local_coord(g, o, lc);
+        for (int d = 0; d < g.dim; ++d) tc[d] = lc[d] + 1;
+        int ci = tile_index(g, tc);
+        float u = tu[ci], v = tv[ci];
+        float lu = (float)(-2.0 * g.dim * (double)u), lv = (float)(-2.0 * g.dim * (double)v);
+        for (int d = 0; d < g.dim; ++d) {
+            int a[3] = {tc[0], tc[1], tc[2]}, b[3] = {tc[0], tc[1], tc[2]};
+            a[d] -= 1;
+            b[d] += 1;
+            int ia = tile_index(g, a), ib = tile_index(g, b);
+            lu = lu + (tu[ia] + tu[ib]);
+            lv = lv + (tv[ia] + tv[ib]);
+        }
+        float uvv = (u * v) * v;
+        float du = std::fmaf(F, 1.0f - u, std::fmaf(Du, lu, -uvv));
+        float dv = std::fmaf(nfk, v, std::fmaf(Dv, lv, uvv));
+        float un = std::fmaf(dt, du, u), vn = std::fmaf(dt, dv, v);
+        std::memcpy(&ou[((size_t)i * g.bs + o) * 4], &un, 4);
+        std::memcpy(&ov[((size_t)i * g.bs + o) * 4], &vn, 4);
+    }
+}
+
+// Runs body(lo, hi) over [0, n) split into `threads` ranges, each thread with FTZ|DAZ set.
+template <typename F>
+void for_chunks(int64_t n, int threads, F body) {
+    threads = std::max(1, std::min<int>(threads, 256));
+    if (threads == 1 || n < 2) {
+        FtzScope ftz;
+        body(0, n);
+        return;
+    }
+    std::vector<std::thread> pool;
+    for (int t = 0; t < threads; ++t) {
+        const int64_t lo = n * t / threads, hi = n * (t + 1) / threads;
+        pool.emplace_back([&body, lo, hi] {
+            FtzScope ftz;
+            body(lo, hi);
+        });
+    }
+    for (auto& th : pool) th.join();
+}
+
 }  // namespace
 
 // =================================================================== C API
@@ -605,27 +681,7 @@ void sgo_heat7(void* h, int src, int dst, float dt, const int64_t* box) {
     auto nn = find_neighbours(*g, NN_STAR);
     std::vector<float> tile;
     std::vector<uint8_t> out(g->data[dst]);
-    for (int64_t i = 0; i < g->n(); ++i) {
-        load_tile(*g, nn, NN_STAR, i, src, tile);
-        for (int o = 0; o < g->bs; ++o) {
-            int lc[3] = {0, 0, 0}, tc[3] = {0, 0, 0};
-            local_coord(*g, o, lc);
-            for (int d = 0; d < g->dim; ++d) tc[d] = lc[d] + 1;
-            float cur = tile[tile_index(*g, tc)];
-            float res = cur;
-            if (active(cur_mask(*g, i, o, box))) {
-                float lap = (float)(-2.0 * g->dim * (double)cur);
-                for (int d = 0; d < g->dim; ++d) {
-                    int a[3] = {tc[0], tc[1], tc[2]}, b[3] = {tc[0], tc[1], tc[2]};
-                    a[d] -= 1;
-                    b[d] += 1;
-                    lap = lap + (tile[tile_index(*g, a)] + tile[tile_index(*g, b)]);
-                }
-                res = std::fmaf(dt, lap, cur);
-            }
-            std::memcpy(&out[((size_t)i * g->bs + o) * 4], &res, 4);
-        }
-    }
+    for (int64_t i = 0; i < g->n(); ++i) heat7_chunk(*g, nn, i, src, dt, box, tile, out);
     g->data[dst].swap(out);
 }
 
@@ -647,35 +703,48 @@ void sgo_gs7(void* h, int pu, int pv, int pu2, int pv2, float Du, float Dv, floa
     std::vector<float> tu, tv;
     std::vector<uint8_t> ou(g->data[pu2]), ov(g->data[pv2]);
     const float nfk = -(F + k);
-    for (int64_t i = 0; i < g->n(); ++i) {
-        load_tile(*g, nn, NN_STAR, i, pu, tu);
-        load_tile(*g, nn, NN_STAR, i, pv, tv);
-        for (int o = 0; o < g->bs; ++o) {
-            if (!active(cur_mask(*g, i, o, box))) continue;
-            int lc[3] = {0, 0, 0}, tc[3] = {0, 0, 0};
-            local_coord(*g, o, lc);
-            for (int d = 0; d < g->dim; ++d) tc[d] = lc[d] + 1;
-            int ci = tile_index(*g, tc);
-            float u = tu[ci], v = tv[ci];
-            float lu = (float)(-2.0 * g->dim * (double)u), lv = (float)(-2.0 * g->dim * (double)v);
-            for (int d = 0; d < g->dim; ++d) {
-                int a[3] = {tc[0], tc[1], tc[2]}, b[3] = {tc[0], tc[1], tc[2]};
-                a[d] -= 1;
-                b[d] += 1;
-                int ia = tile_index(*g, a), ib = tile_index(*g, b);
-                lu = lu + (tu[ia] + tu[ib]);
-                lv = lv + (tv[ia] + tv[ib]);
-            }
-            float uvv = (u * v) * v;
-            float du = std::fmaf(F, 1.0f - u, std::fmaf(Du, lu, -uvv));
-            float dv = std::fmaf(nfk, v, std::fmaf(Dv, lv, uvv));
-            float un = std::fmaf(dt, du, u), vn = std::fmaf(dt, dv, v);
-            std::memcpy(&ou[((size_t)i * g->bs + o) * 4], &un, 4);
-            std::memcpy(&ov[((size_t)i * g->bs + o) * 4], &vn, 4);
-        }
-    }
+    for (int64_t i = 0; i < g->n(); ++i) gs7_chunk(*g, nn, i, pu, pv, Du, Dv, F, nfk, dt, box, tu, tv, ou, ov);
     g->data[pu2].swap(ou);
     g->data[pv2].swap(ov);
+}
+
+// `steps` Gray-Scott / heat steps ping-ponging (pu, pv) -> (pu2, pv2) -> (pu, pv) ...,
+// with the chunks of each step shared out over `threads` host threads.  Every
+// chunk of a step reads only the step's source arrays and writes only its own
+// part of the destination arrays, so the result is the same bits as the serial
+// sgo_gs7 / sgo_heat7 calls, for any thread count.  Every thread sets FTZ|DAZ.
+void sgo_gs7_steps(void* h, int pu, int pv, int pu2, int pv2, float Du, float Dv, float F, float k, float dt,
+                   int steps, int threads) {
+    Grid* g = (Grid*)h;
+    auto nn = find_neighbours(*g, NN_STAR);
+    const float nfk = -(F + k);
+    int a0 = pu, a1 = pv, b0 = pu2, b1 = pv2;
+    for (int s = 0; s < steps; ++s) {
+        std::vector<uint8_t> ou(g->data[b0]), ov(g->data[b1]);
+        for_chunks(g->n(), threads, [&](int64_t lo, int64_t hi) {
+            std::vector<float> tu, tv;
+            for (int64_t i = lo; i < hi; ++i) gs7_chunk(*g, nn, i, a0, a1, Du, Dv, F, nfk, dt, nullptr, tu, tv, ou, ov);
+        });
+        g->data[b0].swap(ou);
+        g->data[b1].swap(ov);
+        std::swap(a0, b0);
+        std::swap(a1, b1);
+    }
+}
+
+void sgo_heat7_steps(void* h, int src, int dst, float dt, int steps, int threads) {
+    Grid* g = (Grid*)h;
+    auto nn = find_neighbours(*g, NN_STAR);
+    int a = src, b = dst;
+    for (int s = 0; s < steps; ++s) {
+        std::vector<uint8_t> out(g->data[b]);
+        for_chunks(g->n(), threads, [&](int64_t lo, int64_t hi) {
+            std::vector<float> tile;
+            for (int64_t i = lo; i < hi; ++i) heat7_chunk(*g, nn, i, a, dt, nullptr, tile, out);
+        });
+        g->data[b].swap(out);
+        std::swap(a, b);
+    }
 }
 
 // Conv3x3x3 (src/SparseGridGpu/tests/SparseGridGpu_tests.cu:887-952) with an

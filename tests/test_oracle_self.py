@@ -108,3 +108,51 @@ def test_workloads_deterministic():
     assert len(e) == 256 and e.min() >= 32 and e.max() <= 384 and np.all(e % 8 == 0)
     reqs = W.requests(duration=0.05)
     assert all(q.kind in ("heat", "gs") and 32 <= q.edge <= 256 for q in reqs)
+
+
+def test_threaded_oracle_steps_equal_serial_calls():
+    """gs7_steps / heat7_steps share each step's chunks over threads: same bits as the serial calls."""
+    ps = W.gray_scott(size=64, nballs=4, rmin=6.0, rmax=14.0, seed=3)
+    keys, data, mask = W.build_block_map(ps.coords, ps.values, ps.size, 8, ps.bck)
+    prm = [W.GS_PARAMS[k] for k in ("Du", "Dv", "F", "k", "dt")]
+
+    def grid():
+        o = O.OracleGrid(ps.size, edge=8, ptypes=[O.T_F32] * 4)
+        for p, b in enumerate([1.0, 0.0, 1.0, 0.0]):
+            o.set_background(p, b)
+        o.load_map(keys, data + [d.copy() for d in data], mask)
+        return o
+
+    a, b = grid(), grid()
+    for k in range(5):
+        s, d = ((0, 1), (2, 3)) if k % 2 == 0 else ((2, 3), (0, 1))
+        a.gs7(s[0], s[1], d[0], d[1], *prm)
+    b.gs7_steps(0, 1, 2, 3, *prm, steps=5, threads=3)
+    for x, y in zip(a.export()[1], b.export()[1]):
+        assert np.array_equal(x, y)
+    a.heat7(0, 2, 0.1)
+    a.heat7(2, 0, 0.1)
+    b.heat7_steps(0, 2, 0.1, 2, threads=4)
+    assert np.array_equal(a.export()[1][0], b.export()[1][0])
+
+
+def test_oracle_reproduces_headline_golden_digests():
+    """The oracle run here gives the digests cached in tests/golden/gs512_oracle.json for the
+    first two steps of the headline Gray-Scott workload (pins the cached fixture)."""
+    import json
+    import os
+    import sys
+    here = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+    sys.path.insert(0, here)
+    import make_gs512_golden as G
+    with open(os.path.join(here, "gs512_oracle.json")) as f:
+        gold = json.load(f)
+    o, keys = G.oracle_grid()
+    prm = [W.GS_PARAMS[k] for k in ("Du", "Dv", "F", "k", "dt")]
+    o.gs7_steps(0, 1, 2, 3, *prm, steps=1)
+    _, d, m = o.export()
+    got = G.field_digest(d[2], d[3], m, len(keys))
+    assert got == gold["checkpoints"]["1"]
+    o.gs7_steps(2, 3, 0, 1, *prm, steps=1)
+    _, d, m = o.export()
+    assert G.field_digest(d[0], d[1], m, len(keys)) == gold["checkpoints"]["2"]
