@@ -64,6 +64,11 @@ def parse():
     ap.add_argument("--serve-seconds", type=float, default=60.0, help="served: arrival window")
     ap.add_argument("--serve-rate", type=float, default=2000.0, help="served: Poisson arrival rate (requests/s)")
     ap.add_argument("--plain-sample", type=int, default=64, help="served: requests solved alone for the baseline")
+    ap.add_argument("--no-sub-records", action="store_true",
+                    help="gs512: leave out the bounded runs of the other configurations")
+    ap.add_argument("--sub-serve-seconds", type=float, default=6.0, help="sub-records: served arrival window")
+    ap.add_argument("--sub-sustained-rate", type=float, default=600.0,
+                    help="sub-records: an arrival rate the served form keeps up with (requests/s)")
     return ap.parse_args()
 
 
@@ -943,6 +948,40 @@ def run_reference(args, dist: Dist):
             "e2e": {"value": round(v, 5), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
+SUB_KEYS = ("metric", "value", "unit", "steps", "ms_per_step", "roofline", "e2e", "cpu_baseline", "clocks",
+            "gpu_launches")
+
+
+def _sub_records(args, dist: Dist) -> dict:
+    """The other benchmark configurations, each a bounded run timed like the headline (CUDA events on
+    the launching stream, max over ranks, nvidia-smi clocks during its timed region): heat on the
+    128^3 shell, the 1024^3 insert / flush / tag / box27 stress, the 256-grid batched form against
+    per-grid plain launches, and the served form at 2000 requests/s and at a rate it sustains."""
+    import copy
+    plans = [
+        ("heat128", run_heat128, dict(steps=100, warmup=5)),
+        ("insert1024", run_insert1024, dict(steps=10, warmup=3)),
+        ("batched256", run_batched256, dict(steps=4, warmup=3)),
+        ("served_2000rps", run_served, dict(steps=1, warmup=3, serve_rate=2000.0, serve_seconds=args.sub_serve_seconds,
+                                            plain_sample=24)),
+        ("served_sustained", run_served, dict(steps=1, warmup=3, serve_rate=args.sub_sustained_rate,
+                                              serve_seconds=args.sub_serve_seconds, plain_sample=24)),
+    ]
+    out = {}
+    for name, fn, over in plans:
+        a = copy.copy(args)
+        for k, v in over.items():
+            setattr(a, k, v)
+        try:
+            line = fn(a, dist)
+            rec = {k: line.get(k) for k in SUB_KEYS if k in line}
+            rec["config"] = line.get("config")
+            out[name] = rec
+        except Exception as e:  # a failing sub-record is reported, the headline line still prints
+            out[name] = {"error": f"{type(e).__name__}: {e}"}
+    return out
+
+
 def main():
     args = parse()
     dist = Dist(args.gpus)
@@ -954,6 +993,10 @@ def main():
                        "batched256": run_batched256, "served": run_served, "ghost512": run_ghost512,
                        "conv1000": run_conv1000}
             line = runners[args.workload](args, dist)
+            if args.workload == "gs512" and not args.no_sub_records:
+                subs = _sub_records(args, dist)
+                if line is not None:
+                    line["sub_records"] = subs
         if line is not None and dist.rank == 0:
             print(json.dumps(line), flush=True)
     finally:

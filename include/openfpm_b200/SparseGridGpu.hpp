@@ -37,6 +37,15 @@
 
 #include "../sgb200.h"
 
+// Position of a chunk in the block map, as the reference's stencil functors receive it
+// (openfpm::sparse_index, src/Vector/map_vector_sparse.hpp).
+namespace openfpm {
+template <typename T>
+struct sparse_index {
+    T id;
+};
+}  // namespace openfpm
+
 namespace openfpm_b200 {
 
 // ------------------------------------------------------------------ support types
@@ -142,10 +151,77 @@ enum mask_sparse { NOT_EXIST = 0, EXIST = 1, PADDING = 2, EXIST_AND_PADDING = 3 
 template <unsigned dim>
 struct NNStar {
     static constexpr int kind = SGB_NN_STAR;
+    static constexpr int nNN = 8;  // 2^dim table entries per chunk, the 2*dim faces first
 };
 template <unsigned dim>
 struct NNFull {
     static constexpr int kind = SGB_NN_FULL;
+    static constexpr int nNN = 27;  // 3^dim
+    // NNFull::getNNindex_offset (src/SparseGridGpu/SparseGridGpu.hpp:331-355): the neighbour slot
+    // (dx + 3 dy + 9 dz, d in {0, 1, 2}) and the offset inside that chunk of a local coordinate that
+    // may lie one chunk outside; true when it does
+    template <unsigned E, typename I>
+    __host__ __device__ static bool getNNindex_offset(const I (&c)[3], unsigned& nn_index, unsigned& offset_nn) {
+        bool out = false;
+        nn_index = 0;
+        offset_nn = 0;
+        unsigned cnt = 1, cnt_off = 1;
+        for (int i = 0; i < 3; ++i) {
+            const int p = 1 - (int)(c[i] < 0) + (int)(c[i] >= (int)E);
+            nn_index += p * cnt;
+            offset_nn += (unsigned)((int)c[i] + (1 - p) * (int)E) * cnt_off;
+            cnt *= 3;
+            cnt_off *= E;
+            out |= p != 1;
+        }
+        return out;
+    }
+};
+
+// IntPow<base, exp>::value (src/util/mathutil.hpp)
+template <unsigned base, unsigned exp>
+struct IntPow {
+    static constexpr unsigned value = base * IntPow<base, exp - 1>::value;
+};
+template <unsigned base>
+struct IntPow<base, 0> {
+    static constexpr unsigned value = 1;
+};
+
+// The aggregate a device view exposes as AggregateType / AggregateBlockType: the grid's
+// properties stored as chunks of BS points, with the mask block last (index pMask).
+template <typename AggregateT, unsigned BS>
+struct block_aggregate {
+    using scalars = typename AggregateT::type;
+    static constexpr unsigned nprop = std::tuple_size<scalars>::value;
+    static constexpr unsigned size = BS;
+};
+namespace detail {
+template <typename A, unsigned p, bool mask = (p == A::nprop)>
+struct scalar_of {
+    using type = typename std::tuple_element<p, typename A::scalars>::type;
+};
+template <typename A, unsigned p>
+struct scalar_of<A, p, true> {
+    using type = unsigned char;
+};
+}  // namespace detail
+// ScalarTypeOf<AggregateBlockType, p>: the point type of property p (unsigned char for the mask)
+template <typename A, unsigned p>
+using ScalarTypeOf = typename detail::scalar_of<A, p>::type;
+// BlockTypeOf<AggregateType, p>: a chunk of property p; ::size points
+template <typename A, unsigned p>
+struct BlockTypeOf {
+    using scalar_type = ScalarTypeOf<A, p>;
+    static constexpr unsigned size = A::size;
+};
+
+// Result of getNNPoint: the chunk position (the background chunk when the neighbour chunk is
+// absent) and the point's offset inside it (block_offset, SparseGridGpu_ker.cuh)
+template <typename I>
+struct block_offset {
+    I pos;
+    I off;
 };
 
 // flush reductions (src/Vector/cuda/map_vector_sparse_cuda_kernels.cuh:51-352)
@@ -260,8 +336,10 @@ __device__ __forceinline__ int64_t find_key(const int64_t* keys, int64_t n, int6
     return (lo < n && keys[lo] == key) ? lo : -1;
 }
 
-// per-CTA slot counter of the insert pools (vct_atomic_add in the reference)
+// per-CTA slot counters of the insert pools (vct_atomic_add in the reference):
+// point slots of insert<p>, chunk slots of insertBlock
 static __shared__ int sgb_pool_counter;
+static __shared__ int sgb_block_counter;
 
 // Generic conv kernel: one CTA per chunk, (E+2)^3 tiles of the NP source
 // fields in shared memory (faces always, edges and corners with an NNFull
@@ -281,9 +359,11 @@ __global__ void conv_kernel(sgb_view v, int src0, int src1, int dst0, int dst1, 
             const int nz = (dx != 0) + (dy != 0) + (dz != 0);
             int64_t sc = chunk;
             if (nz) {
+                // NNFull: the 26 neighbours; NNStar: faces read their neighbour, edge and corner cells
+                // read neighbour 0 (the -x chunk) at the wrapped local coordinate, as the reference's
+                // ghost-layer map does (NNStar::getNNskin, SparseGridGpu_ker_util.hpp:114-139)
                 if (v.nn_kind == SGB_NN_FULL) sc = v.nn[chunk * 27 + (dx + 1) + 3 * (dy + 1) + 9 * (dz + 1)];
-                else if (nz == 1) sc = v.nn[chunk * 8 + (dx ? (dx < 0 ? 0 : 1) : dy ? (dy < 0 ? 2 : 3) : (dz < 0 ? 4 : 5))];
-                else sc = -1;
+                else sc = v.nn[chunk * 8 + (nz > 1 ? 0 : dx ? (dx < 0 ? 0 : 1) : dy ? (dy < 0 ? 2 : 3) : (dz < 0 ? 4 : 5))];
             }
             const int lx = (tx - 1 + E) % E, ly = (ty - 1 + E) % E, lz = (tz - 1 + E) % E;
             const int64_t idx = sc * BS + lx + E * (ly + E * lz);
@@ -342,6 +422,41 @@ __global__ void conv_kernel(sgb_view v, int src0, int src1, int dst0, int dst1, 
 }
 }  // namespace detail
 
+// The chunk slot that insertBlock hands to a CTA: ec.template get<p>()[offset] is
+// property p of the slot's point `offset`, ec.template get<pMask>()[offset] its
+// mask byte (the encap of the reference's blockMap.insert, BlockMapGpu_ker.cuh:199-227).
+// The same encap over a grid chunk is the data block a stencil functor gets
+// (dataBlockLoad / dataBlockStore).
+template <typename AggregateT, unsigned BS>
+struct block_encap {
+    using props = typename AggregateT::type;
+    static constexpr unsigned nprop = std::tuple_size<props>::value;
+    void* val[8];   // arrays of the properties (pools or grid data)
+    uint8_t* mask;  // mask array
+    int64_t slot;   // slot or chunk position in those arrays
+    template <unsigned p>
+    __device__ auto get() const {
+        if constexpr (p == nprop) {
+            return mask + slot * BS;
+        } else {
+            using T = typename std::tuple_element<p, props>::type;
+            return static_cast<T*>(val[p]) + slot * BS;
+        }
+    }
+};
+
+// BlockMapGpu_ker<>::setExist / setPadding / unsetPadding / exist
+// (src/SparseGridGpu/BlockMapGpu_ker.cuh): mask byte helpers of user kernels.
+template <typename A = void, unsigned B = 0, typename C = void>
+struct BlockMapGpu_ker {
+    static __device__ __forceinline__ void setExist(unsigned char& m) { m |= 1; }
+    static __device__ __forceinline__ void unsetExist(unsigned char& m) { m &= ~1; }
+    static __device__ __forceinline__ void setPadding(unsigned char& m) { m |= 2; }
+    static __device__ __forceinline__ void unsetPadding(unsigned char& m) { m &= ~2; }
+    static __device__ __forceinline__ bool exist(unsigned char m) { return m & 1; }
+    static __device__ __forceinline__ bool isPadding(unsigned char m) { return m & 2; }
+};
+
 // ------------------------------------------------------------------ device view
 // Returned by SparseGridGpu::toKernel(); passed by value to user kernels.
 template <typename AggregateT, unsigned E>
@@ -352,8 +467,21 @@ struct SparseGridGpu_ker {
     void* pool_val[8];
     int32_t* pool_cnt;
     int nslot;
+    // chunk-slot pools of insertBlock: key, per-property values, mask bytes, per-CTA count
+    int64_t* blk_key;
+    void* blk_val[8];
+    uint8_t* blk_mask;
+    int32_t* blk_cnt;
+    int nblkslot;
     using props = typename AggregateT::type;
+    using AggregateType = block_aggregate<AggregateT, E * E * E>;
+    using AggregateBlockType = AggregateType;
+    using indexT_ = long;
     static constexpr unsigned blockEdgeSize_ = E;
+    static constexpr unsigned d = 3;
+    static constexpr unsigned dims = 3;
+    static constexpr unsigned pMask = std::tuple_size<props>::value;
+    static constexpr unsigned blockSize = E * E * E;
 
     __host__ __device__ static constexpr unsigned getBlockEdgeSize() { return E; }
 
@@ -365,10 +493,55 @@ struct SparseGridGpu_ker {
         return b * (E * E * E) + l;
     }
 
+    // grid_smb::BlockLinId of a block coordinate (src/Grid/Geometry/grid_smb.hpp:280-299)
+    template <typename CoordT>
+    __device__ int64_t getBlockLinId(const grid_key_dx<3, CoordT>& blockCoord) const {
+        return detail::block_key(v.zorder, v.bsz, blockCoord.get(0), blockCoord.get(1), blockCoord.get(2));
+    }
+
+    // global coordinate of point `offset` of the chunk at block coordinate blockCoord
+    // (SparseGridGpu_ker::getGlobalCoord)
+    template <typename CoordT>
+    __device__ grid_key_dx<3, CoordT> getGlobalCoord(const grid_key_dx<3, CoordT>& blockCoord, unsigned offset) const {
+        grid_key_dx<3, CoordT> k;
+        k.set_d(0, blockCoord.get(0) * E + offset % E);
+        k.set_d(1, blockCoord.get(1) * E + (offset / E) % E);
+        k.set_d(2, blockCoord.get(2) * E + offset / (E * E));
+        return k;
+    }
+
     // vector_sparse_gpu_ker::init (map_vector_sparse_cuda_ker.cuh:129-140)
     __device__ void init() const {
-        if (threadIdx.x == 0 && threadIdx.y == 0 && threadIdx.z == 0) detail::sgb_pool_counter = 0;
+        if (threadIdx.x == 0 && threadIdx.y == 0 && threadIdx.z == 0) {
+            detail::sgb_pool_counter = 0;
+            detail::sgb_block_counter = 0;
+        }
         __syncthreads();
+    }
+
+    // insertBlock(blockId, stride) (BlockMapGpu_ker.cuh:199-227): every thread of the CTA calls
+    // it; the thread with threadIdx.x % stride == 0 takes one chunk slot of this CTA's pool for
+    // chunk id blockId, and the threads with the same threadIdx.x / stride get its encap.
+    // Points written through the encap whose mask byte has EXIST set are inserted at the next
+    // flush, in (CTA, slot, offset) order after the CTA's insert<p> points.  A CTA that takes
+    // more slots than the pool holds makes the next flush fail (SGB_ERANGE).
+    template <unsigned nChunksPerBlocks = 1>
+    __device__ block_encap<AggregateT, E * E * E> insertBlock(int64_t blockId, unsigned stride = 8192) const {
+        __shared__ int slot_of[nChunksPerBlocks];
+        const unsigned group = threadIdx.x / stride;
+        const int64_t blk = blockIdx.x + (int64_t)gridDim.x * (blockIdx.y + (int64_t)gridDim.y * blockIdx.z);
+        if (threadIdx.x % stride == 0 && threadIdx.y == 0 && threadIdx.z == 0) {
+            int slot = atomicAdd(&detail::sgb_block_counter, 1);
+            slot = slot < nblkslot ? slot : nblkslot - 1;  // an overflowing pool is reported at flush
+            blk_key[blk * nblkslot + slot] = blockId;
+            slot_of[group] = slot;
+        }
+        __syncthreads();
+        block_encap<AggregateT, E * E * E> ec;
+        for (int p = 0; p < 8; ++p) ec.val[p] = blk_val[p];
+        ec.mask = blk_mask;
+        ec.slot = blk * nblkslot + slot_of[group];
+        return ec;
     }
 
     // insert<p>(coord): one slot of this CTA's pool (map_vector_sparse_cuda_ker.cuh:309-318)
@@ -390,6 +563,7 @@ struct SparseGridGpu_ker {
         if (threadIdx.x == 0 && threadIdx.y == 0 && threadIdx.z == 0) {
             const int64_t blk = blockIdx.x + (int64_t)gridDim.x * (blockIdx.y + (int64_t)gridDim.y * blockIdx.z);
             pool_cnt[blk] = detail::sgb_pool_counter;
+            if (blk_cnt) blk_cnt[blk] = detail::sgb_block_counter;
         }
     }
 
@@ -435,7 +609,212 @@ struct SparseGridGpu_ker {
         const int64_t pos = detail::find_key(v.keys, v.n, lin / bs);
         return pos >= 0 && (v.mask[pos * bs + lin % bs] & 3) == 3;
     }
+
+    // ---------------------------------------------------------------- stencil functor interface
+    // (SparseGridGpu_ker.cuh:297-372, 551-604, 877-896) for functors applied by applyStencils<S>
+    static __device__ __forceinline__ bool exist(unsigned char m) { return m & 1; }
+    static __device__ __forceinline__ bool isPaddingMask(unsigned char m) { return m & 2; }
+
+    // point coordinate of a linear point id (grid_smb::InvLinId, grid_smb.hpp:263-277)
+    __device__ grid_key_dx<3, int> getCoord(int64_t linId) const {
+        constexpr int64_t bs = E * E * E;
+        int64_t bc[3];
+        detail::block_coords(v.zorder, v.bsz, linId / bs, bc);
+        const int o = (int)(linId % bs);
+        grid_key_dx<3, int> k;
+        k.set_d(0, (int)(bc[0] * E + o % E));
+        k.set_d(1, (int)(bc[1] * E + (o / E) % E));
+        k.set_d(2, (int)(bc[2] * E + o / (E * E)));
+        return k;
+    }
+
+    // the chunk at position pos as a data block (dataBuffer.get(pos) in the reference)
+    __device__ block_encap<AggregateT, E * E * E> getDataBlock(int64_t pos) const {
+        block_encap<AggregateT, E * E * E> ec;
+        for (int p = 0; p < 8; ++p) ec.val[p] = v.data[p];
+        ec.mask = const_cast<uint8_t*>(v.mask);
+        ec.slot = pos;
+        return ec;
+    }
+
+    // enlarged-block (chunk plus one-point halo, (E+2)^3) indexing
+    static __host__ __device__ constexpr unsigned getEnlargedBlockSize() { return (E + 2) * (E + 2) * (E + 2); }
+    __device__ grid_key_dx<3, int> getCoordInEnlargedBlock(unsigned offset) const {
+        grid_key_dx<3, int> k;
+        k.set_d(0, (int)(offset % E) + 1);
+        k.set_d(1, (int)((offset / E) % E) + 1);
+        k.set_d(2, (int)(offset / (E * E)) + 1);
+        return k;
+    }
+    __device__ unsigned getLinIdInEnlargedBlock(unsigned offset) const {
+        return (offset % E + 1) + (E + 2) * (((offset / E) % E + 1) + (E + 2) * (offset / (E * E) + 1));
+    }
+    template <typename C>
+    __device__ unsigned getNeighbourLinIdInEnlargedBlock(const grid_key_dx<3, C>& base, unsigned dimension,
+                                                          char offset) const {
+        int c[3] = {(int)base.get(0), (int)base.get(1), (int)base.get(2)};
+        c[dimension] += offset;
+        return (unsigned)(c[0] + (int)(E + 2) * (c[1] + (int)(E + 2) * c[2]));
+    }
+    template <typename C>
+    __device__ unsigned getNeighbourLinIdInEnlargedBlock(const grid_key_dx<3, C>& base,
+                                                          const grid_key_dx<3, C>& offsets) const {
+        const int c0 = (int)(base.get(0) + offsets.get(0)), c1 = (int)(base.get(1) + offsets.get(1)),
+                  c2 = (int)(base.get(2) + offsets.get(2));
+        return (unsigned)(c0 + (int)(E + 2) * (c1 + (int)(E + 2) * c2));
+    }
+
+    template <unsigned p>
+    __device__ ScalarTypeOf<AggregateType, p> background() const {
+        ScalarTypeOf<AggregateType, p> b;
+        memcpy(&b, &bck[p], sizeof(b));
+        return b;
+    }
+
+    // chunk position of the halo cell (dx, dy, dz) of chunk `chunk` (nz of them non-zero), -1 when
+    // absent.  NNFull: the 26 neighbours.  NNStar (NNStar::getNNskin, SparseGridGpu_ker_util.hpp:
+    // 114-139): faces read their neighbour; edge and corner cells read neighbour 0, the -x chunk,
+    // at the wrapped local coordinate, as the reference's ghost-layer map does.
+    __device__ int64_t halo_chunk(int64_t chunk, int dx, int dy, int dz, int nz) const {
+        if (v.nn_kind == SGB_NN_FULL) return v.nn[chunk * 27 + (dx + 1) + 3 * (dy + 1) + 9 * (dz + 1)];
+        const int slot = nz > 1 ? 0 : (dx ? (dx < 0 ? 0 : 1) : dy ? (dy < 0 ? 2 : 3) : (dz < 0 ? 4 : 5));
+        return v.nn[chunk * 8 + slot];
+    }
+
+    // loadGhostBlock<p> (SparseGridGpu_ker.cuh:551-571 -> loadGhostBlock_impl, SparseGridGpu_ker_util.hpp:
+    // 487-564): every thread of the CTA fills cells of the (E+2)^3 tile of chunk pos with property p;
+    // a cell whose source mask byte is 0 (or whose chunk is absent) takes the background (the mask
+    // property takes the mask byte itself).  The optional mask tile receives the mask bytes.
+    template <unsigned p, typename AggrWrapperT>
+    __device__ void loadGhostBlock(const AggrWrapperT&, openfpm::sparse_index<unsigned> pos,
+                                   ScalarTypeOf<AggregateType, p>* sharedRegion) const {
+        load_tile<p>(pos.id, sharedRegion, nullptr);
+    }
+    template <unsigned p, typename AggrWrapperT>
+    __device__ void loadGhostBlock(const AggrWrapperT&, openfpm::sparse_index<unsigned> pos,
+                                   ScalarTypeOf<AggregateType, p>* sharedRegion, unsigned char* mask) const {
+        load_tile<p>(pos.id, sharedRegion, mask);
+    }
+    template <unsigned p>
+    __device__ void load_tile(int64_t chunk, ScalarTypeOf<AggregateType, p>* tile, unsigned char* mtile) const {
+        using T = ScalarTypeOf<AggregateType, p>;
+        constexpr int TE = E + 2, TT = TE * TE * TE, BS = E * E * E;
+        const int nthr = blockDim.x * blockDim.y * blockDim.z;
+        const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+        T b{};
+        if constexpr (p != pMask) b = background<p>();
+        for (int cell = tid; cell < TT; cell += nthr) {
+            const int tx = cell % TE, ty = (cell / TE) % TE, tz = cell / (TE * TE);
+            const int dx = tx == 0 ? -1 : (tx == TE - 1 ? 1 : 0), dy = ty == 0 ? -1 : (ty == TE - 1 ? 1 : 0),
+                      dz = tz == 0 ? -1 : (tz == TE - 1 ? 1 : 0);
+            const int nz = (dx != 0) + (dy != 0) + (dz != 0);
+            const int64_t sc = nz ? halo_chunk(chunk, dx, dy, dz, nz) : chunk;
+            const int lx = (tx - 1 + E) % E, ly = (ty - 1 + E) % E, lz = (tz - 1 + E) % E;
+            uint8_t m = 0;
+            T val = b;
+            if (sc >= 0) {
+                const int64_t idx = sc * BS + lx + E * (ly + E * lz);
+                m = v.mask[idx];
+                if constexpr (p == pMask) val = m;
+                else if (m != 0) val = static_cast<const T*>(v.data[p])[idx];
+            }
+            tile[cell] = val;
+            if (mtile) mtile[cell] = m;
+        }
+    }
+
+    // storeBlock<p> (SparseGridGpu_ker.cuh:598-604, 877-896): thread `offset` writes its point of the
+    // tile into the chunk.  Points that do not exist receive this property's background (the
+    // reference writes the tile value, the source's background there; every read of a point that
+    // does not exist returns the background, so the two cannot be told apart).
+    template <unsigned p, typename AggrWrapperT>
+    __device__ void storeBlock(AggrWrapperT& block, ScalarTypeOf<AggregateType, p>* sharedRegion) const {
+        constexpr unsigned BS = E * E * E;
+        const unsigned pos = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+        if (pos < BS) {
+            const unsigned char m = block.template get<pMask>()[pos];
+            block.template get<p>()[pos] = m ? sharedRegion[getLinIdInEnlargedBlock(pos)] : background<p>();
+        }
+    }
+
+    // getNNPoint<NN> (SparseGridGpu_ker.cuh:297-327): the chunk position and offset of the point at
+    // `mov` from point `offset` of chunk pos (at most one chunk away); an absent chunk is the
+    // background chunk.  NN is the grid's neighbourhood (NNFull, setNNType<NNFull<3>>).
+    template <typename NN_type, typename I>
+    __device__ block_offset<I> getNNPoint(openfpm::sparse_index<unsigned> pos, unsigned offset,
+                                          const grid_key_dx<3, I>& mov) const {
+        I c[3];
+        for (int i = 0; i < 3; ++i) {
+            c[i] = mov.get(i) + (I)(offset % E);
+            offset /= E;
+        }
+        unsigned nn_index = 0, offset_nn = 0;
+        const bool out = NN_type::template getNNindex_offset<E>(c, nn_index, offset_nn);
+        int64_t nnb = pos.id;
+        if (out) {
+            const int32_t q = v.nn[nn_index + NN_type::nNN * (int64_t)pos.id];
+            nnb = q < 0 ? v.n : q;
+        }
+        return block_offset<I>{(I)nnb, (I)offset_nn};
+    }
+    // get<p>(block_offset): the value stored at that chunk position and offset
+    template <unsigned p, typename I>
+    __device__ ScalarTypeOf<AggregateType, p> get(const block_offset<I>& bo) const {
+        return static_cast<const ScalarTypeOf<AggregateType, p>*>(v.data[p])[(int64_t)bo.pos * (E * E * E) + bo.off];
+    }
 };
+
+// ------------------------------------------------------------------ user stencil functors
+namespace detail {
+template <typename S, typename = void>
+struct is_fixed_stencil : std::false_type {};
+template <typename S>
+struct is_fixed_stencil<S, std::void_t<decltype(S::kind)>> : std::true_type {};
+
+// applyStencilInPlace (SparseGridGpu_kernels.cuh:1045-1094): one CTA of BS threads per chunk,
+// thread `offset` one point; the point's mask is cleared outside the inclusive box; the functor
+// gets the view, the chunk id and position, the point's offset and coordinate, the chunk's data
+// block (to load from and store to) and the mask byte.
+template <typename S, typename Ker, typename... Args>
+__global__ void apply_stencil_inplace(Box<3, int> bx, Ker sg, Args... args) {
+    constexpr unsigned BS = Ker::blockSize;
+    const unsigned dataBlockPos = blockIdx.x;
+    const unsigned offset = threadIdx.x;
+    if (dataBlockPos >= sg.v.n) return;
+    auto dataBlock = sg.getDataBlock(dataBlockPos);
+    const int64_t dataBlockId = sg.v.keys[dataBlockPos];
+    grid_key_dx<3, int> pointCoord = sg.getCoord(dataBlockId * BS + offset);
+    unsigned char curMask = 0;
+    if (offset < BS) {
+        curMask = sg.v.mask[(int64_t)dataBlockPos * BS + offset];
+        for (int i = 0; i < 3; ++i)
+            if (pointCoord.get(i) < bx.getLow(i) || pointCoord.get(i) > bx.getHigh(i)) curMask = 0;
+    }
+    openfpm::sparse_index<unsigned> sdataBlockPos;
+    sdataBlockPos.id = dataBlockPos;
+    S::stencil(sg, (unsigned)dataBlockId, sdataBlockPos, offset, pointCoord, dataBlock, dataBlock, curMask, args...);
+}
+
+// applyStencilInPlaceNoShared (SparseGridGpu_kernels.cuh:1096-1150): one thread per existing point
+// of the existing-point list (chunk position * BS + offset), no shared-memory tiles.
+template <typename S, typename Ker, typename... Args>
+__global__ void apply_stencil_noshared(Box<3, int> bx, Ker sg, const uint32_t* ids, int64_t nids, Args... args) {
+    constexpr unsigned BS = Ker::blockSize;
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= nids) return;
+    const uint32_t id = ids[t];
+    const unsigned dataBlockPos = id / BS, offset = id % BS;
+    auto dataBlock = sg.getDataBlock(dataBlockPos);
+    const int64_t dataBlockId = sg.v.keys[dataBlockPos];
+    grid_key_dx<3, int> pointCoord = sg.getCoord(dataBlockId * BS + offset);
+    unsigned char curMask = sg.v.mask[(int64_t)dataBlockPos * BS + offset];
+    for (int i = 0; i < 3; ++i)
+        if (pointCoord.get(i) < bx.getLow(i) || pointCoord.get(i) > bx.getHigh(i)) curMask = 0;
+    openfpm::sparse_index<unsigned> sdataBlockPos;
+    sdataBlockPos.id = dataBlockPos;
+    S::stencil(sg, (unsigned)dataBlockId, sdataBlockPos, offset, pointCoord, dataBlock, dataBlock, curMask, args...);
+}
+}  // namespace detail
 
 // ------------------------------------------------------------------ host class
 // layout and linearizer tags of the reference's template parameters
@@ -469,6 +848,12 @@ class SparseGridGpu {
     int64_t* pool_lin_ = nullptr;
     void* pool_val_[8] = {};
     int32_t* pool_cnt_ = nullptr;
+    // insertBlock chunk-slot pools
+    int64_t nblkslot_ = 0;
+    int64_t* blk_key_ = nullptr;
+    void* blk_val_[8] = {};
+    uint8_t* blk_mask_ = nullptr;
+    int32_t* blk_cnt_ = nullptr;
     // host copies filled by deviceToHost
     std::vector<int64_t> h_keys_;
     std::vector<std::vector<unsigned char>> h_data_;
@@ -481,7 +866,15 @@ class SparseGridGpu {
         if (pool_cnt_) cudaFree(pool_cnt_);
         pool_lin_ = nullptr;
         pool_cnt_ = nullptr;
-        npools_ = nslot_ = 0;
+        for (auto& p : blk_val_)
+            if (p) cudaFree(p), p = nullptr;
+        if (blk_key_) cudaFree(blk_key_);
+        if (blk_mask_) cudaFree(blk_mask_);
+        if (blk_cnt_) cudaFree(blk_cnt_);
+        blk_key_ = nullptr;
+        blk_mask_ = nullptr;
+        blk_cnt_ = nullptr;
+        npools_ = nslot_ = nblkslot_ = 0;
     }
 
     template <typename... ops>
@@ -538,6 +931,23 @@ class SparseGridGpu {
             if (cudaMalloc(&pool_val_[p], n * es) != cudaSuccess) throw sgb_error(SGB_ENOMEM, "setGPUInsertBuffer");
         }
         cudaMemset(pool_cnt_, 0, nBlock * 4);
+        // insertBlock takes whole chunk slots, as every insert does in the reference: up to nSlot per
+        // CTA, bounded so that the chunk-slot pools stay within 512 MiB (at least one slot per CTA)
+        size_t per_slot = bs;  // mask bytes
+        for (unsigned p = 0; p < nprop; ++p) per_slot += (size_t)bs * (types[p] == SGB_F64 ? 8 : (types[p] == SGB_U8 ? 1 : 4));
+        const size_t cap = (size_t)512 << 20;
+        nblkslot_ = std::max<int64_t>(1, std::min<int64_t>(nSlot, (int64_t)(cap / std::max<size_t>(1, per_slot * nBlock))));
+        const size_t nb = (size_t)nBlock * nblkslot_;
+        if (cudaMalloc(&blk_key_, nb * 8) != cudaSuccess || cudaMalloc(&blk_mask_, nb * bs) != cudaSuccess ||
+            cudaMalloc(&blk_cnt_, nBlock * 4) != cudaSuccess)
+            throw sgb_error(SGB_ENOMEM, "setGPUInsertBuffer (block slots)");
+        for (unsigned p = 0; p < nprop; ++p) {
+            const size_t es = types[p] == SGB_F64 ? 8 : (types[p] == SGB_U8 ? 1 : 4);
+            if (cudaMalloc(&blk_val_[p], nb * bs * es) != cudaSuccess)
+                throw sgb_error(SGB_ENOMEM, "setGPUInsertBuffer (block slots)");
+        }
+        cudaMemset(blk_mask_, 0, nb * bs);  // initializeInsertBuffer (BlockMapGpu_kernels.cuh:110-139)
+        cudaMemset(blk_cnt_, 0, nBlock * 4);
     }
     void setGPUInsertBuffer(dim3 nBlock, dim3 nSlot) {
         setGPUInsertBuffer((int64_t)nBlock.x * nBlock.y * nBlock.z, (int64_t)nSlot.x * nSlot.y * nSlot.z);
@@ -553,6 +963,11 @@ class SparseGridGpu {
         for (int p = 0; p < 8; ++p) k.pool_val[p] = pool_val_[p];
         k.pool_cnt = pool_cnt_;
         k.nslot = (int)nslot_;
+        k.blk_key = blk_key_;
+        for (int p = 0; p < 8; ++p) k.blk_val[p] = blk_val_[p];
+        k.blk_mask = blk_mask_;
+        k.blk_cnt = blk_cnt_;
+        k.nblkslot = (int)nblkslot_;
         return k;
     }
 
@@ -562,6 +977,10 @@ class SparseGridGpu {
         if (npools_) {
             check(sgb_insert_pools(g_, npools_, nslot_, pool_cnt_, pool_lin_, pool_val_, nullptr), "flush (pools)");
             cudaMemset(pool_cnt_, 0, npools_ * 4);
+            check(sgb_insert_blocks(g_, npools_, nblkslot_, blk_cnt_, blk_key_, blk_val_, blk_mask_, nullptr),
+                  "flush (block slots)");
+            cudaMemset(blk_cnt_, 0, npools_ * 4);
+            cudaMemset(blk_mask_, 0, (size_t)npools_ * nblkslot_ * bs);
         }
         auto ops = op_list<v_reduce...>();
         check(sgb_flush(g_, ops.data(), nullptr), "flush");
@@ -590,20 +1009,19 @@ class SparseGridGpu {
         return b;
     }
 
-    // applyStencils<S>(box, mode, args...) for the fixed-function stencils
-    template <typename S>
-    void applyStencils(const Box<dim, int>& box, StencilMode, float dt) {
-        static_assert(S::kind == SGB_HEAT7, "HeatStencil takes dt");
-        run_fixed(S::kind, S::src, S::dst, &dt, 1, box);
-    }
-    template <typename S>
-    void applyStencils(const Box<dim, int>& box, StencilMode, const conv_coeff& cc) {
-        static_assert(S::kind == SGB_BOX27 || S::kind == SGB_BOX27_NS, "Conv3x3x3 takes conv_coeff");
-        float c[27];
-        for (int i = 0; i < 3; ++i)
-            for (int j = 0; j < 3; ++j)
-                for (int k = 0; k < 3; ++k) c[i * 9 + j * 3 + k] = cc.coeff[i][j][k];
-        run_fixed(S::kind, S::src, S::dst, c, 27, box);
+    // applyStencils<S>(box, mode, args...) (SparseGridGpu.hpp:2704-2734).  HeatStencil, Conv3x3x3 and
+    // Conv3x3x3_noshared run the library's fixed-function kernels; any other S is a user functor
+    // with the reference's contract (typedef stencil_type, static __device__ stencil(sparseGrid,
+    // dataBlockId, dataBlockIdPos, offset, pointCoord, dataBlockLoad, dataBlockStore, curMask,
+    // args...)), run one CTA per chunk (STENCIL_MODE_INPLACE) or one thread per existing point
+    // (STENCIL_MODE_INPLACE_NO_SHARED, after tagBoundaries(..., CALCULATE_EXISTING_POINTS)).
+    template <typename S, typename... Args>
+    void applyStencils(const Box<dim, int>& box, StencilMode mode, Args... args) {
+        if constexpr (detail::is_fixed_stencil<S>::value) {
+            apply_fixed<S>(box, args...);
+        } else {
+            apply_user<S>(box, mode, args...);
+        }
     }
 
     // conv family with user __device__ functions (SparseGridGpu.hpp:2568-2683)
@@ -1025,6 +1443,50 @@ class SparseGridGpu {
         int64_t b[6];
         for (unsigned i = 0; i < 3; ++i) b[i] = box.lo[i], b[3 + i] = box.hi[i];
         check(sgb_apply_stencil(g_, kind, src, dst, prm, nprm, b, nullptr), "applyStencils");
+    }
+
+    template <typename S>
+    void apply_fixed(const Box<dim, int>& box, float dt) {
+        static_assert(S::kind == SGB_HEAT7, "HeatStencil takes dt");
+        run_fixed(S::kind, S::src, S::dst, &dt, 1, box);
+    }
+    template <typename S>
+    void apply_fixed(const Box<dim, int>& box, double dt) {
+        apply_fixed<S>(box, (float)dt);
+    }
+    template <typename S>
+    void apply_fixed(const Box<dim, int>& box, const conv_coeff& cc) {
+        static_assert(S::kind == SGB_BOX27 || S::kind == SGB_BOX27_NS, "Conv3x3x3 takes conv_coeff");
+        float c[27];
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j)
+                for (int k = 0; k < 3; ++k) c[i * 9 + j * 3 + k] = cc.coeff[i][j][k];
+        run_fixed(S::kind, S::src, S::dst, c, 27, box);
+    }
+
+    template <typename S, typename... Args>
+    void apply_user(const Box<dim, int>& box, StencilMode mode, Args... args) {
+        using NN = typename S::stencil_type;
+        device_grid_type k{};
+        check(sgb_get_view(g_, NN::kind, &k.v, nullptr), "applyStencils");
+        if (k.v.n == 0) return;
+        for (unsigned p = 0; p < nprop && p < 8; ++p) k.bck[p] = bck_raw_[p];
+        if (mode == STENCIL_MODE_INPLACE_NO_SHARED) {
+            const uint32_t* ids = nullptr;
+            int64_t nids = 0;
+            check(sgb_existing_point_list(g_, &ids, &nids, nullptr), "applyStencils (existing points)");
+            if (nids > 0)
+                detail::apply_stencil_noshared<S><<<(unsigned)((nids + 127) / 128), 128>>>(box, k, ids, nids, args...);
+        } else {
+            detail::apply_stencil_inplace<S><<<(unsigned)k.v.n, bs>>>(box, k, args...);
+        }
+        check(cudaGetLastError() == cudaSuccess ? SGB_OK : SGB_ECUDA, "applyStencils launch");
+        // a functor may store into any point of any property: the library refills the backgrounds
+        // of points that do not exist before its own kernels rely on them
+        for (unsigned p = 0; p < nprop; ++p) {
+            void* d = nullptr;
+            check(sgb_data_buffer(g_, (int)p, &d), "applyStencils");
+        }
     }
 
     template <int NP, int MODE, typename F>

@@ -165,6 +165,20 @@ int sgb_insert_lin(sgb_grid* g, int64_t n, const int64_t* lin_dev, const void* c
 int sgb_insert_pools(sgb_grid* g, int64_t npools, int64_t nslot, const int32_t* counts_dev, const int64_t* lin_dev,
                      const void* const* values_dev, sgb_stream s);
 
+/* Stage the chunk slots written by a user kernel through insertBlock
+ * (src/SparseGridGpu/BlockMapGpu_ker.cuh:199-227: each call takes one whole
+ * chunk slot of its CTA's insert buffer and the CTA writes any of its points,
+ * setting their EXIST mask bits).  npools pools of nslot chunk slots:
+ * counts_dev[b] = slots used by pool b; keys_dev[b*nslot+k] = the slot's chunk
+ * id; values_dev[p] = [npools*nslot*bs] elements of property p (NULL entries
+ * leave the property out); masks_dev = [npools*nslot*bs] mask bytes.  Every
+ * slot point whose mask has EXIST set is staged as an insert, in (pool, slot,
+ * offset) order, until sgb_flush, which reduces duplicates in that order as
+ * the reference reduces its chunk slots.  A count above nslot makes the next
+ * sgb_flush fail with SGB_ERANGE. */
+int sgb_insert_blocks(sgb_grid* g, int64_t npools, int64_t nslot, const int32_t* counts_dev, const int64_t* keys_dev,
+                      const void* const* values_dev, const uint8_t* masks_dev, sgb_stream s);
+
 /* Device view of a grid for user kernels (SparseGridGpu::toKernelNN,
  * SparseGridGpu.hpp:1749-1789): block map pointers and the neighbour table
  * of nn_kind (int32, -1 absent), valid until the next flush or map upload.

@@ -37,6 +37,7 @@ SIGNATURES = {
     "sgb_insert": (_i32, [_vp, _i64, _vp, _vp, _vp]),
     "sgb_insert_lin": (_i32, [_vp, _i64, _vp, _vp, _vp]),
     "sgb_insert_pools": (_i32, [_vp, _i64, _i64, _vp, _vp, _vp, _vp]),
+    "sgb_insert_blocks": (_i32, [_vp, _i64, _i64, _vp, _vp, _vp, _vp, _vp]),
     "sgb_get_view": (_i32, [_vp, _i32, _vp, _vp]),
     "sgb_remove_boxes": (_i32, [_vp, _i64, _vp, _vp]),
     "sgb_existing_points": (_i32, [_vp, _vp, _vp, _i64, _vp, _vp]),

@@ -344,6 +344,64 @@ __global__ void k_count(const uint8_t* mask, int64_t total, unsigned long long* 
     }
 }
 
+// Points of the chunk slots written through insertBlock: per slot (pool b,
+// slot k below the pool's clamped count) the number of mask bytes with EXIST
+// set; one warp per slot, one ballot per 32 mask bytes.
+__global__ void k_block_counts(const uint32_t* pool_counts, int64_t npools, int64_t nslot, const uint8_t* masks,
+                               int bs, uint32_t* out) {
+    const int64_t slot = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (slot >= npools * nslot) return;
+    const int64_t b = slot / nslot, k = slot % nslot;
+    uint32_t c = 0;
+    if (k < (int64_t)pool_counts[b]) {
+        const uint8_t* m = masks + slot * bs;
+        for (int r = 0; r < bs; r += 32) {
+            const bool e = r + lane < bs && (m[r + lane] & 1);
+            c += __popc(__ballot_sync(0xffffffffu, e));
+        }
+    }
+    if (lane == 0) out[slot] = c;
+}
+
+// Emit every EXIST point of every counted slot, in (pool, slot, offset) order,
+// as a staged insert: linear id key * bs + offset and the slot's values.
+__global__ void k_block_emit(const uint32_t* pool_counts, int64_t npools, int64_t nslot, const int64_t* keys,
+                             const uint8_t* masks, const uint32_t* off, Geometry geo, int64_t* out_lin, PoolCopy pc,
+                             unsigned* err) {
+    const int64_t slot = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (slot >= npools * nslot) return;
+    const int64_t b = slot / nslot, k = slot % nslot;
+    if (k >= (int64_t)pool_counts[b]) return;
+    const int bs = geo.bs;
+    int64_t key = keys[slot];
+    const bool key_ok = key >= 0 && key_in_domain(geo, key);
+    const uint8_t* m = masks + slot * bs;
+    uint32_t w = off[slot];
+    for (int r = 0; r < bs; r += 32) {
+        const int o = r + lane;
+        const bool e = o < bs && (m[o] & 1);
+        const unsigned bal = __ballot_sync(0xffffffffu, e);
+        if (e) {
+            const int64_t dst = (int64_t)w + __popc(bal & lanemask_lt());
+            if (!key_ok) atomicOr(err, kErrOutOfDomain);
+            out_lin[dst] = key_ok ? key * bs + o : -1;
+            const int64_t src = slot * bs + o;
+            for (int p = 0; p < pc.nprop; ++p) {
+                const int es = pc.es[p];
+                unsigned char* d = pc.dst[p] + dst * es;
+                if (pc.src[p]) {
+                    for (int q = 0; q < es; ++q) d[q] = pc.src[p][src * es + q];
+                } else {
+                    for (int q = 0; q < es; ++q) d[q] = (unsigned char)(pc.bck[p] >> (8 * q));
+                }
+            }
+        }
+        w += __popc(bal);
+    }
+}
+
 }  // namespace sgb
 
 using namespace sgb;
@@ -542,6 +600,54 @@ int sgb_insert_pools(sgb_grid* g, int64_t npools, int64_t nslot, const int32_t* 
     }
     k_pool_copy<<<(unsigned)npools, 128, 0, s>>>(cnt.as<uint32_t>(), off.as<uint32_t>(), nslot, lin, g->geo,
                                                  g->pend_lin.as<int64_t>() + g->npend, pc, g->err.as<unsigned>());
+    SGB_CUDA(cudaGetLastError());
+    g->npend += add;
+    return SGB_OK;
+}
+
+int sgb_insert_blocks(sgb_grid* g, int64_t npools, int64_t nslot, const int32_t* counts, const int64_t* keys,
+                      const void* const* values, const uint8_t* masks, sgb_stream stream) {
+    if (!g || npools < 0 || nslot <= 0 || nslot > (1 << 30) || (npools > 0 && (!counts || !keys || !masks)))
+        return SGB_EINVAL;
+    if (npools == 0) return SGB_OK;
+    const int64_t nslots = npools * nslot;
+    if (nslots * (int64_t)g->geo.bs >= (int64_t(1) << 32)) {
+        set_error("sgb_insert_blocks: the block pools hold at most 2^32 - 1 chunk points");
+        return SGB_ERANGE;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    DevBuf& cnt = g->scratch[9];
+    DevBuf& per = g->scratch[7];
+    DevBuf& off = g->scratch[8];
+    SGB_TRY(cnt.ensure((size_t)npools * 4 + 16));
+    SGB_TRY(per.ensure((size_t)nslots * 4 + 16));
+    SGB_TRY(off.ensure((size_t)nslots * 4 + 16));
+    k_clamp_counts<<<(unsigned)((npools + 255) / 256), 256, 0, s>>>(counts, npools, (int32_t)nslot, cnt.as<uint32_t>(),
+                                                                     g->err.as<unsigned>());
+    const unsigned wblocks = (unsigned)((nslots * 32 + 255) / 256);
+    k_block_counts<<<wblocks, 256, 0, s>>>(cnt.as<uint32_t>(), npools, nslot, masks, g->geo.bs, per.as<uint32_t>());
+    SGB_CUDA(cudaGetLastError());
+    uint32_t* total = off.as<uint32_t>() + nslots;
+    SGB_TRY(scan_exclusive_u32(per.as<uint32_t>(), off.as<uint32_t>(), nslots, total, &g->scratch[6], s));
+    SGB_TRY(g->hscratch.ensure(64));
+    SGB_CUDA(cudaMemcpyAsync(g->hscratch.p, total, 4, cudaMemcpyDeviceToHost, s));
+    SGB_CUDA(cudaStreamSynchronize(s));
+    const int64_t add = *(uint32_t*)g->hscratch.p;
+    if (add == 0) return SGB_OK;
+    SGB_TRY(g->pend_lin.reserve((size_t)(g->npend + add) * 8));
+    PoolCopy pc{};
+    pc.nprop = g->nprop;
+    for (int p = 0; p < g->nprop; ++p) {
+        const int es = elem_size(g->ptype[p]);
+        SGB_TRY(g->pend_val[p].reserve((size_t)(g->npend + add) * es));
+        pc.src[p] = values ? (const unsigned char*)values[p] : nullptr;
+        if (pc.src[p]) g->pend_has[p] = true;
+        pc.dst[p] = g->pend_val[p].as<unsigned char>() + (size_t)g->npend * es;
+        pc.es[p] = es;
+        pc.bck[p] = bck_pattern(g, p);
+    }
+    k_block_emit<<<wblocks, 256, 0, s>>>(cnt.as<uint32_t>(), npools, nslot, keys, masks, off.as<uint32_t>(), g->geo,
+                                         g->pend_lin.as<int64_t>() + g->npend, pc, g->err.as<unsigned>());
     SGB_CUDA(cudaGetLastError());
     g->npend += add;
     return SGB_OK;

@@ -145,6 +145,20 @@ class SparseGridGpu:
                                            _stream(stream)), "sgb_insert_pools")
         self._keep = (cnt, l, keep)
 
+    def insert_blocks(self, counts: torch.Tensor, keys: torch.Tensor, values, masks: torch.Tensor,
+                      stream=None) -> None:
+        """Stage chunk slots written through insertBlock: counts int32 [npools], keys int64
+        [npools, nslot], values[p] [npools, nslot, bs] or None, masks uint8 [npools, nslot, bs]."""
+        dev = f"cuda:{self.device}"
+        cnt = counts.to(device=dev, dtype=torch.int32).contiguous()
+        k = keys.to(device=dev, dtype=torch.int64).contiguous()
+        m = masks.to(device=dev, dtype=torch.uint8).contiguous()
+        npools, nslot = k.shape
+        ptrs, keep = self._values(values)
+        L.check(self._lib.sgb_insert_blocks(self._h, npools, nslot, cnt.data_ptr(), k.data_ptr(), ptrs, m.data_ptr(),
+                                            _stream(stream)), "sgb_insert_blocks")
+        self._keep_blocks = (cnt, k, m, keep)
+
     def view(self, nn: int = L.NN_STAR, stream=None) -> dict:
         """Device view for user kernels (toKernel): sizes and raw device pointers (sgb_get_view)."""
         v = _View()

@@ -139,6 +139,214 @@ __global__ void remove_even(Ker g) {
     if (in_shape(x, y, z) && (x + y + z) % 2 == 0) g.remove(grid_key_dx<3, int>({x, y, z}));
 }
 
+// insertBlock as the reference's insertSphere3D (SparseGridGpu_testKernels.cuh:144-200): one CTA
+// per 8^3 block of a box starting at `start`, every thread one point; blocks holding a point of the
+// shell r2 <= r < r1 around the box centre take a chunk slot and write their points
+template <unsigned p, typename Ker>
+__global__ void insert_sphere_blocks(Ker sg, grid_key_dx<3, int> start, float r1, float r2, float value) {
+    constexpr unsigned pMask = Ker::pMask;
+    grid_key_dx<3, long> blk({(long)(blockIdx.x + start.get(0) / 8), (long)(blockIdx.y + start.get(1) / 8),
+                              (long)(blockIdx.z + start.get(2) / 8)});
+    const unsigned offset = threadIdx.x;
+    __shared__ bool is_block_empty;
+    if (threadIdx.x == 0) is_block_empty = true;
+    sg.init();
+    const auto blockId = sg.getBlockLinId(blk);
+    const grid_key_dx<3, long> keyg = sg.getGlobalCoord(blk, offset);
+    const long x = keyg.get(0) - (start.get(0) + gridDim.x / 2 * 8);
+    const long y = keyg.get(1) - (start.get(1) + gridDim.y / 2 * 8);
+    const long z = keyg.get(2) - (start.get(2) + gridDim.z / 2 * 8);
+    const float radius = sqrtf((float)(x * x + y * y + z * z));
+    const bool is_active = radius < r1 && radius >= r2;
+    if (is_active) is_block_empty = false;
+    __syncthreads();
+    if (!is_block_empty) {
+        auto ec = sg.insertBlock(blockId);
+        if (is_active) {
+            ec.template get<p>()[offset] = value + (float)(keyg.get(0) + 3 * keyg.get(1));
+            BlockMapGpu_ker<>::setExist(ec.template get<pMask>()[offset]);
+        }
+    }
+    __syncthreads();
+    sg.flush_block_insert();
+}
+
+// insertBlock with two properties per point as insertConstantValue2 (SparseGridGpu_tests.cu:14-43)
+template <unsigned p1, unsigned p2, typename Ker>
+__global__ void insert_constant_blocks(Ker sg, float value) {
+    constexpr unsigned pMask = Ker::pMask;
+    sg.init();
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y,
+              z = blockIdx.z * blockDim.z + threadIdx.z;
+    grid_key_dx<3, int> coord({x, y, z});
+    const int64_t pos = sg.getLinId(coord);
+    const int64_t dataBlockId = pos / 512;
+    const unsigned offset = (unsigned)(pos % 512);
+    auto ec = sg.insertBlock(dataBlockId);  // thread (0, 0, 0) takes the CTA's slot
+    ec.template get<p1>()[offset] = value;
+    ec.template get<p2>()[offset] = value;
+    BlockMapGpu_ker<>::setExist(ec.template get<pMask>()[offset]);
+    __syncthreads();
+    sg.flush_block_insert();
+}
+
+// ---- user stencil functors with the reference's contract (applyStencils<S> with any S)
+// BoundaryStencilSetXRescaled (SparseGridGpu_testKernels.cuh:36-80), in 3-D
+template <unsigned dim, unsigned p_src, unsigned p_dst, typename ScalarT = float>
+struct UserBoundarySetXRescaled {
+    typedef NNStar<dim> stencil_type;
+    static constexpr unsigned supportRadius = 1;
+    template <typename SparseGridT, typename DataBlockWrapperT>
+    static inline __device__ void stencil(SparseGridT& sparseGrid, const unsigned dataBlockId,
+                                          openfpm::sparse_index<unsigned> dataBlockIdPos, unsigned offset,
+                                          grid_key_dx<dim, int>& pointCoord, DataBlockWrapperT& dataBlockLoad,
+                                          DataBlockWrapperT& dataBlockStore, unsigned char curMask, ScalarT minX,
+                                          ScalarT maxX, ScalarT minValue, ScalarT maxValue) {
+        if (curMask == mask_sparse::EXIST_AND_PADDING) {
+            const ScalarT x = pointCoord.get(0);
+            auto value = maxValue * (x - minX) / (maxX - minX - 1);
+            if (x < minX) value = minValue;
+            else if (x > maxX) value = maxValue;
+            dataBlockStore.template get<p_dst>()[offset] = value;
+        }
+    }
+};
+
+// HeatStencil (SparseGridGpu_util_test.cuh:201-290) as user code: loadGhostBlock, enlarged-block
+// indexing, storeBlock
+template <unsigned dim, unsigned p_src, unsigned p_dst>
+struct UserHeatStencil {
+    typedef NNStar<dim> stencil_type;
+    static constexpr unsigned supportRadius = 1;
+    template <typename SparseGridT, typename DataBlockWrapperT>
+    static inline __device__ void stencil(SparseGridT& sparseGrid, const unsigned dataBlockId,
+                                          const openfpm::sparse_index<unsigned> dataBlockIdPos, const unsigned offset,
+                                          const grid_key_dx<dim, int>& pointCoord,
+                                          const DataBlockWrapperT& dataBlockLoad, DataBlockWrapperT& dataBlockStore,
+                                          unsigned char curMask, float dt) {
+        typedef typename SparseGridT::AggregateBlockType AggregateT;
+        typedef ScalarTypeOf<AggregateT, p_src> ScalarT;
+        constexpr unsigned enlargedBlockSize = IntPow<SparseGridT::getBlockEdgeSize() + 2 * supportRadius, dim>::value;
+        __shared__ ScalarT enlargedBlock[enlargedBlockSize];
+        sparseGrid.template loadGhostBlock<p_src>(dataBlockLoad, dataBlockIdPos, enlargedBlock);
+        __syncthreads();
+        decltype(sparseGrid.getLinIdInEnlargedBlock(0)) linId = 0;
+        ScalarT res = 0;
+        if ((curMask & mask_sparse::EXIST) && !(curMask & mask_sparse::PADDING)) {
+            const auto coord = sparseGrid.getCoordInEnlargedBlock(offset);
+            linId = sparseGrid.getLinIdInEnlargedBlock(offset);
+            ScalarT cur = enlargedBlock[linId];
+            ScalarT laplacian = -2.0 * dim * cur;
+            for (int d = 0; d < dim; ++d) {
+                auto nPlusId = sparseGrid.getNeighbourLinIdInEnlargedBlock(coord, d, 1);
+                auto nMinusId = sparseGrid.getNeighbourLinIdInEnlargedBlock(coord, d, -1);
+                ScalarT neighbourPlus = enlargedBlock[nPlusId];
+                ScalarT neighbourMinus = enlargedBlock[nMinusId];
+                laplacian += neighbourMinus + neighbourPlus;
+            }
+            res = cur + dt * laplacian;
+        }
+        __syncthreads();
+        if ((curMask & mask_sparse::EXIST) && !(curMask & mask_sparse::PADDING)) enlargedBlock[linId] = res;
+        __syncthreads();
+        sparseGrid.template storeBlock<p_dst>(dataBlockStore, enlargedBlock);
+    }
+};
+
+// Conv3x3x3 (SparseGridGpu_tests.cu:887-952) as user code over an NNFull tile
+template <unsigned dim, unsigned p_src, unsigned p_dst>
+struct UserConv3x3x3 {
+    typedef NNFull<dim> stencil_type;
+    static constexpr unsigned supportRadius = 1;
+    template <typename SparseGridT, typename DataBlockWrapperT>
+    static inline __device__ void stencil(SparseGridT& sparseGrid, const unsigned dataBlockId,
+                                          openfpm::sparse_index<unsigned> dataBlockIdPos, unsigned offset,
+                                          grid_key_dx<dim, int>& pointCoord, DataBlockWrapperT& dataBlockLoad,
+                                          DataBlockWrapperT& dataBlockStore, unsigned char curMask, conv_coeff& cc) {
+        typedef typename SparseGridT::AggregateBlockType AggregateT;
+        typedef ScalarTypeOf<AggregateT, p_src> ScalarT;
+        constexpr unsigned enlargedBlockSize = IntPow<SparseGridT::getBlockEdgeSize() + 2 * supportRadius, dim>::value;
+        __shared__ ScalarT enlargedBlock[enlargedBlockSize];
+        sparseGrid.template loadGhostBlock<p_src>(dataBlockLoad, dataBlockIdPos, enlargedBlock);
+        __syncthreads();
+        if ((curMask & mask_sparse::EXIST) && !(curMask & mask_sparse::PADDING)) {
+            const auto coord = sparseGrid.getCoordInEnlargedBlock(offset);
+            ScalarT tot = 0.0;
+            for (int i = 0; i < dim; ++i)
+                for (int j = 0; j < dim; ++j)
+                    for (int k = 0; k < dim; ++k) {
+                        grid_key_dx<dim, int> key;
+                        key.set_d(0, i - 1);
+                        key.set_d(1, j - 1);
+                        key.set_d(2, k - 1);
+                        auto nPlusId = sparseGrid.getNeighbourLinIdInEnlargedBlock(coord, key);
+                        tot += enlargedBlock[nPlusId] * cc.coeff[i][j][k];
+                    }
+            dataBlockStore.template get<p_dst>()[offset] = tot;
+        }
+    }
+};
+
+// Conv3x3x3_noshared (SparseGridGpu_tests.cu:955-1010) as user code: getNNPoint + get
+template <unsigned dim, unsigned p_src, unsigned p_dst>
+struct UserConv3x3x3NoShared {
+    typedef NNFull<dim> stencil_type;
+    static constexpr unsigned supportRadius = 1;
+    template <typename SparseGridT, typename DataBlockWrapperT>
+    static inline __device__ void stencil(SparseGridT& sparseGrid, const unsigned dataBlockId,
+                                          openfpm::sparse_index<unsigned> dataBlockIdPos, unsigned offset,
+                                          grid_key_dx<dim, int>& pointCoord, DataBlockWrapperT& dataBlockLoad,
+                                          DataBlockWrapperT& dataBlockStore, unsigned char curMask, conv_coeff& cc) {
+        typedef typename SparseGridT::AggregateBlockType AggregateT;
+        typedef ScalarTypeOf<AggregateT, p_src> ScalarT;
+        if ((curMask & mask_sparse::EXIST) && !(curMask & mask_sparse::PADDING)) {
+            ScalarT tot = 0.0;
+            for (int i = 0; i < dim; ++i)
+                for (int j = 0; j < dim; ++j)
+                    for (int k = 0; k < dim; ++k) {
+                        grid_key_dx<dim, int> key;
+                        key.set_d(0, k - 1);
+                        key.set_d(1, j - 1);
+                        key.set_d(2, i - 1);
+                        block_offset<int> pos = sparseGrid.template getNNPoint<stencil_type>(dataBlockIdPos, offset, key);
+                        tot += sparseGrid.template get<p_src>(pos) * cc.coeff[i][j][k];
+                    }
+            dataBlockStore.template get<p_dst>()[offset] = tot;
+        }
+    }
+};
+
+// loadGhostBlock with a mask tile: writes into p_dst, at every existing point, the number of its 26
+// halo neighbours whose mask byte is set (exercises the NNStar edge / corner rule when run on NNStar)
+template <unsigned p_src, unsigned p_dst>
+struct UserCountTile {
+    typedef NNStar<3> stencil_type;
+    template <typename SparseGridT, typename DataBlockWrapperT>
+    static inline __device__ void stencil(SparseGridT& sparseGrid, const unsigned, openfpm::sparse_index<unsigned> pos,
+                                          unsigned offset, grid_key_dx<3, int>&, DataBlockWrapperT& load,
+                                          DataBlockWrapperT& store, unsigned char curMask) {
+        __shared__ float tile[1000];
+        __shared__ unsigned char mtile[1000];
+        sparseGrid.template loadGhostBlock<p_src>(load, pos, tile, mtile);
+        __syncthreads();
+        if (curMask & 1) {
+            const auto c = sparseGrid.getCoordInEnlargedBlock(offset);
+            float acc = 0;
+            for (int dz = -1; dz <= 1; ++dz)
+                for (int dy = -1; dy <= 1; ++dy)
+                    for (int dx = -1; dx <= 1; ++dx) {
+                        grid_key_dx<3, int> o;
+                        o.set_d(0, dx);
+                        o.set_d(1, dy);
+                        o.set_d(2, dz);
+                        const unsigned id = sparseGrid.getNeighbourLinIdInEnlargedBlock(c, o);
+                        acc += (mtile[id] & 1) ? tile[id] : 0.0f;
+                    }
+            store.template get<p_dst>()[offset] = acc;
+        }
+    }
+};
+
 int main() {
     const size_t sz[3] = {N, N, N};
     gpu::ofp_context_t ctx;
@@ -549,6 +757,196 @@ int main() {
                 all.find("POINTS " + std::to_string(npts) + " float") != std::string::npos;
         std::remove(vtk.c_str());
         CHECK(wrote, "write_vtk");
+    }
+
+    // ---------------------------------------------------------------- insertBlock (chunk slots)
+    {
+        // the sphere shell of insertSphere3D written through insertBlock, against the same points
+        // through the staged C ABI insert
+        Grid6 bg(sz), rg(sz);
+        bg.setBackgroundValue<0>(0.0f);
+        rg.setBackgroundValue<0>(0.0f);
+        const dim3 gsz(N / 8, N / 8, N / 8);
+        bg.setGPUInsertBuffer(gsz, dim3(1, 1, 1));
+        insert_sphere_blocks<0><<<gsz, 512>>>(bg.toKernel(), grid_key_dx<3, int>({0, 0, 0}), 28.0f, 12.0f, 0.5f);
+        bg.flush<smax_<0>>(ctx, FLUSH_ON_DEVICE);
+        std::vector<int32_t> sc;
+        std::vector<float> sv;
+        for (int bz = 0; bz < N / 8; ++bz)
+            for (int by = 0; by < N / 8; ++by)
+                for (int bx = 0; bx < N / 8; ++bx)
+                    for (int o = 0; o < 512; ++o) {
+                        const long x = bx * 8 + o % 8, y = by * 8 + (o / 8) % 8, z = bz * 8 + o / 64;
+                        const long dx = x - N / 2, dy = y - N / 2, dz = z - N / 2;
+                        const float r = sqrtf((float)(dx * dx + dy * dy + dz * dz));
+                        if (r < 28.0f && r >= 12.0f) {
+                            sc.insert(sc.end(), {(int32_t)x, (int32_t)y, (int32_t)z});
+                            sv.push_back(0.5f + (float)(x + 3 * y));
+                        }
+                    }
+        int32_t* dc;
+        float* dv;
+        cudaMalloc(&dc, sc.size() * 4);
+        cudaMalloc(&dv, sv.size() * 4);
+        cudaMemcpy(dc, sc.data(), sc.size() * 4, cudaMemcpyHostToDevice);
+        cudaMemcpy(dv, sv.data(), sv.size() * 4, cudaMemcpyHostToDevice);
+        const void* vals[6] = {dv, nullptr, nullptr, nullptr, nullptr, nullptr};
+        check(sgb_insert(rg.handle(), (int64_t)sv.size(), dc, vals, nullptr), "sgb_insert");
+        int ops[6] = {SGB_OP_MAX, SGB_OP_NONE, SGB_OP_NONE, SGB_OP_NONE, SGB_OP_NONE, SGB_OP_NONE};
+        check(sgb_flush(rg.handle(), ops, nullptr), "sgb_flush");
+        cudaDeviceSynchronize();
+        cudaFree(dc);
+        cudaFree(dv);
+        HostMap A = download(bg.handle(), 6), B = download(rg.handle(), 6);
+        CHECK(!A.keys.empty() && A.keys == B.keys && A.mask == B.mask && same(A, 0, B, 0, existing) &&
+                  bg.countExistingElements() == sv.size(),
+              "insertBlock_sphere_shell");
+
+        // insertConstantValue2: two properties through one chunk slot per CTA, twice (the second
+        // flush merges into the existing chunks with smax_)
+        Grid6 cg(sz);
+        cg.setGPUInsertBuffer(gsz, dim3(1, 1, 1));
+        insert_constant_blocks<0, 2><<<gsz, dim3(8, 8, 8)>>>(cg.toKernel(), 3.0f);
+        cg.flush<smax_<0>, smax_<2>>(ctx, FLUSH_ON_DEVICE);
+        insert_constant_blocks<0, 2><<<gsz, dim3(8, 8, 8)>>>(cg.toKernel(), 2.0f);
+        cg.flush<smax_<0>, smax_<2>>(ctx, FLUSH_ON_DEVICE);
+        cg.deviceToHost<0, 2>();
+        bool all3 = cg.countExistingElements() == (size_t)N * N * N;
+        for (int z = 0; z < N && all3; z += 3)
+            for (int y = 0; y < N; y += 5)
+                for (int x = 0; x < N; ++x) {
+                    const grid_key_dx<3, int> k({x, y, z});
+                    all3 = all3 && cg.get<0>(k) == 3.0f && cg.get<2>(k) == 3.0f;
+                }
+        CHECK(all3, "insertBlock_constant_two_properties");
+    }
+
+    // ---------------------------------------------------------------- user stencil functors
+    {
+        // testStencilHeat (SparseGridGpu_tests.cu:472-518) in 3-D: a 16^3 grid of 2^3 chunks, padding
+        // points set to 10 x / 15 by a boundary functor, then 1000 pairs of heat steps of the
+        // reference's HeatStencil written as user code: the interior relaxes to the linear profile
+        typedef SparseGridGpu<3, aggregate<float, float>, 8> Grid2;
+        const size_t s16[3] = {16, 16, 16};
+        Grid2 hg(s16), fg(s16);
+        for (Grid2* g : {&hg, &fg}) {
+            g->setBackgroundValue<0>(0.0f);
+            g->setGPUInsertBuffer(dim3(2, 2, 2), dim3(1, 1, 1));
+            insert_constant_blocks<0, 1><<<dim3(2, 2, 2), dim3(8, 8, 8)>>>(g->toKernel(), 0.0f);
+            g->flush<smax_<0>, smax_<1>>(ctx, FLUSH_ON_DEVICE);
+            g->findNeighbours();
+            g->tagBoundaries(ctx);
+            g->applyStencils<UserBoundarySetXRescaled<3, 0, 0>>(g->getBox(), STENCIL_MODE_INPLACE, 0.0, 16, 0.0, 10.0);
+        }
+        for (int it = 0; it < 1000; ++it) {
+            hg.applyStencils<UserHeatStencil<3, 0, 1>>(hg.getBox(), STENCIL_MODE_INPLACE, 0.1f);
+            hg.applyStencils<UserHeatStencil<3, 1, 0>>(hg.getBox(), STENCIL_MODE_INPLACE, 0.01f);
+            if (it < 50) {  // the library's fixed-function HeatStencil on the twin grid
+                fg.applyStencils<HeatStencil<3, 0, 1>>(fg.getBox(), STENCIL_MODE_INPLACE, 0.1f);
+                fg.applyStencils<HeatStencil<3, 1, 0>>(fg.getBox(), STENCIL_MODE_INPLACE, 0.01f);
+            }
+            if (it == 49) {
+                HostMap a = download(hg.handle(), 2), b = download(fg.handle(), 2);
+                CHECK(same(a, 0, b, 0, existing) && same(a, 1, b, 1, existing), "user_HeatStencil_equals_fixed_50");
+            }
+        }
+        hg.deviceToHost<0, 1>();
+        bool prof = hg.countExistingElements() == 4096;
+        for (int z = 0; z < 16; ++z)
+            for (int y = 0; y < 16; ++y)
+                for (int x = 0; x < 16; ++x) {
+                    const float expect = 10.0f * x / 15.0f;
+                    prof = prof && std::fabs(hg.get<1>(grid_key_dx<3, int>({x, y, z})) - expect) < 1e-2f;
+                }
+        CHECK(prof, "testStencilHeat_3d_user_functor_linear_profile");
+
+        // testStencil_lap_simplified (SparseGridGpu_tests.cu:520-566) in 3-D with conv_cross lambdas
+        Grid2 lg(s16);
+        lg.setBackgroundValue<0>(0.0f);
+        lg.setGPUInsertBuffer(dim3(2, 2, 2), dim3(1, 1, 1));
+        insert_constant_blocks<0, 1><<<dim3(2, 2, 2), dim3(8, 8, 8)>>>(lg.toKernel(), 0.0f);
+        lg.flush<smax_<0>, smax_<1>>(ctx, FLUSH_ON_DEVICE);
+        lg.findNeighbours();
+        lg.tagBoundaries(ctx);
+        lg.applyStencils<UserBoundarySetXRescaled<3, 0, 0>>(lg.getBox(), STENCIL_MODE_INPLACE, 0.0, 16, 0.0, 10.0);
+        for (int it = 0; it < 1000; ++it) {
+            lg.conv_cross<0, 1, 1>({0, 0, 0}, {16, 16, 16}, [] __device__(float& u, cross_stencil<3, float>& cs) {
+                return u + (cs.xm[0] + cs.xp[0] + cs.xm[1] + cs.xp[1] + cs.xm[2] + cs.xp[2] - 6.0f * u) * 0.1f;
+            });
+            lg.conv_cross<1, 0, 1>({0, 0, 0}, {16, 16, 16}, [] __device__(float& u, cross_stencil<3, float>& cs) {
+                return u + (cs.xm[0] + cs.xp[0] + cs.xm[1] + cs.xp[1] + cs.xm[2] + cs.xp[2] - 6.0f * u) * 0.1f;
+            });
+        }
+        lg.deviceToHost<0, 1>();
+        bool lap = true;
+        for (int z = 0; z < 16; ++z)
+            for (int y = 0; y < 16; ++y)
+                for (int x = 0; x < 16; ++x)
+                    lap = lap && std::fabs(lg.get<1>(grid_key_dx<3, int>({x, y, z})) - 10.0f * x / 15.0f) < 1e-2f;
+        CHECK(lap, "testStencil_lap_simplified_3d_conv_cross");
+
+        // Conv3x3x3 and Conv3x3x3_noshared as user functors against the library's kernels, on the
+        // shell grid (holes, absent neighbour chunks), bit for bit at the active points
+        Grid6 cg(sz);
+        cg.setBackgroundValue<0>(0.0f);
+        cg.setGPUInsertBuffer(dim3(N / 8, N / 8, N / 8), dim3(1024, 1, 1));
+        insert_shape<0><<<dim3(N / 8, N / 8, N / 8), dim3(8, 8, 8)>>>(cg.toKernel());
+        cg.flush<smax_<0>>(ctx, FLUSH_ON_DEVICE);
+        cg.setNNType<NNFull<3>>();
+        cg.tagBoundaries<NNFull<3>>(ctx, No_check(), tag_boundaries::CALCULATE_EXISTING_POINTS);
+        conv_coeff cc;
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j)
+                for (int k = 0; k < 3; ++k) cc.coeff[i][j][k] = 0.01f * (float)(1 + i + 3 * j + 9 * k);
+        cg.applyStencils<UserConv3x3x3<3, 0, 1>>(cg.getBox(), STENCIL_MODE_INPLACE, cc);
+        cg.applyStencils<Conv3x3x3<3, 0, 2>>(cg.getBox(), STENCIL_MODE_INPLACE, cc);
+        cg.applyStencils<UserConv3x3x3NoShared<3, 0, 3>>(cg.getBox(), STENCIL_MODE_INPLACE_NO_SHARED, cc);
+        cg.applyStencils<Conv3x3x3_noshared<3, 0, 4>>(cg.getBox(), STENCIL_MODE_INPLACE_NO_SHARED, cc);
+        cudaDeviceSynchronize();
+        HostMap C = download(cg.handle(), 6);
+        size_t nact = 0;
+        for (uint8_t m : C.mask) nact += active(m);
+        CHECK(nact > 1000 && same(C, 1, C, 2, active), "user_Conv3x3x3_equals_fixed");
+        CHECK(same(C, 3, C, 4, active), "user_Conv3x3x3_noshared_equals_fixed");
+
+        // loadGhostBlock with a mask tile on NNStar: the edge / corner halo cells come from neighbour 0
+        // (the -x chunk) at the wrapped coordinate, as the reference's ghost-layer map gives them
+        cg.setNNType<NNStar<3>>();
+        cg.applyStencils<UserCountTile<0, 5>>(cg.getBox(), STENCIL_MODE_INPLACE);
+        cudaDeviceSynchronize();
+        HostMap T = download(cg.handle(), 6);
+        const int bz8 = N / 8;
+        auto pos_of = [&](int bx, int by, int bz) -> long {
+            if (bx < 0 || by < 0 || bz < 0 || bx >= bz8 || by >= bz8 || bz >= bz8) return -1;
+            const long key = bx + bz8 * (by + (long)bz8 * bz);
+            for (size_t i = 0; i < T.keys.size(); ++i)
+                if (T.keys[i] == key) return (long)i;
+            return -1;
+        };
+        bool rule = true;
+        for (size_t c = 0; c < T.keys.size() && rule; ++c) {
+            const int bx = (int)(T.keys[c] % bz8), by = (int)((T.keys[c] / bz8) % bz8), bz = (int)(T.keys[c] / (bz8 * bz8));
+            for (int o = 0; o < 512; ++o) {
+                if (!(T.mask[c * 512 + o] & 1)) continue;
+                const int lx = o % 8, ly = (o / 8) % 8, lz = o / 64;
+                float acc = 0;
+                for (int dz = -1; dz <= 1; ++dz)
+                    for (int dy = -1; dy <= 1; ++dy)
+                        for (int dx = -1; dx <= 1; ++dx) {
+                            const int tx = lx + dx, ty = ly + dy, tz = lz + dz;
+                            const int ox = tx < 0 ? -1 : (tx > 7 ? 1 : 0), oy = ty < 0 ? -1 : (ty > 7 ? 1 : 0),
+                                      oz = tz < 0 ? -1 : (tz > 7 ? 1 : 0);
+                            const int nout = (ox != 0) + (oy != 0) + (oz != 0);
+                            long src = (long)c;
+                            if (nout == 1) src = pos_of(bx + ox, by + oy, bz + oz);
+                            else if (nout > 1) src = pos_of(bx - 1, by, bz);
+                            const int w = ((tx + 8) % 8) + 8 * (((ty + 8) % 8) + 8 * ((tz + 8) % 8));
+                            acc += (src >= 0 && (T.mask[src * 512 + w] & 1)) ? T.data[0][src * 512 + w] : 0.0f;
+                        }
+                if (std::memcmp(&acc, &T.data[5][c * 512 + o], 4) != 0) rule = false;
+            }
+        }
+        CHECK(rule, "loadGhostBlock_nnstar_edge_corner_rule");
     }
 
     int st = sgb_check_device_errors(grid.handle(), nullptr);

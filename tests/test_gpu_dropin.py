@@ -106,3 +106,60 @@ def test_view_describes_the_block_map(sgb):
         exp[exp == v["n"]] = -1
         used = ref != -1 if nn == O.NN_STAR else np.ones_like(ref, bool)
         assert np.array_equal(t[used], exp[used])
+
+
+@pytest.mark.parametrize("edge", [8, 4])
+@pytest.mark.parametrize("op", ["sRight_", "sadd_", "smax_"])
+def test_insert_blocks_matches_chunk_slot_flush(sgb, edge, op):
+    """Chunk slots written through insertBlock (BlockMapGpu_ker.cuh:199-227), flushed onto a map
+    that already holds points: bit-exact against the oracle's chunk-slot flush
+    (segreduce_total / solve_conflicts restated), duplicates across slots and pools included."""
+    rng = np.random.default_rng(31 + edge)
+    size = (48, 40, 56)
+    bs = edge ** 3
+    bsz = [(s + edge - 1) // edge for s in size]
+    nkeys = bsz[0] * bsz[1] * bsz[2]
+    npools, nslot = 13, 5
+    counts = rng.integers(1, nslot + 1, npools).astype(np.int32)
+    keys = rng.integers(0, nkeys, (npools, nslot)).astype(np.int64)
+    keys[3:6, :2] = keys[0, 0]  # the same chunk in several slots and pools
+    masks = (rng.random((npools, nslot, bs)) < 0.3).astype(np.uint8)
+    masks[..., 0] = 1  # every slot holds at least one point
+    v0 = rng.random((npools, nslot, bs)).astype(np.float32)
+    v1 = rng.integers(-500, 500, (npools, nslot, bs)).astype(np.int32)
+    ops = [op, op]
+    oops = [getattr(O, {"sRight_": "OP_RIGHT", "sadd_": "OP_ADD", "smax_": "OP_MAX"}[op])] * 2
+
+    g = sgb.SparseGridGpu(size, ["f32", "i32"], edge=edge)
+    o = O.OracleGrid(size, edge=edge, ptypes=[O.T_F32, O.T_I32])
+    # points already in the map, so that slots merge with old chunks
+    pts = rng.integers(0, size, size=(3000, 3)).astype(np.int64)
+    pv = [rng.random(3000).astype(np.float32), rng.integers(-9, 9, 3000).astype(np.int32)]
+    g.insert(torch.from_numpy(pts).cuda(), [torch.from_numpy(x).cuda() for x in pv])
+    g.flush(["smax_", "smax_"])
+    o.insert_flush(pts, pv, [O.OP_MAX, O.OP_MAX])
+
+    g.insert_blocks(torch.from_numpy(counts), torch.from_numpy(keys), [torch.from_numpy(v0), torch.from_numpy(v1)],
+                    torch.from_numpy(masks))
+    g.flush(ops)
+    sel = np.concatenate([np.arange(c) + i * nslot for i, c in enumerate(counts)])
+    o.flush_chunks(keys.reshape(-1)[sel], [v0.reshape(-1, bs)[sel].reshape(-1), v1.reshape(-1, bs)[sel].reshape(-1)],
+                   masks.reshape(-1, bs)[sel].reshape(-1), oops)
+    kg, dg, mg = g.deviceToHost()
+    ko, do, mo = o.export()
+    n = len(ko)
+    assert np.array_equal(kg, ko) and np.array_equal(mg[: n * bs], mo[: n * bs])
+    ex = (mo[: n * bs] & 1).astype(bool)
+    for p in range(2):
+        assert np.array_equal(dg[p][: n * bs][ex].view(np.uint8), do[p][: n * bs][ex].view(np.uint8)), f"prop {p}"
+    g.check_device_errors()
+
+
+def test_insert_blocks_overflow_is_reported(sgb):
+    g = sgb.SparseGridGpu((16, 16, 16), ["f32"], edge=8)
+    masks = torch.ones((1, 2, 512), dtype=torch.uint8)
+    g.insert_blocks(torch.tensor([3], dtype=torch.int32), torch.zeros((1, 2), dtype=torch.int64),
+                    [torch.ones((1, 2, 512))], masks)
+    with pytest.raises(sgb.SgbError, match="insert pool"):
+        g.flush(["smax_"])
+    g.check_device_errors()
