@@ -444,7 +444,7 @@ def run_insert1024(args, dist: Dist):
     from openfpm_data_b200 import workloads as W
     torch.cuda.set_device(dist.local)
     nsteps = args.steps if args.steps <= 200 else 20
-    nwarm = max(3, min(args.warmup, 5))
+    nwarm = max(3, min(args.warmup, 8))
     size = (1024, 1024, 1024)
     g = sgb.SparseGridGpu(size, ["f32", "i32", "f32"], edge=8, device=dist.local)
     coeff = [1.0 / 27.0] * 27
@@ -960,7 +960,7 @@ def _sub_records(args, dist: Dist) -> dict:
     import copy
     plans = [
         ("heat128", run_heat128, dict(steps=100, warmup=5)),
-        ("insert1024", run_insert1024, dict(steps=10, warmup=3)),
+        ("insert1024", run_insert1024, dict(steps=10, warmup=8)),
         ("batched256", run_batched256, dict(steps=4, warmup=3)),
         ("served_2000rps", run_served, dict(steps=1, warmup=3, serve_rate=2000.0, serve_seconds=args.sub_serve_seconds,
                                             plain_sample=24)),

@@ -431,7 +431,10 @@ int sgb_batch_add(sgb_batch* b, sgb_grid* g, int kind, const int* src, const int
 /* Drop a slot; its chunks are compacted away before the next step. */
 int sgb_batch_remove(sgb_batch* b, int slot, sgb_stream s);
 /* Advance the batch by nsteps global steps: one persistent launch per step
- * over all chunks, captured as one CUDA graph when use_graph != 0. */
+ * over all chunks, captured as one CUDA graph when use_graph != 0.  The batch
+ * keeps the instantiated graph and updates it in place on the next call with
+ * the same nsteps.  The call returns without waiting for the GPU: the steps
+ * run on stream s in order with the batch's other calls on that stream. */
 int sgb_batch_step(sgb_batch* b, int nsteps, int use_graph, sgb_stream s);
 /* Steps a slot has done so far (<= its nsteps). */
 int sgb_batch_slot_steps(const sgb_batch* b, int slot, int64_t* done);
@@ -443,6 +446,14 @@ int sgb_batch_extract(sgb_batch* b, int slot, sgb_grid* g, int* final_is_dst, sg
  * holding the state after the steps the slot has done. */
 int sgb_batch_read(sgb_batch* b, int slot, int64_t* keys_host, uint8_t* mask_host, float* const* fields_host,
                    int64_t* nchunks, sgb_stream s);
+/* sgb_batch_read without the host wait (no reference counterpart; for a
+ * serving loop that keeps the GPU busy): the copies are queued on stream s,
+ * in order with the batch's steps; the host buffers (pinned for an
+ * asynchronous copy) hold the slot's state once the stream has reached them.
+ * A removed slot's data stays in place until a later call compacts the batch
+ * on the same stream, so a read queued before that compaction is safe. */
+int sgb_batch_read_async(sgb_batch* b, int slot, int64_t* keys_host, uint8_t* mask_host, float* const* fields_host,
+                         int64_t* nchunks, sgb_stream s);
 int sgb_batch_info(const sgb_batch* b, int* ngrids, int64_t* nchunks, int64_t* bytes);
 /* Launch configuration of the batched kernels (as sgb_set_launch_config). */
 int sgb_batch_set_launch_config(sgb_batch* b, int ctas_per_sm, int stages);

@@ -83,6 +83,7 @@ SIGNATURES = {
     "sgb_batch_slot_steps": (_i32, [_vp, _i32, _vp]),
     "sgb_batch_extract": (_i32, [_vp, _i32, _vp, _vp, _vp]),
     "sgb_batch_read": (_i32, [_vp, _i32, _vp, _vp, _vp, _vp, _vp]),
+    "sgb_batch_read_async": (_i32, [_vp, _i32, _vp, _vp, _vp, _vp, _vp]),
     "sgb_batch_info": (_i32, [_vp, _vp, _vp, _vp]),
     "sgb_batch_set_launch_config": (_i32, [_vp, _i32, _i32]),
 }

@@ -38,6 +38,15 @@ struct sgb_batch {
     bool holes = false;    // removed slots to compact
     int num_sms = 148, ctas_per_sm = 0, stages = 0;  // 0: automatic
     sgb::DevBuf err;
+    // the instantiated graph of the last sgb_batch_step call with use_graph, updated in place for the
+    // next call of the same step count (kernel arguments change, the graph's shape does not)
+    cudaGraphExec_t exec = nullptr;
+    int exec_nsteps = -1;
+    // pinned staging of the grids table: two buffers used in turn, each free once its copy event fired
+    void* grids_host[2] = {nullptr, nullptr};
+    size_t grids_host_bytes[2] = {0, 0};
+    cudaEvent_t grids_done[2] = {nullptr, nullptr};
+    int grids_turn = 0;
 };
 
 namespace sgb {
@@ -119,14 +128,28 @@ static int batch_compact(sgb_batch* b, cudaStream_t s) {
     return SGB_OK;
 }
 
+// Upload the grids table without a host wait: it is staged in one of two pinned buffers, taken in
+// turn; a buffer is rewritten only after the event recorded behind its previous copy has fired.
 static int batch_upload_grids(sgb_batch* b, cudaStream_t s) {
     if (!b->dirty) return SGB_OK;
-    std::vector<GridInfo> h(b->slots.size());
-    for (size_t i = 0; i < h.size(); ++i) h[i] = b->slots[i].gi;
-    SGB_TRY(b->grids.ensure(std::max<size_t>(1, h.size()) * sizeof(GridInfo)));
-    if (!h.empty())
-        SGB_CUDA(cudaMemcpyAsync(b->grids.p, h.data(), h.size() * sizeof(GridInfo), cudaMemcpyHostToDevice, s));
-    SGB_CUDA(cudaStreamSynchronize(s));  // h goes out of scope
+    const size_t bytes = std::max<size_t>(1, b->slots.size()) * sizeof(GridInfo);
+    SGB_TRY(b->grids.ensure(bytes));
+    const int k = b->grids_turn;
+    b->grids_turn ^= 1;
+    if (b->grids_done[k]) SGB_CUDA(cudaEventSynchronize(b->grids_done[k]));
+    else SGB_CUDA(cudaEventCreateWithFlags(&b->grids_done[k], cudaEventDisableTiming));
+    if (b->grids_host_bytes[k] < bytes) {
+        if (b->grids_host[k]) cudaFreeHost(b->grids_host[k]);
+        b->grids_host[k] = nullptr;
+        b->grids_host_bytes[k] = 0;
+        SGB_CUDA(cudaMallocHost(&b->grids_host[k], bytes * 2));
+        b->grids_host_bytes[k] = bytes * 2;
+    }
+    GridInfo* h = static_cast<GridInfo*>(b->grids_host[k]);
+    for (size_t i = 0; i < b->slots.size(); ++i) h[i] = b->slots[i].gi;
+    if (!b->slots.empty())
+        SGB_CUDA(cudaMemcpyAsync(b->grids.p, h, b->slots.size() * sizeof(GridInfo), cudaMemcpyHostToDevice, s));
+    SGB_CUDA(cudaEventRecord(b->grids_done[k], s));
     b->dirty = false;
     return SGB_OK;
 }
@@ -185,6 +208,14 @@ int sgb_batch_create(sgb_batch** out, int device) {
 int sgb_batch_destroy(sgb_batch* b) {
     if (!b) return SGB_EINVAL;
     DeviceGuard dg(b->device);
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    for (int k = 0; k < 2; ++k) {
+        if (b->grids_done[k]) {
+            cudaEventSynchronize(b->grids_done[k]);
+            cudaEventDestroy(b->grids_done[k]);
+        }
+        if (b->grids_host[k]) cudaFreeHost(b->grids_host[k]);
+    }
     for (DevBuf* d : {&b->keys, &b->mask, &b->nn, &b->gid, &b->grids, &b->keys2, &b->mask2, &b->nn2, &b->gid2, &b->err})
         d->release();
     for (int k = 0; k < 2; ++k)
@@ -304,16 +335,47 @@ int sgb_batch_step(sgb_batch* b, int nsteps, int use_graph, sgb_stream stream) {
     }
     int st;
     if (use_graph) {
+        // capture the nsteps launches, then update the cached executable graph in place (same shape:
+        // only kernel arguments differ) or instantiate a new one; the launch does not wait for the GPU
         const int64_t T0 = b->T;
-        st = run_graph(
-            [&](cudaStream_t cs) -> int {
-                for (int k = 0; k < nsteps; ++k) {
-                    int r = batch_launch(b, T0 + k, cs);
-                    if (r != SGB_OK) return r;
+        cudaStream_t cap;
+        SGB_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+        cudaGraph_t graph = nullptr;
+        st = SGB_OK;
+        cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            for (int k = 0; k < nsteps && st == SGB_OK; ++k) st = batch_launch(b, T0 + k, cap);
+            const cudaError_t e2 = cudaStreamEndCapture(cap, &graph);
+            if (st == SGB_OK && e2 != cudaSuccess) st = cuda_status(e2, "cudaStreamEndCapture");
+        } else {
+            st = cuda_status(e, "cudaStreamBeginCapture");
+        }
+        if (st == SGB_OK) {
+            bool updated = false;
+            if (b->exec && b->exec_nsteps == nsteps) {
+                cudaGraphExecUpdateResultInfo info;
+                updated = cudaGraphExecUpdate(b->exec, graph, &info) == cudaSuccess;
+                if (!updated) cudaGetLastError();  // clear the update failure; instantiate instead
+            }
+            if (!updated) {
+                if (b->exec) cudaGraphExecDestroy(b->exec);
+                b->exec = nullptr;
+                b->exec_nsteps = -1;
+                e = cudaGraphInstantiate(&b->exec, graph, 0);
+                if (e != cudaSuccess) {
+                    b->exec = nullptr;
+                    st = cuda_status(e, "cudaGraphInstantiate");
+                } else {
+                    b->exec_nsteps = nsteps;
                 }
-                return SGB_OK;
-            },
-            s);
+            }
+            if (st == SGB_OK) {
+                e = cudaGraphLaunch(b->exec, s);
+                if (e != cudaSuccess) st = cuda_status(e, "cudaGraphLaunch");
+            }
+        }
+        if (graph) cudaGraphDestroy(graph);
+        cudaStreamDestroy(cap);
     } else {
         st = SGB_OK;
         for (int k = 0; k < nsteps && st == SGB_OK; ++k) st = batch_launch(b, b->T + k, s);
@@ -367,8 +429,8 @@ int sgb_batch_info(const sgb_batch* b, int* ngrids, int64_t* nchunks, int64_t* b
 
 }  // extern "C"
 
-extern "C" int sgb_batch_read(sgb_batch* b, int slot, int64_t* keys, uint8_t* mask, float* const* fields,
-                              int64_t* nchunks, sgb_stream stream) {
+static int batch_read(sgb_batch* b, int slot, int64_t* keys, uint8_t* mask, float* const* fields, int64_t* nchunks,
+                      sgb_stream stream, bool wait) {
     if (!b || slot < 0 || slot >= (int)b->slots.size() || !b->slots[slot].live) return SGB_EINVAL;
     const auto& sl = b->slots[slot];
     cudaStream_t s = (cudaStream_t)stream;
@@ -386,6 +448,16 @@ extern "C" int sgb_batch_read(sgb_batch* b, int slot, int64_t* keys, uint8_t* ma
                     SGB_CUDA(cudaMemcpyAsync(fields[p], b->field[cur][p].as<float>() + sl.off * bs, sl.n * bs * 4,
                                              cudaMemcpyDeviceToHost, s));
     }
-    SGB_CUDA(cudaStreamSynchronize(s));
+    if (wait) SGB_CUDA(cudaStreamSynchronize(s));
     return SGB_OK;
+}
+
+extern "C" int sgb_batch_read(sgb_batch* b, int slot, int64_t* keys, uint8_t* mask, float* const* fields,
+                              int64_t* nchunks, sgb_stream stream) {
+    return batch_read(b, slot, keys, mask, fields, nchunks, stream, true);
+}
+
+extern "C" int sgb_batch_read_async(sgb_batch* b, int slot, int64_t* keys, uint8_t* mask, float* const* fields,
+                                    int64_t* nchunks, sgb_stream stream) {
+    return batch_read(b, slot, keys, mask, fields, nchunks, stream, false);
 }

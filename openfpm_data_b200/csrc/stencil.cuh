@@ -14,24 +14,38 @@ __device__ __forceinline__ bool in_box(const StencilParams& prm, int64_t cx, int
            cz >= prm.box_lo[2] && cz <= prm.box_hi[2];
 }
 
-// HeatStencil update (src/SparseGridGpu/tests/utils/SparseGridGpu_util_test.cuh:256-274):
-//   lap = (float)(-2.0*dim*cur); lap += xm + xp; lap += ym + yp; lap += zm + zp;
-//   res = cur + dt*lap  (contracted to an FMA by nvcc)
-__device__ __forceinline__ float heat_update(float cur, float xm, float xp, float ym, float yp, float zm, float zp,
-                                             float dt) {
-    float lap = __fmul_rn(-6.0f, cur);
-    lap = __fadd_rn(lap, __fadd_rn(xm, xp));
+// HeatStencil's Laplacian (src/SparseGridGpu/tests/utils/SparseGridGpu_util_test.cuh:256-274) as
+// nvcc compiles that source:
+//   ScalarT laplacian = -2.0 * dim * cur;           // a double product, narrowed to float
+//   laplacian += neighbourMinus + neighbourPlus;    // per dimension, x first
+//   res = cur + dt * laplacian;
+// -6 * cur is exact in double, so its narrowing equals a float multiply, which nvcc's default FMA
+// contraction fuses with the first add: lap = fma(-6, cur, xm + xp), then + (ym + yp), + (zm + zp),
+// and res = fma(dt, lap, cur).  (The drop-in test compiles the reference's functor and checks this
+// rounding point by point.)
+__device__ __forceinline__ float lap7_heat(float c, float xm, float xp, float ym, float yp, float zm, float zp) {
+    float lap = __fmaf_rn(-6.0f, c, __fadd_rn(xm, xp));
     lap = __fadd_rn(lap, __fadd_rn(ym, yp));
-    lap = __fadd_rn(lap, __fadd_rn(zm, zp));
-    return __fmaf_rn(dt, lap, cur);
+    return __fadd_rn(lap, __fadd_rn(zm, zp));
 }
 
-// 7-point Laplacian in HeatStencil's association order.
+__device__ __forceinline__ float heat_update(float cur, float xm, float xp, float ym, float yp, float zm, float zp,
+                                             float dt) {
+    return __fmaf_rn(dt, lap7_heat(cur, xm, xp, ym, yp, zm, zp), cur);
+}
+
+// 7-point Laplacian of the Gray-Scott update (the oracle's conv2_b definition): -6 c rounded on its own,
+// then the neighbour pairs in HeatStencil's order.
 __device__ __forceinline__ float lap7(float c, float xm, float xp, float ym, float yp, float zm, float zp) {
     float lap = __fmul_rn(-6.0f, c);
     lap = __fadd_rn(lap, __fadd_rn(xm, xp));
     lap = __fadd_rn(lap, __fadd_rn(ym, yp));
     return __fadd_rn(lap, __fadd_rn(zm, zp));
+}
+
+template <int KIND>
+__device__ __forceinline__ float lap7k(float c, float xm, float xp, float ym, float yp, float zm, float zp) {
+    return KIND == SGB_HEAT7 ? lap7_heat(c, xm, xp, ym, yp, zm, zp) : lap7(c, xm, xp, ym, yp, zm, zp);
 }
 
 // Gray-Scott as a conv2_b user function:
@@ -71,10 +85,13 @@ struct LaunchDesc {
     StencilParams prm;
     int64_t t;
     unsigned* err;
+    const uint64_t* ebits;  // EXIST / active bitmaps (single-grid 8^3 launches; NULL otherwise)
+    const uint64_t* abits;
 };
 
 int launch_fields(const LaunchDesc& L, cudaStream_t s);
 int launch_e8(const LaunchDesc& L, cudaStream_t s);  // pipelined 8^3 kernel (stencil8.cu)
+int launch_rows(const LaunchDesc& L, cudaStream_t s);  // row-sparse single-grid 8^3 kernel (stencil8r.cu)
 GridInfo grid_info_of(const StencilParams& prm);
 
 // Capture `body(stream)` into a CUDA graph, launch it on `s`, wait for it.

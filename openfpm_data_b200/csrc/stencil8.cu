@@ -288,10 +288,10 @@ __global__ void __launch_bounds__(kThreads8, KIND == SGB_GS7 ? 6 : 8)
                     const float xm = ld1(aXm[p] + zz * sXm);
                     const float xp = ld1(aXp[p] + zz * sXp);
                     const float4 c = cv[p], zm = zmv[p];
-                    lap[p].x = lap7(c.x, xm, c.y, ym.x, yp.x, zm.x, zp.x);
-                    lap[p].y = lap7(c.y, c.x, c.z, ym.y, yp.y, zm.y, zp.y);
-                    lap[p].z = lap7(c.z, c.y, c.w, ym.z, yp.z, zm.z, zp.z);
-                    lap[p].w = lap7(c.w, c.z, xp, ym.w, yp.w, zm.w, zp.w);
+                    lap[p].x = lap7k<KIND>(c.x, xm, c.y, ym.x, yp.x, zm.x, zp.x);
+                    lap[p].y = lap7k<KIND>(c.y, c.x, c.z, ym.y, yp.y, zm.y, zp.y);
+                    lap[p].z = lap7k<KIND>(c.z, c.y, c.w, ym.z, yp.z, zm.z, zp.z);
+                    lap[p].w = lap7k<KIND>(c.w, c.z, xp, ym.w, yp.w, zm.w, zp.w);
                     cur[p] = c;
                     zmv[p] = c;
                     cv[p] = zp;

@@ -623,6 +623,20 @@ class Batch:
                 "sgb_batch_read")
         return keys, mask, fields
 
+    def read_async(self, slot: int, nfields: int, bs: int = 512, stream=None):
+        """Queue the copy of a slot's state into fresh pinned host tensors on `stream` and return
+        (keys, mask, [fields], event): the arrays hold the state once `event` has completed."""
+        n = self.nchunks(slot)
+        keys = torch.empty(max(n, 1), dtype=torch.int64).pin_memory()
+        mask = torch.empty(max(n * bs, 1), dtype=torch.uint8).pin_memory()
+        fields = [torch.empty(max(n * bs, 1), dtype=torch.float32).pin_memory() for _ in range(nfields)]
+        ptrs = (C.c_void_p * nfields)(*[f.data_ptr() for f in fields])
+        L.check(self._lib.sgb_batch_read_async(self._h, slot, keys.data_ptr(), mask.data_ptr(), ptrs, None,
+                                               _stream(stream)), "sgb_batch_read_async")
+        ev = torch.cuda.Event()
+        ev.record(stream if stream is not None else torch.cuda.current_stream())
+        return keys.numpy()[:n], mask.numpy()[: n * bs], [f.numpy()[: n * bs] for f in fields], ev
+
     def info(self):
         ng, nc, nb = C.c_int(), C.c_int64(), C.c_int64()
         L.check(self._lib.sgb_batch_info(self._h, C.byref(ng), C.byref(nc), C.byref(nb)), "sgb_batch_info")

@@ -83,35 +83,52 @@ class ServeStats:
 
 
 class Server:
-    """Admission by HBM budget + continuous batching over two resident batches."""
+    """Admission by HBM budget + continuous batching over two resident batches.
+
+    The loop never waits for a quantum it has just launched: each kind's batch
+    steps on its own stream (heat and Gray-Scott quanta run concurrently), new
+    requests are built on a third stream and joined to their batch by a stream
+    dependency, and finished requests are read back asynchronously into pinned
+    memory behind the quantum that finished them; the host collects them by
+    polling their completion events.  At most `depth` quanta per kind are
+    queued ahead of the GPU, so a newly admitted request waits for at most
+    that many quanta before its first step."""
 
     def __init__(self, budget_bytes: float = 150e9, quantum: int = 25, device: int = 0, use_graph: bool = True,
-                 ctas_per_sm: int = 0, stages: int = 0, keep_results: bool = False):
+                 ctas_per_sm: int = 0, stages: int = 0, keep_results: bool = False, depth: int = 2):
+        import torch
         self.budget = int(budget_bytes)
         self.quantum = quantum
         self.device = device
         self.use_graph = use_graph
         self.keep_results = keep_results
+        self.depth = max(1, int(depth))
         self.batches: Dict[str, Batch] = {k: Batch(device) for k in KIND}
         if ctas_per_sm or stages:
             for b in self.batches.values():
                 b.set_launch_config(ctas_per_sm, stages)
-        self.pool: Dict[tuple, SparseGridGpu] = {}
+        self.streams = {k: torch.cuda.Stream(device=device) for k in KIND}
+        self.admit_stream = torch.cuda.Stream(device=device)
+        # staging grids per (kind, edge): [grid, event after the batch copied it (None: free)]
+        self.pool: Dict[tuple, list] = {}
         self.used = 0
         self.active: Dict[tuple, tuple] = {}
+        self.reading: list = []
         self.results: Dict[int, list] = {}
 
-    def _staging(self, kind: str, edge: int) -> SparseGridGpu:
-        key = (kind, edge)
-        g = self.pool.get(key)
-        if g is None:
-            nf = NFIELDS[kind]
-            g = SparseGridGpu((edge,) * 3, ["f32"] * (2 * nf), edge=8, device=self.device)
-            if kind == "gs":
-                for p, b in enumerate([1.0, 0.0, 1.0, 0.0]):
-                    g.setBackgroundValue(p, b)
-            self.pool[key] = g
-        return g
+    def _staging(self, kind: str, edge: int) -> list:
+        entries = self.pool.setdefault((kind, edge), [])
+        for ent in entries:
+            if ent[1] is None or ent[1].query():
+                return ent
+        nf = NFIELDS[kind]
+        g = SparseGridGpu((edge,) * 3, ["f32"] * (2 * nf), edge=8, device=self.device)
+        if kind == "gs":
+            for p, b in enumerate([1.0, 0.0, 1.0, 0.0]):
+                g.setBackgroundValue(p, b)
+        ent = [g, None]
+        entries.append(ent)
+        return ent
 
     @staticmethod
     def estimate_bytes(req: W.Request) -> int:
@@ -125,78 +142,119 @@ class Server:
         return chunks * bytes_per_chunk(req.kind)
 
     def admit(self, req: W.Request, now: float) -> bool:
+        import torch
         est = self.estimate_bytes(req)
         if self.used + est > self.budget:
             return False
-        g = self._staging(req.kind, req.edge)
+        ent = self._staging(req.kind, req.edge)
+        g = ent[0]
         nf = NFIELDS[req.kind]
         init = 0 if req.kind == "heat" else 1
-        g.build_balls(balls_of(req), init, req.vseed, list(range(nf)))
+        # the scene is built on the admission stream (its chunk count is read back there, without
+        # waiting for the quanta in flight); the batch copies it on its own stream after that
+        g.build_balls(balls_of(req), init, req.vseed, list(range(nf)), stream=self.admit_stream)
+        cs = self.streams[req.kind]
+        cs.wait_stream(self.admit_stream)
         src, dst = list(range(nf)), list(range(nf, 2 * nf))
         prm = HEAT_PARAMS if req.kind == "heat" else GS_PARAMS
         b = self.batches[req.kind]
         try:
-            slot = b.add(g, KIND[req.kind], src, dst, prm, req.steps)
+            slot = b.add(g, KIND[req.kind], src, dst, prm, req.steps, stream=cs)
         except L.SgbError as e:
             if e.status != L.ENOMEM:
                 raise
             return False  # the device is fuller than the budget says: retry once memory is returned
+        ev = torch.cuda.Event()
+        ev.record(cs)
+        ent[1] = ev  # the staging grid may be rebuilt once the batch has copied it
         n = g.nchunks
         used = n * bytes_per_chunk(req.kind)
         self.used += used
-        self.active[(req.kind, slot)] = (req, now, used, n, g.countExistingElements())
+        self.active[(req.kind, slot)] = (req, now, used, n)
         return True
 
-    def retire(self, now_fn, stats: ServeStats) -> None:
+    def _start_reads(self) -> None:
+        """Queue the read-back of every request whose steps are all launched, behind those steps."""
         for key in list(self.active):
             kind, slot = key
-            req, t_admit, used, n, points = self.active[key]
+            req, t_admit, used, n = self.active[key]
             b = self.batches[kind]
             if b.slot_steps(slot) < req.steps:
                 continue
-            # the response: the request's block map and final fields, read into pinned host memory
-            keys, mask, fields = b.read(slot, NFIELDS[kind], staged=not self.keep_results)
-            if self.keep_results:
-                self.results[req.rid] = [keys, mask, fields]
-            b.remove(slot)
-            self.used -= used
+            data = b.read_async(slot, NFIELDS[kind], stream=self.streams[kind])
+            self.reading.append((req, kind, slot, used, t_admit, data))
             del self.active[key]
-            stats.done.append(Done(req.rid, kind, req.t_arrival, t_admit, now_fn(), points, req.steps))
+
+    def _collect(self, now_fn, stats: ServeStats) -> None:
+        """Finish the requests whose read-back has completed: the response is in host memory."""
+        still = []
+        for item in self.reading:
+            req, kind, slot, used, t_admit, (keys, mask, fields, ev) = item
+            if not ev.query():
+                still.append(item)
+                continue
+            t_done = now_fn()
+            if self.keep_results:
+                self.results[req.rid] = [keys.copy(), mask.copy(), [f.copy() for f in fields]]
+            points = int(np.count_nonzero(mask & 1))
+            self.batches[kind].remove(slot)
+            self.used -= used
+            stats.done.append(Done(req.rid, kind, req.t_arrival, t_admit, t_done, points, req.steps))
+        self.reading = still
 
     def run(self, reqs: List[W.Request], realtime: bool = True, time_limit: Optional[float] = None) -> ServeStats:
         """Serve a request list.  realtime=True releases requests at their
         arrival times (open loop); otherwise all are available at t = 0."""
+        import torch
         stats = ServeStats()
         pending = deque(sorted(reqs, key=lambda r: r.t_arrival))
+        queued = {k: deque() for k in KIND}  # events after each kind's quanta in flight
         t0 = time.perf_counter()
         now_fn = lambda: time.perf_counter() - t0  # noqa: E731
-        while pending or self.active:
+        while pending or self.active or self.reading:
             now = now_fn()
             if time_limit is not None and now > time_limit:
                 break
+            self._collect(now_fn, stats)
             while pending and (not realtime or pending[0].t_arrival <= now):
                 if not self.admit(pending[0], now):
-                    if not self.active:  # cannot ever fit
+                    if not self.active and not self.reading:  # cannot ever fit
                         stats.rejected += 1
                         pending.popleft()
                         continue
                     break
                 pending.popleft()
             stats.peak_bytes = max(stats.peak_bytes, self.used)
-            if not self.active:
-                if pending:
-                    time.sleep(max(0.0, min(pending[0].t_arrival - now_fn(), 0.002)))
-                continue
+            launched = False
             for kind, b in self.batches.items():
-                if any(k == kind for k, _ in self.active):
-                    b.step(self.quantum, use_graph=self.use_graph)
-            self.retire(now_fn, stats)
+                if not any(k == kind for k, _ in self.active):
+                    continue
+                q = queued[kind]
+                while len(q) >= self.depth:  # keep at most `depth` quanta queued ahead of the GPU
+                    q.popleft().synchronize()
+                b.step(self.quantum, use_graph=self.use_graph, stream=self.streams[kind])
+                ev = torch.cuda.Event()
+                ev.record(self.streams[kind])
+                q.append(ev)
+                launched = True
+            self._start_reads()
+            if not launched:
+                if self.reading:
+                    time.sleep(0.0002)
+                elif pending:
+                    time.sleep(max(0.0, min(pending[0].t_arrival - now_fn(), 0.002)))
+        for q in queued.values():
+            for ev in q:
+                ev.synchronize()
         stats.wall = now_fn()
         return stats
 
     def close(self):
-        for g in self.pool.values():
-            g.close()
+        import torch
+        torch.cuda.synchronize(self.device)
+        for entries in self.pool.values():
+            for g, _ in entries:
+                g.close()
         for b in self.batches.values():
             b.close()
 

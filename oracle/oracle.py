@@ -74,6 +74,7 @@ def _load():
         d = C.c_double
         _lib.sgo_heat7_f64.argtypes = [vp, vp, vp, d, d, i32]
         _lib.sgo_gs7_f64.argtypes = [vp, vp, vp, vp, vp, d, d, d, d, d, d, d, i32]
+        _lib.sgo_gs7_f64_mt.argtypes = [vp, vp, vp, vp, vp, d, d, d, d, d, d, d, i32, i32]
         _cpu.cpub_create.restype = vp
         _cpu.cpub_create.argtypes = [vp, i32, vp]
         _cpu.cpub_destroy.argtypes = [vp]
@@ -410,11 +411,12 @@ class OracleGrid:
         _lib.sgo_heat7_f64(self._h, _ptr(a), _ptr(b), dt, bck, steps)
         return a
 
-    def gs7_f64(self, u, v, Du, Dv, F, k, dt, bcku, bckv, steps):
+    def gs7_f64(self, u, v, Du, Dv, F, k, dt, bcku, bckv, steps, threads=1):
         u = np.ascontiguousarray(u, dtype=np.float64).copy()
         v = np.ascontiguousarray(v, dtype=np.float64).copy()
         u2, v2 = u.copy(), v.copy()
-        _lib.sgo_gs7_f64(self._h, _ptr(u), _ptr(v), _ptr(u2), _ptr(v2), Du, Dv, F, k, dt, bcku, bckv, steps)
+        _lib.sgo_gs7_f64_mt(self._h, _ptr(u), _ptr(v), _ptr(u2), _ptr(v2), Du, Dv, F, k, dt, bcku, bckv, steps,
+                            int(threads))
         return u, v
 
     # -- point access (host get<p>(coord), BlockMapGpu.hpp:108-126) --------

@@ -373,12 +373,16 @@ void heat7_chunk(const Grid& g, const std::vector<int64_t>& nn, int64_t i, int s
         float cur = tile[tile_index(g, tc)];
         float res = cur;
         if (active(cur_mask(g, i, o, box))) {
-            float lap = (float)(-2.0 * g.dim * (double)cur);
+            // laplacian = -2.0*dim*cur (exact in double, narrowed to float), then per dimension
+            // += neighbourMinus + neighbourPlus: nvcc fuses the narrowed product with the first sum
+            // (x) into one fma; res = cur + dt*laplacian is an fma too
+            float lap = 0.0f;
             for (int d = 0; d < g.dim; ++d) {
                 int a[3] = {tc[0], tc[1], tc[2]}, b[3] = {tc[0], tc[1], tc[2]};
                 a[d] -= 1;
                 b[d] += 1;
-                lap = lap + (tile[tile_index(g, a)] + tile[tile_index(g, b)]);
+                const float pair = tile[tile_index(g, a)] + tile[tile_index(g, b)];
+                lap = d == 0 ? std::fmaf((float)(-2.0 * g.dim), cur, pair) : lap + pair;
             }
             res = std::fmaf(dt, lap, cur);
         }
@@ -415,6 +419,22 @@ void gs7_chunk(const Grid& g, const std::vector<int64_t>& nn, int64_t i, int pu,
         std::memcpy(&ou[((size_t)i * g.bs + o) * 4], &un, 4);
         std::memcpy(&ov[((size_t)i * g.bs + o) * 4], &vn, 4);
     }
+}
+
+// Runs body(lo, hi) over [0, n) split into `threads` ranges (the floating-point mode as it is).
+template <typename F>
+void for_chunks_plain(int64_t n, int threads, F body) {
+    threads = std::max(1, std::min<int>(threads, 256));
+    if (threads == 1 || n < 2) {
+        body(0, n);
+        return;
+    }
+    std::vector<std::thread> pool;
+    for (int t = 0; t < threads; ++t) {
+        const int64_t lo = n * t / threads, hi = n * (t + 1) / threads;
+        pool.emplace_back([&body, lo, hi] { body(lo, hi); });
+    }
+    for (auto& th : pool) th.join();
 }
 
 // Runs body(lo, hi) over [0, n) split into `threads` ranges, each thread with FTZ|DAZ set.
@@ -672,9 +692,13 @@ void sgo_tag_boundaries(void* h, int kind) {
 // HeatStencil::stencil (src/SparseGridGpu/tests/utils/SparseGridGpu_util_test.cuh:
 // 224-290) driven by applyStencilInPlace: active points get
 //   lap = (float)(-2.0*dim*cur); lap += xm + xp; ... ; res = cur + dt*lap
-// (an FMA under nvcc), every other point of the destination chunk receives
-// the tile value (its own value, or the background when its mask is 0):
-// storeBlock writes the whole chunk (SparseGridGpu_ker.cuh:877-896).
+// with the roundings nvcc gives that source: the double product -6*cur is
+// exact, so its narrowing to float is a float multiply, which the default FMA
+// contraction fuses with the first sum, lap = fma(-6, cur, xm + xp), and
+// res = fma(dt, lap, cur) (the drop-in test compiles the reference's functor
+// and checks this point by point).  Every other point of the destination
+// chunk receives the tile value (its own value, or the background when its
+// mask is 0): storeBlock writes the whole chunk (SparseGridGpu_ker.cuh:877-896).
 void sgo_heat7(void* h, int src, int dst, float dt, const int64_t* box) {
     FtzScope ftz;
     Grid* g = (Grid*)h;
@@ -858,14 +882,25 @@ void sgo_heat7_f64(void* h, double* f_src, double* f_dst, double dt, double bck,
     else if (a != f_src) std::memcpy(f_src, a, sizeof(double) * (size_t)(g->n() + 1) * bs);
 }
 
+void sgo_gs7_f64_mt(void* h, double* u, double* v, double* u2, double* v2, double Du, double Dv, double F,
+                    double k, double dt, double bcku, double bckv, int steps, int threads);
+
 void sgo_gs7_f64(void* h, double* u, double* v, double* u2, double* v2, double Du, double Dv, double F,
                  double k, double dt, double bcku, double bckv, int steps) {
+    sgo_gs7_f64_mt(h, u, v, u2, v2, Du, Dv, F, k, dt, bcku, bckv, steps, 1);
+}
+
+// The same with the chunks of each step shared out over host threads (no FTZ: a double-precision
+// reference keeps its subnormals).
+void sgo_gs7_f64_mt(void* h, double* u, double* v, double* u2, double* v2, double Du, double Dv, double F,
+                    double k, double dt, double bcku, double bckv, int steps, int threads) {
     Grid* g = (Grid*)h;
     auto nn = find_neighbours(*g, NN_STAR);
     const int bs = g->bs, e = g->edge, K = nnn(*g, NN_STAR);
     double *ua = u, *va = v, *ub = u2, *vb = v2;
     for (int s = 0; s < steps; ++s) {
-        for (int64_t i = 0; i < g->n(); ++i) {
+      for_chunks_plain(g->n(), threads, [&](int64_t c0, int64_t c1) {
+        for (int64_t i = c0; i < c1; ++i) {
             for (int o = 0; o < bs; ++o) {
                 uint8_t m = g->mask[(size_t)i * bs + o];
                 size_t idx = (size_t)i * bs + o;
@@ -895,6 +930,7 @@ void sgo_gs7_f64(void* h, double* u, double* v, double* u2, double* v2, double D
                 vb[idx] = cv + dt * (Dv * lv + uvv - (F + k) * cv);
             }
         }
+      });
         std::swap(ua, ub);
         std::swap(va, vb);
     }

@@ -838,6 +838,63 @@ int main() {
             g->tagBoundaries(ctx);
             g->applyStencils<UserBoundarySetXRescaled<3, 0, 0>>(g->getBox(), STENCIL_MODE_INPLACE, 0.0, 16, 0.0, 10.0);
         }
+        {
+            // which rounding does nvcc give the reference's HeatStencil?  One step of the functor on a
+            // twin grid, against the two candidate roundings of the first Laplacian term computed
+            // here: -6 cur rounded, then + (xm + xp) rounded; or both in one fused multiply-add
+            Grid2 dg(s16);
+            dg.setBackgroundValue<0>(0.0f);
+            dg.setGPUInsertBuffer(dim3(2, 2, 2), dim3(1, 1, 1));
+            insert_constant_blocks<0, 1><<<dim3(2, 2, 2), dim3(8, 8, 8)>>>(dg.toKernel(), 0.0f);
+            dg.flush<smax_<0>, smax_<1>>(ctx, FLUSH_ON_DEVICE);
+            dg.tagBoundaries(ctx);
+            dg.applyStencils<UserBoundarySetXRescaled<3, 0, 0>>(dg.getBox(), STENCIL_MODE_INPLACE, 0.0, 16, 0.0, 10.0);
+            for (int k = 0; k < 6; ++k) {  // some structure in the interior first
+                dg.applyStencils<HeatStencil<3, 0, 1>>(dg.getBox(), STENCIL_MODE_INPLACE, 0.1f);
+                dg.applyStencils<HeatStencil<3, 1, 0>>(dg.getBox(), STENCIL_MODE_INPLACE, 0.1f);
+            }
+            HostMap pre = download(dg.handle(), 2);
+            dg.applyStencils<UserHeatStencil<3, 0, 1>>(dg.getBox(), STENCIL_MODE_INPLACE, 0.1f);
+            HostMap post = download(dg.handle(), 2);
+            auto at = [&](int x, int y, int z) -> float {
+                if (x < 0 || y < 0 || z < 0 || x >= 16 || y >= 16 || z >= 16) return 0.0f;
+                const long key = (x / 8) + 2 * ((y / 8) + 2 * (long)(z / 8));
+                for (size_t i = 0; i < pre.keys.size(); ++i)
+                    if (pre.keys[i] == key) {
+                        const size_t o = i * 512 + (x % 8) + 8 * ((y % 8) + 8 * (z % 8));
+                        return pre.mask[o] ? pre.data[0][o] : 0.0f;
+                    }
+                return 0.0f;
+            };
+            size_t nact = 0, sep_ok = 0, fused_ok = 0;
+            for (size_t c = 0; c < pre.keys.size(); ++c) {
+                const int bx = (int)(pre.keys[c] % 2), by = (int)((pre.keys[c] / 2) % 2), bz = (int)(pre.keys[c] / 4);
+                for (int o = 0; o < 512; ++o) {
+                    if ((pre.mask[c * 512 + o] & 3) != 1) continue;
+                    const int x = bx * 8 + o % 8, y = by * 8 + (o / 8) % 8, z = bz * 8 + o / 64;
+                    const float cur = at(x, y, z);
+                    const float sx = at(x - 1, y, z) + at(x + 1, y, z), sy = at(x, y - 1, z) + at(x, y + 1, z),
+                                sz = at(x, y, z - 1) + at(x, y, z + 1);
+                    volatile float m6 = (float)(-6.0 * (double)cur);
+                    float lsep = m6 + sx;
+                    lsep = lsep + sy;
+                    lsep = lsep + sz;
+                    float lfus = std::fmaf(-6.0f, cur, sx);
+                    lfus = lfus + sy;
+                    lfus = lfus + sz;
+                    const float rsep = std::fmaf(0.1f, lsep, cur), rfus = std::fmaf(0.1f, lfus, cur);
+                    const float got = post.data[1][c * 512 + o];
+                    ++nact;
+                    sep_ok += std::memcmp(&got, &rsep, 4) == 0;
+                    fused_ok += std::memcmp(&got, &rfus, 4) == 0;
+                }
+            }
+            std::printf("  reference HeatStencil compiled here: %zu active points, %zu match the separate rounding, "
+                        "%zu the fused multiply-add\n",
+                        nact, sep_ok, fused_ok);
+            // the library's HeatStencil (and the oracle) use the rounding nvcc gives the reference's source
+            CHECK(nact > 0 && fused_ok == nact, "HeatStencil_rounding_is_the_fused_multiply_add");
+        }
         for (int it = 0; it < 1000; ++it) {
             hg.applyStencils<UserHeatStencil<3, 0, 1>>(hg.getBox(), STENCIL_MODE_INPLACE, 0.1f);
             hg.applyStencils<UserHeatStencil<3, 1, 0>>(hg.getBox(), STENCIL_MODE_INPLACE, 0.01f);
@@ -847,6 +904,13 @@ int main() {
             }
             if (it == 49) {
                 HostMap a = download(hg.handle(), 2), b = download(fg.handle(), 2);
+                for (int p = 0; p < 2; ++p)
+                    for (size_t i = 0; i < a.keys.size() * 512; ++i)
+                        if (existing(a.mask[i]) && std::memcmp(&a.data[p][i], &b.data[p][i], 4) != 0) {
+                            std::printf("  first difference: property %d point %zu mask %d user %.9g fixed %.9g\n", p, i,
+                                        (int)a.mask[i], a.data[p][i], b.data[p][i]);
+                            break;
+                        }
                 CHECK(same(a, 0, b, 0, existing) && same(a, 1, b, 1, existing), "user_HeatStencil_equals_fixed_50");
             }
         }

@@ -4,9 +4,12 @@ balls, seed 1; workloads.gray_scott) after 1, 2, 100 and 1000 steps.
 
 For each checkpoint it records the SHA-256 of u and v at the existing points
 (float32 bytes in (chunk position, offset) order) plus their float64 sums, so
-a GPU run can be checked bit for bit without shipping 53 MB of fields.  The
-oracle is the checker only; this script runs it once (a few minutes on 8
-host threads).
+a GPU run can be checked bit for bit without shipping 53 MB of fields.  At
+100 and 1000 steps it also records the error of those FP32 fields against the
+same update in double precision (the FP64 oracle): max absolute error and the
+normwise relative error ||f32 - f64|| / ||f64|| over the existing points, per
+field.  The oracle is the checker only; this script runs it once (FP32: a
+few minutes on 8 host threads; FP64: about ten more).
 
 Usage: python tests/golden/make_gs512_golden.py
 """
@@ -48,22 +51,40 @@ def oracle_grid():
     return o, keys
 
 
+def fp64_error(f32, f64, ex):
+    a = np.asarray(f32, dtype=np.float64)[ex]
+    b = np.asarray(f64, dtype=np.float64)[ex]
+    return {"max_abs": float(np.max(np.abs(a - b))),
+            "normwise_rel": float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))}
+
+
 def main():
     O.build()
     prm = [W.GS_PARAMS[k] for k in ("Du", "Dv", "F", "k", "dt")]
     o, keys = oracle_grid()
     n = len(keys)
     out = {"workload": "gray_scott_512^3_chunk8^3_40balls_seed1", "params": prm, "chunks": n, "checkpoints": {}}
+    _, data0, mask0 = o.export()
+    ex = (mask0[: n * 512] & 1).astype(bool)
+    u64 = np.asarray(data0[0], dtype=np.float64)
+    v64 = np.asarray(data0[1], dtype=np.float64)
     done = 0
     t0 = time.time()
     for cp in CHECKPOINTS:
         # continue the ping-pong from buffer pair (0, 1) or (2, 3) depending on the steps done so far
         src, dst = ((0, 1), (2, 3)) if done % 2 == 0 else ((2, 3), (0, 1))
         o.gs7_steps(src[0], src[1], dst[0], dst[1], *prm, steps=cp - done)
-        done = cp
         _, data, mask = o.export()
-        fu, fv = (2, 3) if done % 2 == 1 else (0, 1)
-        out["checkpoints"][str(cp)] = field_digest(data[fu], data[fv], mask, n)
+        fu, fv = (2, 3) if cp % 2 == 1 else (0, 1)
+        rec = field_digest(data[fu], data[fv], mask, n)
+        if cp >= 100:  # the same steps in double precision, continued from the previous checkpoint
+            u64, v64 = o.gs7_f64(u64, v64, *prm[:4], prm[4], 1.0, 0.0, cp - done, threads=os.cpu_count() or 1)
+            rec["fp64_error"] = {"u": fp64_error(data[fu][: n * 512], u64[: n * 512], ex),
+                                 "v": fp64_error(data[fv][: n * 512], v64[: n * 512], ex)}
+        elif cp == 2:
+            u64, v64 = o.gs7_f64(u64, v64, *prm[:4], prm[4], 1.0, 0.0, 2, threads=os.cpu_count() or 1)
+        done = cp
+        out["checkpoints"][str(cp)] = rec
         print(f"step {cp}: {time.time() - t0:.1f} s", flush=True)
     with open(OUT, "w") as f:
         json.dump(out, f, indent=1)
