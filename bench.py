@@ -67,7 +67,7 @@ def parse():
     ap.add_argument("--no-sub-records", action="store_true",
                     help="gs512: leave out the bounded runs of the other configurations")
     ap.add_argument("--sub-serve-seconds", type=float, default=6.0, help="sub-records: served arrival window")
-    ap.add_argument("--sub-sustained-rate", type=float, default=600.0,
+    ap.add_argument("--sub-sustained-rate", type=float, default=400.0,
                     help="sub-records: an arrival rate the served form keeps up with (requests/s)")
     return ap.parse_args()
 

@@ -564,7 +564,6 @@ extern "C" int sgb_flush(sgb_grid* g, const int* ops, sgb_stream stream) {
     g->nn_valid[0] = g->nn_valid[1] = false;
     g->nnhash_ok = false;
     g->bits_valid = false;
-    g->abits_valid = false;
     g->epts_valid = false;
     return st;
 }

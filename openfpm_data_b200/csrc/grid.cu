@@ -144,7 +144,6 @@ static void invalidate_derived(sgb_grid* g) {
     g->nn_valid[0] = g->nn_valid[1] = false;
     g->nnhash_ok = false;
     g->bits_valid = false;
-    g->abits_valid = false;
     g->epts_valid = false;
 }
 
@@ -487,7 +486,6 @@ int sgb_destroy(sgb_grid* g) {
     g->nn[1].release();
     g->nnhash.release();
     g->bits.release();
-    g->abits.release();
     g->epts.release();
     for (auto& L : g->links) {
         L.pad_pos.release();
@@ -506,7 +504,6 @@ int sgb_destroy(sgb_grid* g) {
 int sgb_existence_changed(sgb_grid* g) {
     if (!g) return SGB_EINVAL;
     g->bits_valid = false;
-    g->abits_valid = false;
     g->epts_valid = false;
     return SGB_OK;
 }
@@ -524,9 +521,7 @@ int sgb_release_scratch(sgb_grid* g) {
     }
     if (g->npend == 0) g->pend_lin.release();
     g->bits.release();
-    g->abits.release();
     g->bits_valid = false;
-    g->abits_valid = false;
     g->epts.release();
     g->epts_valid = false;
     g->nnhash.release();
@@ -725,7 +720,6 @@ int sgb_mask_buffer(sgb_grid* g, uint8_t** dev) {
     *dev = g->mask.as<uint8_t>();
     for (int p = 0; p < g->nprop; ++p) g->clean[p] = false;  // existence may change
     g->bits_valid = false;
-    g->abits_valid = false;
     g->epts_valid = false;
     return SGB_OK;
 }

@@ -245,8 +245,6 @@ struct sgb_grid {
     bool nnhash_ok = false;  // built for the current keys (any key change invalidates both nn tables)
     sgb::DevBuf bits;     // uint64 existence bitmaps, bs/64 words per chunk
     bool bits_valid = false;
-    sgb::DevBuf abits;    // uint64 bitmaps of the active points (EXIST and not PADDING), same layout
-    bool abits_valid = false;
     // existing-point list (e_points): uint32 chunk position * bs + offset
     sgb::DevBuf epts;
     int64_t nepts = 0;
@@ -276,7 +274,6 @@ namespace sgb {
 // neighbours.cu
 int ensure_neighbours(sgb_grid* g, int nn, cudaStream_t s);
 int ensure_bits(sgb_grid* g, cudaStream_t s);
-int ensure_active_bits(sgb_grid* g, cudaStream_t s);
 
 // points.cu
 int ensure_point_list(sgb_grid* g, cudaStream_t s);

@@ -163,19 +163,6 @@ __global__ void k_bits(const uint8_t* __restrict__ mask, int64_t n, int bs, uint
     reinterpret_cast<uint16_t*>(bits)[t] = (uint16_t)b;
 }
 
-// Bitmaps of the active points (mask & 3 == 1: EXIST and not PADDING), laid out as k_bits'.
-__global__ void k_abits(const uint8_t* __restrict__ mask, int64_t n, int bs, uint64_t* bits) {
-    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (t >= n * (bs >> 4)) return;
-    const uint4 v = __ldg(reinterpret_cast<const uint4*>(mask) + t);
-    auto four = [](unsigned w) {
-        const unsigned x = w & ~(w >> 1) & 0x01010101u;
-        return (x | x >> 7 | x >> 14 | x >> 21) & 0xfu;
-    };
-    const unsigned b = four(v.x) | four(v.y) << 4 | four(v.z) << 8 | four(v.w) << 12;
-    reinterpret_cast<uint16_t*>(bits)[t] = (uint16_t)b;
-}
-
 // tagBoundaries (src/SparseGridGpu/SparseGridGpu_kernels.cuh:676-737) with
 // NNStar::isPadding (SparseGridGpu_ker_util.hpp:141-157) for 8^3 chunks: one
 // warp per chunk; lanes 0..7 hold the 64-bit z-slices of the existence
@@ -310,20 +297,6 @@ int ensure_bits(sgb_grid* g, cudaStream_t s) {
     return SGB_OK;
 }
 
-int ensure_active_bits(sgb_grid* g, cudaStream_t s) {
-    if (g->abits_valid) return SGB_OK;
-    const int words = g->geo.bs / 64;
-    SGB_TRY(g->abits.grow((size_t)(g->n + 1) * words * 8));
-    if (g->n > 0) {
-        const int64_t threads = g->n * (g->geo.bs / 16);
-        k_abits<<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(g->mask.as<uint8_t>(), g->n, g->geo.bs,
-                                                                   g->abits.as<uint64_t>());
-        SGB_CUDA(cudaGetLastError());
-    }
-    g->abits_valid = true;
-    return SGB_OK;
-}
-
 }  // namespace sgb
 
 using namespace sgb;
@@ -367,7 +340,6 @@ int sgb_tag_boundaries(sgb_grid* g, int nn, sgb_stream stream) {
                                                      g->geo.edge, nn, g->mask.as<uint8_t>());
     }
     SGB_CUDA(cudaGetLastError());
-    g->abits_valid = false;  // PADDING bits changed
     return SGB_OK;
 }
 

@@ -161,7 +161,6 @@ extern "C" int sgb_remove_boxes(sgb_grid* g, int64_t nboxes, const int64_t* boxe
     SGB_CUDA(cudaStreamSynchronize(s));
     // existence changed; chunks, neighbours and backgrounds did not
     g->bits_valid = false;
-    g->abits_valid = false;
     g->epts_valid = false;
     return SGB_OK;
 }

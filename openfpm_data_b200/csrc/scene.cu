@@ -196,7 +196,6 @@ extern "C" int sgb_build_balls(sgb_grid* g, int nballs, const float* balls, int 
     g->nn_valid[0] = g->nn_valid[1] = false;
     g->nnhash_ok = false;
     g->bits_valid = false;
-    g->abits_valid = false;
     g->epts_valid = false;
     return SGB_OK;
 }

@@ -524,11 +524,7 @@ int launch_fields(const LaunchDesc& L, cudaStream_t s) {
     if (L.n == 0) return SGB_OK;
     // the pipelined kernel takes the x halo from the neighbouring index positions, which hold the
     // x neighbours only under the x-fastest chunk ids
-    if (L.kind != SGB_BOX27 && L.edge == 8 && !L.use_tile && !L.geo.zorder) {
-        // one grid over its whole domain: the row-sparse kernel (bitmaps instead of mask tiles)
-        if (!L.grids && !L.prm.has_box && L.ebits && L.abits) return launch_rows(L, s);
-        return launch_e8(L, s);
-    }
+    if (L.kind != SGB_BOX27 && L.edge == 8 && !L.use_tile && !L.geo.zorder) return launch_e8(L, s);
     if (L.kind == SGB_BOX27 && L.edge == 8 && !L.use_tile && !L.grids) {
         // 4 CTAs of four warps per SM are resident (128 registers a thread)
         const int64_t want = (L.n + kW27Warps - 1) / kW27Warps;
@@ -568,20 +564,8 @@ int launch_stencil_impl(sgb_grid* g, int kind, const int* src, const int* dst, c
     SGB_TRY(ensure_neighbours(g, nnk, s));
     const int np = kind == SGB_GS7 ? 2 : 1;
     for (int j = 0; j < np; ++j) SGB_TRY(ensure_clean(g, src[j], s));
-    // the row-sparse kernel writes only rows that hold an existing point: the other points of the
-    // destination must hold its background already
-    const bool rows = kind != SGB_BOX27 && g->geo.edge == 8 && !use_tile && !g->geo.zorder && !prm.has_box;
-    if (rows) {
-        for (int j = 0; j < np; ++j) SGB_TRY(ensure_clean(g, dst[j], s));
-        SGB_TRY(ensure_bits(g, s));
-        SGB_TRY(ensure_active_bits(g, s));
-    }
     LaunchDesc L;
     std::memset(&L, 0, sizeof(L));
-    if (rows) {
-        L.ebits = g->bits.as<uint64_t>();
-        L.abits = g->abits.as<uint64_t>();
-    }
     L.kind = kind;
     L.edge = g->geo.edge;
     L.use_tile = use_tile;
@@ -650,10 +634,6 @@ int sgb_run_steps(sgb_grid* g, int kind, const int* src, const int* dst, const f
     if (nsteps == 0 || g->n == 0) return SGB_OK;
     SGB_TRY(ensure_neighbours(g, kind == SGB_BOX27 || kind == SGB_BOX27_NS ? SGB_NN_FULL : SGB_NN_STAR, s));
     if (kind == SGB_BOX27_NS || kind == SGB_BOX27) SGB_TRY(ensure_point_list(g, s));  // built outside the capture
-    if (kind == SGB_HEAT7 || kind == SGB_GS7) {  // the row-sparse kernel's bitmaps, outside the capture
-        SGB_TRY(ensure_bits(g, s));
-        SGB_TRY(ensure_active_bits(g, s));
-    }
     // both halves of the ping-pong are read as sources; no sanitising inside a capture
     for (int j = 0; j < (kind == SGB_GS7 ? 2 : 1); ++j) {
         SGB_TRY(ensure_clean(g, src[j], s));

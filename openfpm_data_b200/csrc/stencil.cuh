@@ -85,13 +85,10 @@ struct LaunchDesc {
     StencilParams prm;
     int64_t t;
     unsigned* err;
-    const uint64_t* ebits;  // EXIST / active bitmaps (single-grid 8^3 launches; NULL otherwise)
-    const uint64_t* abits;
 };
 
 int launch_fields(const LaunchDesc& L, cudaStream_t s);
 int launch_e8(const LaunchDesc& L, cudaStream_t s);  // pipelined 8^3 kernel (stencil8.cu)
-int launch_rows(const LaunchDesc& L, cudaStream_t s);  // row-sparse single-grid 8^3 kernel (stencil8r.cu)
 GridInfo grid_info_of(const StencilParams& prm);
 
 // Capture `body(stream)` into a CUDA graph, launch it on `s`, wait for it.

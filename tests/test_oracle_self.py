@@ -156,3 +156,20 @@ def test_oracle_reproduces_headline_golden_digests():
     o.gs7_steps(2, 3, 0, 1, *prm, steps=1)
     _, d, m = o.export()
     assert G.field_digest(d[0], d[1], m, len(keys)) == gold["checkpoints"]["2"]
+
+
+def test_heat_config0_fp32_within_1e5_of_fp64():
+    """Config 0 (heat 128^3 shell, 100 steps): the FP32 oracle, which the GPU matches bit for bit,
+    stays within 1e-5 relative of the same update in double precision at every active point."""
+    ps = W.heat_shell()
+    keys, data, mask = W.build_block_map(ps.coords, ps.values, ps.size, 8, ps.bck)
+    o = O.OracleGrid(ps.size, edge=8, ptypes=[O.T_F32] * 2)
+    o.load_map(keys, data + [data[0].copy()], mask)
+    f64 = o.heat7_f64(data[0], W.HEAT_DT, 0.0, 100)
+    o.heat7_steps(0, 1, W.HEAT_DT, 100)
+    _, d, m = o.export()
+    n = len(keys)
+    ex = (m[: n * 512] & 1).astype(bool)
+    a = d[0][: n * 512][ex].astype(np.float64)
+    b = f64[: n * 512][ex]
+    assert np.max(np.abs(a - b) / np.maximum(np.abs(b), 1e-30)) < 1e-5
