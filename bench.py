@@ -44,7 +44,7 @@ UNIT = "Gpts/s"
 ALG_BYTES_PER_PT = 17
 # the library's default launch configuration of the pipelined 8^3 kernel (automatic ring depth)
 DEFAULT_CTAS_PER_SM, DEFAULT_STAGES = "auto", "auto"
-WORKLOADS = ("gs512", "heat128", "insert1024", "batched256", "served", "ghost512", "conv1000")
+WORKLOADS = ("gs512", "heat128", "insert1024", "batched256", "served", "ghost512", "conv1000", "conv2b")
 
 
 def parse():
@@ -703,6 +703,44 @@ def run_served(args, dist: Dist):
                  gpu_launches=None, clocks=clk)
 
 
+def run_conv2b(args, dist: Dist):
+    """Gray-Scott on the 512^3 benchmark grid written as a conv2_b user lambda against the C++ header
+    (the reference's way to write a user stencil), against the library's fixed-function GS7 kernel on the
+    same grid: both Gpts/s (CUDA events, `steps` steps after `warmup`) and a one-step bit-for-bit check.
+    Runs openfpm_data_b200/bench_conv.cu, built like the drop-in test."""
+    from openfpm_data_b200 import build as B
+    from openfpm_data_b200 import workloads as W
+    exe = B.build_conv_bench()
+    ps = W.gray_scott()
+    keys, data, mask = W.build_block_map(ps.coords, ps.values, ps.size, 8, ps.bck)
+    n = len(keys)
+    with tempfile.TemporaryDirectory() as td:
+        path = os.path.join(td, "map.bin")
+        with open(path, "wb") as fh:
+            fh.write(np.int64(n).tobytes())
+            fh.write(keys.astype(np.int64).tobytes())
+            for d, b in zip(data, ps.bck):
+                fh.write(np.concatenate([d, np.full(512, b, np.float32)]).astype(np.float32).tobytes())
+            fh.write(np.concatenate([mask, np.zeros(512, np.uint8)]).tobytes())
+        # the program runs on its device 0: this rank's GPU
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+        devs = vis.split(",") if vis else [str(i) for i in range(dist.local + 1)]
+        env = dict(os.environ, CUDA_VISIBLE_DEVICES=devs[dist.local] if dist.local < len(devs) else str(dist.local))
+        r = subprocess.run([exe, path, str(max(1, args.steps)), str(max(3, args.warmup))], capture_output=True,
+                           text=True, timeout=900, env=env)
+    if r.returncode != 0:
+        raise RuntimeError(f"bench_conv failed ({r.returncode}): {r.stderr[-500:]}")
+    res = json.loads([ln for ln in r.stdout.splitlines() if ln.startswith("{")][-1])
+    steps = res["steps"]
+    t = res["active_points"] * steps / (res["conv2_b_gpts"] * 1e9)
+    return _line("conv2_b user-lambda Gray-Scott Gpts/s (512^3 sparse grid)", res["conv2_b_gpts"], "Gpts/s", dist,
+                 args, steps, t, {"workload": "gray_scott_512^3_chunk8^3_40balls_seed1", "route": "conv2_b lambda",
+                                  "fixed_function_gs7_gpts": res["gs7_gpts"],
+                                  "conv2_b_over_gs7": res["conv2_b_over_gs7"],
+                                  "one_step_bit_equal_to_gs7": res["one_step_bit_equal"]},
+                 roofline=None, cpu_baseline=None, e2e=None, gpu_launches=steps, clocks=None)
+
+
 def _ghost_boxes(size=512, width=1):
     """The six ghost slabs of a 2x2x2 decomposition of the 512^3 grid: for each
     mid-plane, the `width` layers on either side of it (inclusive boxes)."""
@@ -962,6 +1000,7 @@ def _sub_records(args, dist: Dist) -> dict:
         ("heat128", run_heat128, dict(steps=100, warmup=5)),
         ("insert1024", run_insert1024, dict(steps=10, warmup=8)),
         ("batched256", run_batched256, dict(steps=4, warmup=3)),
+        ("conv2b_gs512", run_conv2b, dict(steps=200, warmup=10)),
         ("served_2000rps", run_served, dict(steps=1, warmup=3, serve_rate=2000.0, serve_seconds=args.sub_serve_seconds,
                                             plain_sample=24)),
         ("served_sustained", run_served, dict(steps=1, warmup=3, serve_rate=args.sub_sustained_rate,
@@ -991,7 +1030,7 @@ def main():
         else:
             runners = {"gs512": run_ours, "heat128": run_heat128, "insert1024": run_insert1024,
                        "batched256": run_batched256, "served": run_served, "ghost512": run_ghost512,
-                       "conv1000": run_conv1000}
+                       "conv1000": run_conv1000, "conv2b": run_conv2b}
             line = runners[args.workload](args, dist)
             if args.workload == "gs512" and not args.no_sub_records:
                 subs = _sub_records(args, dist)

@@ -258,12 +258,24 @@ struct cross_stencil {
     T xp[dim];
 };
 
+// Layout of a chunk plus its one-point halo in shared memory: (E+2) x (E+2) rows of RS elements,
+// x = -1 .. E at elements X0 - 1 .. X0 + E, so that every row's E interior elements start on a
+// 16-byte boundary (they are copied 16 bytes at a time).
+template <typename T, int E>
+struct tile_layout {
+    static constexpr int X0 = sizeof(T) >= 16 ? 1 : 16 / (int)sizeof(T);
+    static constexpr int RS = ((X0 + E + 1 + X0 - 1) / X0) * X0;  // X0 - 1 .. X0 + E, rounded to X0
+    static constexpr int T2 = E + 2;
+    static constexpr int SIZE = RS * T2 * T2;
+    __host__ __device__ static constexpr int index(int i, int j, int k) { return X0 + i + RS * ((j + 1) + T2 * (k + 1)); }
+};
+
 // halo-indexed tile accessor (src/SparseGrid/cp_block.hpp:14-97): u(i, j, k)
 // for local coordinates i, j, k in [-1, edge]
 template <typename T, int E>
 struct cp_block {
     T* ptr;
-    __device__ T& operator()(int i, int j, int k) const { return ptr[(i + 1) + (E + 2) * ((j + 1) + (E + 2) * (k + 1))]; }
+    __device__ T& operator()(int i, int j, int k) const { return ptr[tile_layout<T, E>::index(i, j, k)]; }
 };
 
 // chunk data handle passed to conv2_b functions: block.template get<p>()[offset]
@@ -310,6 +322,15 @@ __host__ __device__ inline void block_coords(int zorder, const int64_t* bsz, int
         bc[2] = (int64_t)morton_compact3((uint64_t)key >> 2);
         return;
     }
+    if (key >= 0 && key <= 0xffffffffLL && bsz[0] <= 0xffffffffLL && bsz[1] <= 0xffffffffLL) {
+        // the same quotients in 32-bit arithmetic (a 64-bit division is a long software sequence)
+        const uint32_t k = (uint32_t)key, b0 = (uint32_t)bsz[0], b1 = (uint32_t)bsz[1];
+        const uint32_t q = k / b0;
+        bc[0] = (int64_t)(k - q * b0);
+        bc[1] = (int64_t)(q % b1);
+        bc[2] = (int64_t)(q / b1);
+        return;
+    }
     bc[0] = key % bsz[0];
     bc[1] = (key / bsz[0]) % bsz[1];
     bc[2] = key / (bsz[0] * bsz[1]);
@@ -341,84 +362,180 @@ __device__ __forceinline__ int64_t find_key(const int64_t* keys, int64_t n, int6
 static __shared__ int sgb_pool_counter;
 static __shared__ int sgb_block_counter;
 
-// Generic conv kernel: one CTA per chunk, (E+2)^3 tiles of the NP source
-// fields in shared memory (faces always, edges and corners with an NNFull
-// table), the user function called for every active point inside the box.
-template <int E, int NP, int MODE, typename F>
-__global__ void conv_kernel(sgb_view v, int src0, int src1, int dst0, int dst1, Box<3, int> box, F f) {
-    constexpr int T = E + 2, TT = T * T * T, BS = E * E * E;
-    __shared__ float tile[NP][TT];
-    const float* src[2] = {static_cast<const float*>(v.data[src0]), static_cast<const float*>(v.data[src1])};
-    float* dst[2] = {static_cast<float*>(v.data[dst0]), static_cast<float*>(v.data[dst1])};
-    const float bck[2] = {src[0][v.n * BS], src[1][v.n * BS]};  // background chunk
-    for (int64_t chunk = blockIdx.x; chunk < v.n; chunk += gridDim.x) {
-        for (int cell = threadIdx.x; cell < TT; cell += blockDim.x) {
-            const int tx = cell % T, ty = (cell / T) % T, tz = cell / (T * T);
-            const int dx = tx == 0 ? -1 : (tx == T - 1 ? 1 : 0), dy = ty == 0 ? -1 : (ty == T - 1 ? 1 : 0),
-                      dz = tz == 0 ? -1 : (tz == T - 1 ? 1 : 0);
-            const int nz = (dx != 0) + (dy != 0) + (dz != 0);
-            int64_t sc = chunk;
-            if (nz) {
-                // NNFull: the 26 neighbours; NNStar: faces read their neighbour, edge and corner cells
-                // read neighbour 0 (the -x chunk) at the wrapped local coordinate, as the reference's
-                // ghost-layer map does (NNStar::getNNskin, SparseGridGpu_ker_util.hpp:114-139)
-                if (v.nn_kind == SGB_NN_FULL) sc = v.nn[chunk * 27 + (dx + 1) + 3 * (dy + 1) + 9 * (dz + 1)];
-                else sc = v.nn[chunk * 8 + (nz > 1 ? 0 : dx ? (dx < 0 ? 0 : 1) : dy ? (dy < 0 ? 2 : 3) : (dz < 0 ? 4 : 5))];
+// cp.async copies of one element (4 or 8 bytes) into shared memory; other sizes are copied by the
+// thread itself
+template <typename T>
+__device__ __forceinline__ void async_copy_elem(T* dst_smem, const T* src) {
+    if constexpr (sizeof(T) == 4 || sizeof(T) == 8) {
+        asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"((unsigned)__cvta_generic_to_shared(dst_smem)),
+                     "l"(src), "n"((int)sizeof(T))
+                     : "memory");
+    } else {
+        *dst_smem = *src;
+    }
+}
+__device__ __forceinline__ void async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void async_wait_one() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+__device__ __forceinline__ void async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// Conv kernel for user lambdas: each CTA takes chunks blockIdx.x, + gridDim.x, ... and keeps two
+// halo tiles per source field in shared memory (tile_layout).  While one chunk is computed from one
+// tile, the next chunk's tile is gathered into the other by cp.async copies, row by row: the E
+// interior elements of a row in 16-byte copies from the chunk the row lies in (the chunk itself, a
+// face neighbour, or for rows along a halo edge the edge neighbour under NNFull and neighbour 0, the
+// -x chunk, at the wrapped coordinate under NNStar, as the reference's ghost-layer map gives them),
+// the two x-halo elements one by one.  Absent chunks give the background.  The next chunk's
+// neighbour row and key are fetched one chunk earlier still.  The lambda runs for every active point
+// inside the box (conv_cross writes every point of the chunk).
+template <typename T>
+__device__ __forceinline__ void async_copy16(T* dst_smem, const T* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((unsigned)__cvta_generic_to_shared(dst_smem)),
+                 "l"(src)
+                 : "memory");
+}
+
+template <int E, int NP, int MODE, typename T0, typename T1, typename U0, typename U1, typename F>
+__global__ void __launch_bounds__(256) conv_kernel(sgb_view v, int src0, int src1, int dst0, int dst1,
+                                                   Box<3, int> box, T0 bk0, T1 bk1, F f) {
+    using L0 = tile_layout<T0, E>;
+    using L1 = tile_layout<T1, E>;
+    constexpr int BS = E * E * E, T2 = E + 2, ROWS = T2 * T2;
+    __shared__ __align__(16) T0 tile0[2][L0::SIZE];
+    __shared__ __align__(16) T1 tile1[2][NP == 2 ? L1::SIZE : 16];
+    __shared__ int32_t nnrow[2][27];
+    const T0* s0 = static_cast<const T0*>(v.data[src0]);
+    const T1* s1 = static_cast<const T1*>(v.data[src1]);
+    U0* d0 = static_cast<U0*>(v.data[dst0]);
+    U1* d1 = static_cast<U1*>(v.data[dst1]);
+    const int kn = v.nn_kind == SGB_NN_FULL ? 27 : 8;
+    const int tid = threadIdx.x;
+    const int64_t stride = gridDim.x;
+    int64_t c = blockIdx.x;
+    if (c >= v.n) return;
+    auto fetch = [&](int64_t ch, int32_t& row, int64_t& key) {
+        row = (ch < v.n && tid < kn) ? v.nn[ch * kn + tid] : -1;
+        key = ch < v.n ? v.keys[ch] : 0;
+    };
+    // chunk position holding halo offset (dx, dy, dz) of chunk ch (nz of them non-zero), -1 absent
+    auto source = [&](int64_t ch, int b, int dx, int dy, int dz) -> int64_t {
+        const int nz = (dx != 0) + (dy != 0) + (dz != 0);
+        if (nz == 0) return ch;
+        if (kn == 27) return nnrow[b][(dx + 1) + 3 * (dy + 1) + 9 * (dz + 1)];
+        return nnrow[b][nz > 1 ? 0 : dx ? (dx < 0 ? 0 : 1) : dy ? (dy < 0 ? 2 : 3) : (dz < 0 ? 4 : 5)];
+    };
+    // work item w of a tile: row w / 4 ((j, k) from -1 .. E), part w % 4: interior halves 0 and 1
+    // (16-byte copies; a row is split in two whenever it is 32 bytes or more), or the x-halo elements
+    // 2 (x = -1) and 3 (x = E)
+    auto gather_field = [&](auto* tile, const auto* src, auto bk, int64_t ch, int b) {
+        using T = typename std::remove_cv<typename std::remove_pointer<decltype(src)>::type>::type;
+        using LT = tile_layout<T, E>;
+        constexpr bool vec = (E * sizeof(T)) % 16 == 0;
+        constexpr int VPR = vec ? (int)(E * sizeof(T) / 16) : 0;  // 16-byte pieces per row interior
+        constexpr int PARTS = vec ? VPR + 2 : E + 2;
+        for (int w = tid; w < ROWS * PARTS; w += blockDim.x) {
+            const int r = w / PARTS, part = w % PARTS;
+            const int j = r % T2 - 1, k = r / T2 - 1;
+            const int dy = j < 0 ? -1 : (j >= E ? 1 : 0), dz = k < 0 ? -1 : (k >= E ? 1 : 0);
+            const int ly = (j + E) % E, lz = (k + E) % E;
+            T* rowp = tile + LT::index(0, j, k);
+            if (vec && part < VPR) {  // 16 bytes of the row's interior
+                const int64_t sc = source(ch, b, 0, dy, dz);
+                const int e0 = part * (16 / (int)sizeof(T));
+                if (sc >= 0) {
+                    async_copy16(rowp + e0, src + sc * BS + E * (ly + E * lz) + e0);
+                } else {
+#pragma unroll
+                    for (int q = 0; q < 16 / (int)sizeof(T); ++q) rowp[e0 + q] = bk;
+                }
+            } else {
+                // vec: the x-halo elements (part VPR: x = -1, VPR + 1: x = E); otherwise element i - 1
+                const int i = vec ? (part == VPR ? -1 : E) : part - 1;
+                const int dx = i < 0 ? -1 : (i >= E ? 1 : 0);
+                const int64_t sc = source(ch, b, dx, dy, dz);
+                const int lx = (i + E) % E;
+                if (sc >= 0) async_copy_elem(rowp + i, src + sc * BS + lx + E * (ly + E * lz));
+                else rowp[i] = bk;
             }
-            const int lx = (tx - 1 + E) % E, ly = (ty - 1 + E) % E, lz = (tz - 1 + E) % E;
-            const int64_t idx = sc * BS + lx + E * (ly + E * lz);
-            for (int p = 0; p < NP; ++p) tile[p][cell] = sc >= 0 ? src[p][idx] : bck[p];
         }
+    };
+    auto gather = [&](int64_t ch, int b) {
+        gather_field(tile0[b], s0, bk0, ch, b);
+        if (NP == 2) gather_field(tile1[b], s1, bk1, ch, b);
+        async_commit();
+    };
+    int32_t row;
+    int64_t key_cur, key_next, key_far;
+    fetch(c, row, key_cur);
+    if (tid < kn) nnrow[0][tid] = row;
+    fetch(c + stride, row, key_next);
+    __syncthreads();
+    gather(c, 0);
+    for (int b = 0; c < v.n; c += stride, b ^= 1) {
+        const int64_t cn = c + stride;
+        // the next chunk's neighbour row to shared memory (the gather that read that buffer last is
+        // complete: every thread passed the barriers of the last iteration)
+        if (tid < kn) nnrow[b ^ 1][tid] = row;
+        fetch(cn + stride, row, key_far);
+        __syncthreads();  // row visible; every thread is done with tile[b ^ 1] (chunk c - stride)
+        if (cn < v.n) gather(cn, b ^ 1);
+        else async_commit();  // an empty group keeps the count of groups in flight uniform
+        async_wait_one();     // this chunk's gather has landed
         __syncthreads();
         int64_t bcd[3];
-        detail::block_coords(v.zorder, v.bsz, v.keys[chunk], bcd);
+        detail::block_coords(v.zorder, v.bsz, key_cur, bcd);
         const int64_t bx = bcd[0], by = bcd[1], bz = bcd[2];
-        for (int pnt = threadIdx.x; pnt < BS; pnt += blockDim.x) {
+        for (int pnt = tid; pnt < BS; pnt += blockDim.x) {
             const int i = pnt % E, j = (pnt / E) % E, k = pnt / (E * E);
-            const uint8_t m = v.mask[chunk * BS + pnt];
+            const uint8_t m = v.mask[c * BS + pnt];
             const int64_t gx = bx * E + i, gy = by * E + j, gz = bz * E + k;
             const bool in = gx >= box.lo[0] && gx <= box.hi[0] && gy >= box.lo[1] && gy <= box.hi[1] &&
                             gz >= box.lo[2] && gz <= box.hi[2];
             const bool act = (m & 1) && !(m & 2) && in;
-            const int c = (i + 1) + T * ((j + 1) + T * (k + 1));
-            const int64_t g = chunk * BS + pnt;
+            const int64_t g = c * BS + pnt;
+            const T0* t0 = tile0[b];
             if constexpr (MODE == 0) {  // conv_cross: storeBlock of the whole chunk
-                float res = tile[0][c];
+                const int cc = L0::index(i, j, k);
+                T0 res = t0[cc];
                 if (act) {
-                    cross_stencil<3, float> cs;
-                    cs.xm[0] = tile[0][c - 1];
-                    cs.xp[0] = tile[0][c + 1];
-                    cs.xm[1] = tile[0][c - T];
-                    cs.xp[1] = tile[0][c + T];
-                    cs.xm[2] = tile[0][c - T * T];
-                    cs.xp[2] = tile[0][c + T * T];
-                    float u = tile[0][c];
+                    cross_stencil<3, T0> cs;
+                    cs.xm[0] = t0[cc - 1];
+                    cs.xp[0] = t0[cc + 1];
+                    cs.xm[1] = t0[cc - L0::RS];
+                    cs.xp[1] = t0[cc + L0::RS];
+                    cs.xm[2] = t0[cc - L0::RS * T2];
+                    cs.xp[2] = t0[cc + L0::RS * T2];
+                    T0 u = t0[cc];
                     res = f(u, cs);
                 }
-                dst[0][g] = res;
+                d0[g] = (U0)res;
             } else if (act) {
-                cp_block<float, E> u{tile[0]}, w{tile[NP - 1]};
+                cp_block<T0, E> u{const_cast<T0*>(t0)};
+                cp_block<T1, E> w{const_cast<T1*>(tile1[NP == 2 ? b : 0])};
                 if constexpr (MODE == 1) {  // conv
-                    dst[0][g] = f(u, i, j, k);
+                    d0[g] = (U0)f(u, i, j, k);
                 } else if constexpr (MODE == 2) {  // conv2
-                    float r1 = 0, r2 = 0;
+                    U0 r1 = 0;
+                    U1 r2 = 0;
                     f(r1, r2, u, w, i, j, k);
-                    dst[0][g] = r1;
-                    dst[1][g] = r2;
+                    d0[g] = r1;
+                    d1[g] = r2;
                 } else if constexpr (MODE == 3) {  // conv2_b
-                    float r1 = 0, r2 = 0;
-                    data_block<8> blk{v.data, chunk, BS};
+                    U0 r1 = 0;
+                    U1 r2 = 0;
+                    data_block<8> blk{v.data, c, BS};
                     f(r1, r2, u, w, blk, pnt, i, j, k);
-                    dst[0][g] = r1;
-                    dst[1][g] = r2;
+                    d0[g] = r1;
+                    d1[g] = r2;
                 } else {  // conv_cross_b: the chunk's data block and the point's offset as well
-                    data_block<8> blk{v.data, chunk, BS};
-                    dst[0][g] = f(u, blk, pnt, i, j, k);
+                    data_block<8> blk{v.data, c, BS};
+                    d0[g] = (U0)f(u, blk, pnt, i, j, k);
                 }
             }
         }
-        __syncthreads();
+        key_cur = key_next;
+        key_next = key_far;
     }
+    async_wait_all();
 }
 }  // namespace detail
 
@@ -1027,28 +1144,29 @@ class SparseGridGpu {
     // conv family with user __device__ functions (SparseGridGpu.hpp:2568-2683)
     template <unsigned p_src, unsigned p_dst, unsigned stencil_size, typename F>
     void conv_cross(grid_key_dx<3> start, grid_key_dx<3> stop, F f) {
-        launch_conv<1, 0>(p_src, p_src, p_dst, p_dst, start, stop, f);
+        launch_conv<1, 0, p_src, p_src, p_dst, p_dst>(start, stop, f);
     }
     template <unsigned p_src, unsigned p_dst, unsigned stencil_size, typename F>
     void conv(grid_key_dx<3> start, grid_key_dx<3> stop, F f) {
-        launch_conv<1, 1>(p_src, p_src, p_dst, p_dst, start, stop, f);
+        launch_conv<1, 1, p_src, p_src, p_dst, p_dst>(start, stop, f);
     }
     // conv_cross_b (SparseGridGpu.hpp:2606-2621): f(cp_block, data_block, offset, i, j, k) over the
-    // NNStar halo (edge and corner cells read the background), written at active points
+    // NNStar halo (edge and corner cells read neighbour 0 as the reference's ghost-layer map does),
+    // written at active points
     template <unsigned p_src, unsigned p_dst, unsigned stencil_size, typename F>
     void conv_cross_b(grid_key_dx<3> start, grid_key_dx<3> stop, F f) {
         const int keep = nn_kind_;
         nn_kind_ = SGB_NN_STAR;
-        launch_conv<1, 4>(p_src, p_src, p_dst, p_dst, start, stop, f);
+        launch_conv<1, 4, p_src, p_src, p_dst, p_dst>(start, stop, f);
         nn_kind_ = keep;
     }
     template <unsigned s1, unsigned s2, unsigned d1, unsigned d2, unsigned stencil_size, typename F>
     void conv2(grid_key_dx<3> start, grid_key_dx<3> stop, F f) {
-        launch_conv<2, 2>(s1, s2, d1, d2, start, stop, f);
+        launch_conv<2, 2, s1, s2, d1, d2>(start, stop, f);
     }
     template <unsigned s1, unsigned s2, unsigned d1, unsigned d2, unsigned stencil_size, typename F>
     void conv2_b(grid_key_dx<3> start, grid_key_dx<3> stop, F f) {
-        launch_conv<2, 3>(s1, s2, d1, d2, start, stop, f);
+        launch_conv<2, 3, s1, s2, d1, d2>(start, stop, f);
     }
 
     // deviceToHost<p...>(): the block map and listed properties to host copies
@@ -1489,16 +1607,27 @@ class SparseGridGpu {
         }
     }
 
-    template <int NP, int MODE, typename F>
-    void launch_conv(unsigned s1, unsigned s2, unsigned d1, unsigned d2, grid_key_dx<3> start, grid_key_dx<3> stop,
-                     F f) {
+    template <int NP, int MODE, unsigned s1, unsigned s2, unsigned d1, unsigned d2, typename F>
+    void launch_conv(grid_key_dx<3> start, grid_key_dx<3> stop, F f) {
+        using T0 = typename std::tuple_element<s1, props>::type;
+        using T1 = typename std::tuple_element<s2, props>::type;
+        using U0 = typename std::tuple_element<d1, props>::type;
+        using U1 = typename std::tuple_element<d2, props>::type;
         sgb_view v;
         check(sgb_get_view(g_, nn_kind_, &v, nullptr), "conv");
         if (v.n == 0) return;
         Box<3, int> box;
         for (int i = 0; i < 3; ++i) box.lo[i] = (int)start.get(i), box.hi[i] = (int)stop.get(i);
-        const unsigned blocks = (unsigned)(v.n < 148 * 8 ? v.n : 148 * 8);
-        detail::conv_kernel<blockEdgeSize, NP, MODE><<<blocks, 256>>>(v, (int)s1, (int)s2, (int)d1, (int)d2, box, f);
+        T0 b0;
+        T1 b1;
+        std::memcpy(&b0, &bck_raw_[s1], sizeof(T0));
+        std::memcpy(&b1, &bck_raw_[s2], sizeof(T1));
+        int sms = 148;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
+        const int64_t cap = (int64_t)sms * 8;  // eight 256-thread CTAs per SM
+        const unsigned blocks = (unsigned)(v.n < cap ? v.n : cap);
+        detail::conv_kernel<blockEdgeSize, NP, MODE, T0, T1, U0, U1>
+            <<<blocks, 256>>>(v, (int)s1, (int)s2, (int)d1, (int)d2, box, b0, b1, f);
         check(cudaGetLastError() == cudaSuccess ? SGB_OK : SGB_ECUDA, "conv launch");
         if (MODE == 0) {
             // storeBlock semantics put source values into the destination's

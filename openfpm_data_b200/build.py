@@ -101,8 +101,34 @@ def build_dropin_test(force: bool = False, verbose: bool = False) -> str:
     return DROPIN_BIN
 
 
+CONV_BENCH_SRC = os.path.join(HERE, "bench_conv.cu")
+CONV_BENCH_BIN = os.path.join(OBJ_DIR, "bench_conv")
+
+
+def build_conv_bench(force: bool = False, verbose: bool = False) -> str:
+    """Compile the conv2_b-vs-GS7 throughput program (user lambda code against the C++ header)."""
+    lib = build(verbose=verbose)
+    deps = [CONV_BENCH_SRC, lib] + glob.glob(os.path.join(ROOT, "include", "**", "*.h*"), recursive=True)
+    if not force and os.path.exists(CONV_BENCH_BIN) and all(os.path.getmtime(d) <= os.path.getmtime(CONV_BENCH_BIN)
+                                                            for d in deps):
+        return CONV_BENCH_BIN
+    os.makedirs(OBJ_DIR, exist_ok=True)
+    nvcc = os.environ.get("NVCC", "nvcc")
+    tmp = CONV_BENCH_BIN + ".tmp"
+    cmd = [nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
+           "--extended-lambda", "-ftz=true", "-fmad=true", "-I", os.path.join(ROOT, "include"),
+           "-o", tmp, CONV_BENCH_SRC, "-L", HERE, "-lsgb200", "-Xlinker", "-rpath,$ORIGIN/.."]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+    os.replace(tmp, CONV_BENCH_BIN)
+    return CONV_BENCH_BIN
+
+
 if __name__ == "__main__":
     build(force="--force" in sys.argv, verbose=True)
     print(LIB)
     if "--dropin" in sys.argv:
         print(build_dropin_test(force="--force" in sys.argv, verbose=True))
+    if "--conv-bench" in sys.argv:
+        print(build_conv_bench(force="--force" in sys.argv, verbose=True))
