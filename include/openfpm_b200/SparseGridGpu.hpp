@@ -258,16 +258,19 @@ struct cross_stencil {
     T xp[dim];
 };
 
-// Layout of a chunk plus its one-point halo in shared memory: (E+2) x (E+2) rows of RS elements,
-// x = -1 .. E at elements X0 - 1 .. X0 + E, so that every row's E interior elements start on a
-// 16-byte boundary (they are copied 16 bytes at a time).
+// Layout of a chunk plus its one-point halo in shared memory: E + 2 planes of E + 2 rows of RS
+// elements, x = -1 .. E at elements X0 - 1 .. X0 + E, so that every row's E interior elements start
+// on a 16-byte boundary (they are copied 16 bytes at a time).  For 4-byte types the plane stride PS
+// is padded to 8 banks past a multiple of 32: a warp reading 8 x 2 x 2 points (two rows of two
+// planes) then touches 32 distinct banks, for the point itself and for each of its six neighbours.
 template <typename T, int E>
 struct tile_layout {
     static constexpr int X0 = sizeof(T) >= 16 ? 1 : 16 / (int)sizeof(T);
     static constexpr int RS = ((X0 + E + 1 + X0 - 1) / X0) * X0;  // X0 - 1 .. X0 + E, rounded to X0
     static constexpr int T2 = E + 2;
-    static constexpr int SIZE = RS * T2 * T2;
-    __host__ __device__ static constexpr int index(int i, int j, int k) { return X0 + i + RS * ((j + 1) + T2 * (k + 1)); }
+    static constexpr int PS = sizeof(T) == 4 ? RS * T2 + (40 - (RS * T2) % 32) % 32 : RS * T2;
+    static constexpr int SIZE = PS * T2;
+    __host__ __device__ static constexpr int index(int i, int j, int k) { return X0 + i + RS * (j + 1) + PS * (k + 1); }
 };
 
 // halo-indexed tile accessor (src/SparseGrid/cp_block.hpp:14-97): u(i, j, k)
@@ -375,8 +378,10 @@ __device__ __forceinline__ void async_copy_elem(T* dst_smem, const T* src) {
     }
 }
 __device__ __forceinline__ void async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void async_wait_one() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
-__device__ __forceinline__ void async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void async_wait_group() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
 
 // Conv kernel for user lambdas: each CTA takes chunks blockIdx.x, + gridDim.x, ... and keeps two
 // halo tiles per source field in shared memory (tile_layout).  While one chunk is computed from one
@@ -384,9 +389,10 @@ __device__ __forceinline__ void async_wait_all() { asm volatile("cp.async.wait_a
 // interior elements of a row in 16-byte copies from the chunk the row lies in (the chunk itself, a
 // face neighbour, or for rows along a halo edge the edge neighbour under NNFull and neighbour 0, the
 // -x chunk, at the wrapped coordinate under NNStar, as the reference's ghost-layer map gives them),
-// the two x-halo elements one by one.  Absent chunks give the background.  The next chunk's
-// neighbour row and key are fetched one chunk earlier still.  The lambda runs for every active point
-// inside the box (conv_cross writes every point of the chunk).
+// the two x-halo elements one by one.  Absent chunks give the background.  One barrier per chunk:
+// a thread waits for its own copies of the chunk, the barrier makes every thread's copies visible
+// and closes the reads of the other tile, and only then is the next chunk's gather issued.  The
+// lambda runs for every active point inside the box (conv_cross writes every point of the chunk).
 template <typename T>
 __device__ __forceinline__ void async_copy16(T* dst_smem, const T* src) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((unsigned)__cvta_generic_to_shared(dst_smem)),
@@ -394,105 +400,228 @@ __device__ __forceinline__ void async_copy16(T* dst_smem, const T* src) {
                  : "memory");
 }
 
+// Copy plan of one field's halo tile for thread `tid` of NT.  Work items are numbered with the
+// 16-byte pieces of the row interiors first (rows (j, k) = -1 .. E, j fastest), then the two x-halo
+// elements of every row (every element of every row when a row interior is not a multiple of 16
+// bytes); a thread takes items tid, tid + NT, ...  An item's place in the tile, its offset inside the
+// source chunk and the neighbour-table slot it reads (0 .. 26, SELF for the chunk itself) are the
+// same for every chunk, so each thread works them out once.
+template <typename T, int E, int NT>
+struct tile_plan {
+    using LT = tile_layout<T, E>;
+    static constexpr int T2 = E + 2, ROWS = T2 * T2, BS = E * E * E, SELF = 27;
+    static constexpr bool VEC = sizeof(T) <= 16 && (E * sizeof(T)) % 16 == 0;
+    static constexpr int PER = VEC ? 16 / (int)sizeof(T) : 1;  // elements of a piece
+    static constexpr int VPR = VEC ? E / PER : 0;               // pieces per row interior
+    static constexpr int NVEC = ROWS * VPR;
+    static constexpr int NITEM = NVEC + ROWS * (VEC ? 2 : E + 2);
+    static constexpr int ITEMS = (NITEM + NT - 1) / NT;
+    int toff[ITEMS];  // element offset in the tile; -1: no item
+    int soff[ITEMS];  // element offset in the source chunk | slot << 16
+
+    __device__ static int slot_of(int kn, int dx, int dy, int dz) {
+        const int nz = (dx != 0) + (dy != 0) + (dz != 0);
+        if (nz == 0) return SELF;
+        if (kn == 27) return (dx + 1) + 3 * (dy + 1) + 9 * (dz + 1);
+        return nz > 1 ? 0 : dx ? (dx < 0 ? 0 : 1) : dy ? (dy < 0 ? 2 : 3) : (dz < 0 ? 4 : 5);
+    }
+    __device__ void init(int tid, int kn) {
+#pragma unroll
+        for (int q = 0; q < ITEMS; ++q) {
+            const int w = tid + q * NT;
+            toff[q] = -1;
+            soff[q] = 0;
+            if (w >= NITEM) continue;
+            int r, i;
+            if (w < NVEC) {
+                r = w / (VPR > 0 ? VPR : 1);
+                i = (w % (VPR > 0 ? VPR : 1)) * PER;
+            } else if (VEC) {
+                r = (w - NVEC) / 2;
+                i = (w - NVEC) % 2 ? E : -1;
+            } else {
+                r = (w - NVEC) / (E + 2);
+                i = (w - NVEC) % (E + 2) - 1;
+            }
+            const int j = r % T2 - 1, k = r / T2 - 1;
+            const int dx = i < 0 ? -1 : (i >= E ? 1 : 0), dy = j < 0 ? -1 : (j >= E ? 1 : 0),
+                      dz = k < 0 ? -1 : (k >= E ? 1 : 0);
+            const int lx = (i + E) % E, ly = (j + E) % E, lz = (k + E) % E;
+            toff[q] = LT::index(i, j, k);
+            soff[q] = (lx + E * (ly + E * lz)) | slot_of(kn, dx, dy, dz) << 16;
+        }
+    }
+    // issue this thread's copies of chunk table `nnrow` (slot SELF: the chunk) into `tile`; with
+    // NF == 2 the same items of a second field of the same type as well
+    template <int NF>
+    __device__ void issue(int tid, const int32_t* nnrow, T* tile, const T* src, T bk, T* tile2, const T* src2,
+                          T bk2) const {
+#pragma unroll
+        for (int q = 0; q < ITEMS; ++q) {
+            if (toff[q] < 0) continue;
+            const int sc = nnrow[soff[q] >> 16];
+            const int64_t so = (int64_t)sc * BS + (soff[q] & 0xffff);
+            if (VEC && tid + q * NT < NVEC) {
+                if (sc >= 0) {
+                    async_copy16(tile + toff[q], src + so);
+                    if (NF == 2) async_copy16(tile2 + toff[q], src2 + so);
+                } else {
+#pragma unroll
+                    for (int e = 0; e < PER; ++e) {
+                        tile[toff[q] + e] = bk;
+                        if (NF == 2) tile2[toff[q] + e] = bk2;
+                    }
+                }
+            } else {
+                if (sc >= 0) {
+                    async_copy_elem(tile + toff[q], src + so);
+                    if (NF == 2) async_copy_elem(tile2 + toff[q], src2 + so);
+                } else {
+                    tile[toff[q]] = bk;
+                    if (NF == 2) tile2[toff[q]] = bk2;
+                }
+            }
+        }
+    }
+};
+
 template <int E, int NP, int MODE, typename T0, typename T1, typename U0, typename U1, typename F>
-__global__ void __launch_bounds__(256) conv_kernel(sgb_view v, int src0, int src1, int dst0, int dst1,
-                                                   Box<3, int> box, T0 bk0, T1 bk1, F f) {
+__global__ void __launch_bounds__(256, 6) conv_kernel(sgb_view v, int src0, int src1, int dst0, int dst1,
+                                                      Box<3, int> box, int full_box, T0 bk0, T1 bk1, F f) {
+    constexpr int NT = 256;
     using L0 = tile_layout<T0, E>;
-    using L1 = tile_layout<T1, E>;
-    constexpr int BS = E * E * E, T2 = E + 2, ROWS = T2 * T2;
-    __shared__ __align__(16) T0 tile0[2][L0::SIZE];
-    __shared__ __align__(16) T1 tile1[2][NP == 2 ? L1::SIZE : 16];
-    __shared__ int32_t nnrow[2][27];
+    using P0 = tile_plan<T0, E, NT>;
+    using P1 = tile_plan<T1, E, NT>;
+    constexpr bool SAME = std::is_same<T0, T1>::value;
+    constexpr int BS = E * E * E, NPT = (BS + NT - 1) / NT;
+    constexpr int NB = 2;  // halo tiles per field: chunks s + 1 .. s + NB - 1 are in flight while s computes
+    constexpr int M = NB + 1;    // slots of per-chunk metadata (neighbour row, box)
+    constexpr bool BITS = E <= 10;  // box as one bit per in-box x, y and z, or lo / hi per dimension
+    constexpr int NBW = BITS ? 1 : 6;
+    __shared__ __align__(16) T0 tile0[NB][L0::SIZE];
+    __shared__ __align__(16) T1 tile1[NB][NP == 2 ? tile_layout<T1, E>::SIZE : 16];
+    __shared__ int32_t nnrow[M][28];
+    __shared__ int32_t boxc[M][NBW];
     const T0* s0 = static_cast<const T0*>(v.data[src0]);
     const T1* s1 = static_cast<const T1*>(v.data[src1]);
     U0* d0 = static_cast<U0*>(v.data[dst0]);
     U1* d1 = static_cast<U1*>(v.data[dst1]);
     const int kn = v.nn_kind == SGB_NN_FULL ? 27 : 8;
     const int tid = threadIdx.x;
-    const int64_t stride = gridDim.x;
-    int64_t c = blockIdx.x;
-    if (c >= v.n) return;
-    auto fetch = [&](int64_t ch, int32_t& row, int64_t& key) {
-        row = (ch < v.n && tid < kn) ? v.nn[ch * kn + tid] : -1;
-        key = ch < v.n ? v.keys[ch] : 0;
-    };
-    // chunk position holding halo offset (dx, dy, dz) of chunk ch (nz of them non-zero), -1 absent
-    auto source = [&](int64_t ch, int b, int dx, int dy, int dz) -> int64_t {
-        const int nz = (dx != 0) + (dy != 0) + (dz != 0);
-        if (nz == 0) return ch;
-        if (kn == 27) return nnrow[b][(dx + 1) + 3 * (dy + 1) + 9 * (dz + 1)];
-        return nnrow[b][nz > 1 ? 0 : dx ? (dx < 0 ? 0 : 1) : dy ? (dy < 0 ? 2 : 3) : (dz < 0 ? 4 : 5)];
-    };
-    // work item w of a tile: row w / 4 ((j, k) from -1 .. E), part w % 4: interior halves 0 and 1
-    // (16-byte copies; a row is split in two whenever it is 32 bytes or more), or the x-halo elements
-    // 2 (x = -1) and 3 (x = E)
-    auto gather_field = [&](auto* tile, const auto* src, auto bk, int64_t ch, int b) {
-        using T = typename std::remove_cv<typename std::remove_pointer<decltype(src)>::type>::type;
-        using LT = tile_layout<T, E>;
-        constexpr bool vec = (E * sizeof(T)) % 16 == 0;
-        constexpr int VPR = vec ? (int)(E * sizeof(T) / 16) : 0;  // 16-byte pieces per row interior
-        constexpr int PARTS = vec ? VPR + 2 : E + 2;
-        for (int w = tid; w < ROWS * PARTS; w += blockDim.x) {
-            const int r = w / PARTS, part = w % PARTS;
-            const int j = r % T2 - 1, k = r / T2 - 1;
-            const int dy = j < 0 ? -1 : (j >= E ? 1 : 0), dz = k < 0 ? -1 : (k >= E ? 1 : 0);
-            const int ly = (j + E) % E, lz = (k + E) % E;
-            T* rowp = tile + LT::index(0, j, k);
-            if (vec && part < VPR) {  // 16 bytes of the row's interior
-                const int64_t sc = source(ch, b, 0, dy, dz);
-                const int e0 = part * (16 / (int)sizeof(T));
-                if (sc >= 0) {
-                    async_copy16(rowp + e0, src + sc * BS + E * (ly + E * lz) + e0);
-                } else {
-#pragma unroll
-                    for (int q = 0; q < 16 / (int)sizeof(T); ++q) rowp[e0 + q] = bk;
-                }
+    const int64_t stride = gridDim.x, c0 = blockIdx.x;
+    if (c0 >= v.n) return;
+    // this CTA's chunks are c0, c0 + stride, ...: chunk number s is at position c0 + s * stride
+    const int64_t nmine = (v.n - c0 + stride - 1) / stride;
+    auto pos = [&](int64_t s) { return c0 + s * stride; };
+    P0 plan0;
+    P1 plan1;
+    plan0.init(tid, kn);
+    if (NP == 2 && !SAME) plan1.init(tid, kn);
+    auto gather = [&](int64_t s) {  // chunk number s into tile s % NB (its metadata in slot s % M)
+        if (s < nmine) {
+            const int b = (int)(s % NB), m = (int)(s % M);
+            if constexpr (NP == 2 && SAME) {
+                plan0.template issue<2>(tid, nnrow[m], tile0[b], s0, bk0, reinterpret_cast<T0*>(tile1[b]),
+                                        reinterpret_cast<const T0*>(s1), (T0)bk1);
             } else {
-                // vec: the x-halo elements (part VPR: x = -1, VPR + 1: x = E); otherwise element i - 1
-                const int i = vec ? (part == VPR ? -1 : E) : part - 1;
-                const int dx = i < 0 ? -1 : (i >= E ? 1 : 0);
-                const int64_t sc = source(ch, b, dx, dy, dz);
-                const int lx = (i + E) % E;
-                if (sc >= 0) async_copy_elem(rowp + i, src + sc * BS + lx + E * (ly + E * lz));
-                else rowp[i] = bk;
+                plan0.template issue<1>(tid, nnrow[m], tile0[b], s0, bk0, nullptr, nullptr, bk0);
+                if constexpr (NP == 2) plan1.template issue<1>(tid, nnrow[m], tile1[b], s1, bk1, nullptr, nullptr, bk1);
             }
         }
+        async_commit();  // one group per chunk number, empty past the end
     };
-    auto gather = [&](int64_t ch, int b) {
-        gather_field(tile0[b], s0, bk0, ch, b);
-        if (NP == 2) gather_field(tile1[b], s1, bk1, ch, b);
-        async_commit();
-    };
-    int32_t row;
-    int64_t key_cur, key_next, key_far;
-    fetch(c, row, key_cur);
-    if (tid < kn) nnrow[0][tid] = row;
-    fetch(c + stride, row, key_next);
-    __syncthreads();
-    gather(c, 0);
-    for (int b = 0; c < v.n; c += stride, b ^= 1) {
-        const int64_t cn = c + stride;
-        // the next chunk's neighbour row to shared memory (the gather that read that buffer last is
-        // complete: every thread passed the barriers of the last iteration)
-        if (tid < kn) nnrow[b ^ 1][tid] = row;
-        fetch(cn + stride, row, key_far);
-        __syncthreads();  // row visible; every thread is done with tile[b ^ 1] (chunk c - stride)
-        if (cn < v.n) gather(cn, b ^ 1);
-        else async_commit();  // an empty group keeps the count of groups in flight uniform
-        async_wait_one();     // this chunk's gather has landed
-        __syncthreads();
+    auto row_of = [&](int64_t s) { return (s < nmine && tid < kn) ? v.nn[pos(s) * kn + tid] : -1; };
+    auto box_of = [&](int64_t key, int32_t* out) {
         int64_t bcd[3];
-        detail::block_coords(v.zorder, v.bsz, key_cur, bcd);
-        const int64_t bx = bcd[0], by = bcd[1], bz = bcd[2];
-        for (int pnt = tid; pnt < BS; pnt += blockDim.x) {
-            const int i = pnt % E, j = (pnt / E) % E, k = pnt / (E * E);
-            const uint8_t m = v.mask[c * BS + pnt];
-            const int64_t gx = bx * E + i, gy = by * E + j, gz = bz * E + k;
-            const bool in = gx >= box.lo[0] && gx <= box.hi[0] && gy >= box.lo[1] && gy <= box.hi[1] &&
-                            gz >= box.lo[2] && gz <= box.hi[2];
-            const bool act = (m & 1) && !(m & 2) && in;
-            const int64_t g = c * BS + pnt;
-            const T0* t0 = tile0[b];
+        detail::block_coords(v.zorder, v.bsz, key, bcd);
+        uint32_t w = 0;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const int64_t o = bcd[d] * E, l = box.lo[d] - o, h = box.hi[d] - o;
+            const int lo = l < 0 ? 0 : (l > E ? E : (int)l), hi = h < -1 ? -1 : (h >= E ? E - 1 : (int)h);
+            if constexpr (BITS) {
+                if (hi >= lo) w |= (((1u << (hi + 1)) - 1) & ~((1u << lo) - 1)) << (d * E);
+            } else {
+                out[2 * d] = lo;
+                out[2 * d + 1] = hi;
+            }
+        }
+        if constexpr (BITS) out[0] = (int32_t)w;
+    };
+    // metadata of chunk number s into slot s % M: its neighbour row (loaded earlier into `row`), its own
+    // position, and (thread 0, unless the box holds the whole grid) its box from `key`
+    auto publish = [&](int64_t s, int32_t row, int64_t key) {
+        if (s >= nmine) return;
+        const int m = (int)(s % M);
+        if (tid < kn) nnrow[m][tid] = row;
+        if (tid == 0) {
+            nnrow[m][P0::SELF] = (int32_t)pos(s);
+            if (!full_box) box_of(key, boxc[m]);
+        }
+    };
+    // point q of this thread, q = 0 .. NPT - 1 (offset in the chunk; i, j, k its coordinates).  In 8^3
+    // chunks a warp takes x = 0 .. 7 of rows (j, j + 1) in planes (k, k + 1).
+    auto point = [&](int q, int& i, int& j, int& k) {
+        const int w = tid + q * NT;
+        i = w % E;
+        j = E == 8 ? ((w >> 5) & 3) * 2 + ((w >> 3) & 1) : (w / E) % E;
+        k = E == 8 ? (w >> 7) * 2 + ((w >> 4) & 1) : w / (E * E);
+        return i + E * (j + E * k);
+    };
+    uint8_t m_cur[NPT], m_next[NPT];
+    auto masks_of = [&](int64_t s, uint8_t* m) {
+#pragma unroll
+        for (int q = 0; q < NPT; ++q) {
+            int i, j, k;
+            const int pnt = point(q, i, j, k);
+            m[q] = (s < nmine && (BS % NT == 0 || tid + q * NT < BS)) ? v.mask[pos(s) * BS + pnt] : (uint8_t)0;
+        }
+    };
+    auto key_of = [&](int64_t s) { return (tid == 0 && !full_box && s < nmine) ? v.keys[pos(s)] : (int64_t)0; };
+    // prologue: chunk numbers 0 .. NB - 2 in flight
+    for (int64_t s = 0; s < NB - 1; ++s) publish(s, row_of(s), key_of(s));
+    int32_t row = row_of(NB - 1);
+    int64_t key = key_of(NB - 1);
+    masks_of(0, m_cur);
+    __syncthreads();
+    for (int64_t s = 0; s < NB - 1; ++s) gather(s);
+    for (int64_t it = 0; it < nmine; ++it) {
+        // slot (it + NB - 1) % M last served chunk it - 2, whose readers are all behind the last barrier
+        publish(it + NB - 1, row, key);
+        row = row_of(it + NB);
+        key = key_of(it + NB);
+        if constexpr (NB == 2) async_wait_group<0>();
+        else async_wait_group<NB - 2>();  // this thread's copies of chunk it
+        __syncthreads();  // everyone's copies of chunk it landed; everyone is done with chunk it - 1's tile
+        gather(it + NB - 1);
+        masks_of(it + 1, m_next);
+        const int b = (int)(it % NB), mslot = (int)(it % M);
+        uint32_t bw = ~0u;
+        int lo[3] = {0, 0, 0}, hi[3] = {E - 1, E - 1, E - 1};
+        if (!full_box) {
+            if constexpr (BITS) {
+                bw = (uint32_t)boxc[mslot][0];
+            } else {
+#pragma unroll
+                for (int d = 0; d < 3; ++d) lo[d] = boxc[mslot][2 * d], hi[d] = boxc[mslot][2 * d + 1];
+            }
+        }
+        const T0* t0 = tile0[b];
+        const int64_t c = pos(it), base = c * BS;
+#pragma unroll
+        for (int q = 0; q < NPT; ++q) {
+            if (BS % NT != 0 && tid + q * NT >= BS) break;
+            int i, j, k;
+            const int pnt = point(q, i, j, k);
+            bool in;
+            if constexpr (BITS) {
+                const uint32_t pm = (1u << i) | (1u << (E + j)) | (1u << (2 * E + k));
+                in = (bw & pm) == pm;
+            } else {
+                in = i >= lo[0] && i <= hi[0] && j >= lo[1] && j <= hi[1] && k >= lo[2] && k <= hi[2];
+            }
+            const bool act = (m_cur[q] & 3) == 1 && in;
+            const int64_t g = base + pnt;
             if constexpr (MODE == 0) {  // conv_cross: storeBlock of the whole chunk
                 const int cc = L0::index(i, j, k);
                 T0 res = t0[cc];
@@ -502,8 +631,8 @@ __global__ void __launch_bounds__(256) conv_kernel(sgb_view v, int src0, int src
                     cs.xp[0] = t0[cc + 1];
                     cs.xm[1] = t0[cc - L0::RS];
                     cs.xp[1] = t0[cc + L0::RS];
-                    cs.xm[2] = t0[cc - L0::RS * T2];
-                    cs.xp[2] = t0[cc + L0::RS * T2];
+                    cs.xm[2] = t0[cc - L0::PS];
+                    cs.xp[2] = t0[cc + L0::PS];
                     T0 u = t0[cc];
                     res = f(u, cs);
                 }
@@ -532,11 +661,12 @@ __global__ void __launch_bounds__(256) conv_kernel(sgb_view v, int src0, int src
                 }
             }
         }
-        key_cur = key_next;
-        key_next = key_far;
+#pragma unroll
+        for (int q = 0; q < NPT; ++q) m_cur[q] = m_next[q];
     }
-    async_wait_all();
+    async_wait_group<0>();
 }
+
 }  // namespace detail
 
 // The chunk slot that insertBlock hands to a CTA: ec.template get<p>()[offset] is
@@ -1622,12 +1752,18 @@ class SparseGridGpu {
         T1 b1;
         std::memcpy(&b0, &bck_raw_[s1], sizeof(T0));
         std::memcpy(&b1, &bck_raw_[s2], sizeof(T1));
-        int sms = 148;
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
-        const int64_t cap = (int64_t)sms * 8;  // eight 256-thread CTAs per SM
+        // every existing point lies in [0, size): a box that holds all of it needs no per-chunk test
+        int full_box = 1;
+        for (int i = 0; i < 3; ++i) full_box &= box.lo[i] <= 0 && (int64_t)box.hi[i] >= (int64_t)size_[i] - 1;
+        auto kern = detail::conv_kernel<blockEdgeSize, NP, MODE, T0, T1, U0, U1, F>;
+        int dev = 0, sms = 148, per_sm = 1;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, 0);
+        // one wave of resident CTAs, each walking its share of the chunks
+        const int64_t cap = (int64_t)sms * (per_sm > 0 ? per_sm : 1);
         const unsigned blocks = (unsigned)(v.n < cap ? v.n : cap);
-        detail::conv_kernel<blockEdgeSize, NP, MODE, T0, T1, U0, U1>
-            <<<blocks, 256>>>(v, (int)s1, (int)s2, (int)d1, (int)d2, box, b0, b1, f);
+        kern<<<blocks, 256>>>(v, (int)s1, (int)s2, (int)d1, (int)d2, box, full_box, b0, b1, f);
         check(cudaGetLastError() == cudaSuccess ? SGB_OK : SGB_ECUDA, "conv launch");
         if (MODE == 0) {
             // storeBlock semantics put source values into the destination's
