@@ -258,18 +258,19 @@ struct cross_stencil {
     T xp[dim];
 };
 
-// Layout of a chunk plus its one-point halo in shared memory: E + 2 planes of E + 2 rows of RS
-// elements, x = -1 .. E at elements X0 - 1 .. X0 + E, so that every row's E interior elements start
-// on a 16-byte boundary (they are copied 16 bytes at a time).  For 4-byte types the plane stride PS
-// is padded to 8 banks past a multiple of 32: a warp reading 8 x 2 x 2 points (two rows of two
-// planes) then touches 32 distinct banks, for the point itself and for each of its six neighbours.
+// Layout of a chunk plus its one-point halo in shared memory: E + 2 planes of E + 2 rows, row (j, k)
+// starting at element RS * (j + 1) + PS * (k + 1) and holding x = -1 .. E at its elements X0 - 1 ..
+// X0 + E, so that its E interior elements start on a 16-byte boundary (they are copied 16 bytes at a
+// time).  The row stride RS is the smallest multiple of X0 above E + 1: a row's x = E element may sit
+// in the next row's first X0 - 1 elements, which that row leaves unused.
 template <typename T, int E>
 struct tile_layout {
     static constexpr int X0 = sizeof(T) >= 16 ? 1 : 16 / (int)sizeof(T);
-    static constexpr int RS = ((X0 + E + 1 + X0 - 1) / X0) * X0;  // X0 - 1 .. X0 + E, rounded to X0
+    static constexpr int RS = ((E + 2 + X0 - 1) / X0) * X0;
     static constexpr int T2 = E + 2;
-    static constexpr int PS = sizeof(T) == 4 ? RS * T2 + (40 - (RS * T2) % 32) % 32 : RS * T2;
-    static constexpr int SIZE = PS * T2;
+    static constexpr int PS = RS * T2;
+    // one past the last element (x = E of row (E, E)), rounded up to X0
+    static constexpr int SIZE = ((X0 + E + RS * (T2 - 1) + PS * (T2 - 1) + 1 + X0 - 1) / X0) * X0;
     __host__ __device__ static constexpr int index(int i, int j, int k) { return X0 + i + RS * (j + 1) + PS * (k + 1); }
 };
 
@@ -485,10 +486,14 @@ struct tile_plan {
     }
 };
 
+// threads per CTA of the conv kernel: two warps share a chunk (fewer threads per chunk spend fewer
+// instructions on the per-chunk work, and more registers per thread keep more points in flight)
+constexpr int kConvThreads = 64;
+
 template <int E, int NP, int MODE, typename T0, typename T1, typename U0, typename U1, typename F>
-__global__ void __launch_bounds__(256, 6) conv_kernel(sgb_view v, int src0, int src1, int dst0, int dst1,
+__global__ void __launch_bounds__(kConvThreads, 8) conv_kernel(sgb_view v, int src0, int src1, int dst0, int dst1,
                                                       Box<3, int> box, int full_box, T0 bk0, T1 bk1, F f) {
-    constexpr int NT = 256;
+    constexpr int NT = kConvThreads;
     using L0 = tile_layout<T0, E>;
     using P0 = tile_plan<T0, E, NT>;
     using P1 = tile_plan<T1, E, NT>;
@@ -504,8 +509,8 @@ __global__ void __launch_bounds__(256, 6) conv_kernel(sgb_view v, int src0, int 
     __shared__ int32_t boxc[M][NBW];
     const T0* s0 = static_cast<const T0*>(v.data[src0]);
     const T1* s1 = static_cast<const T1*>(v.data[src1]);
-    U0* d0 = static_cast<U0*>(v.data[dst0]);
-    U1* d1 = static_cast<U1*>(v.data[dst1]);
+    U0* const d0g = static_cast<U0*>(v.data[dst0]);
+    U1* const d1g = static_cast<U1*>(v.data[dst1]);
     const int kn = v.nn_kind == SGB_NN_FULL ? 27 : 8;
     const int tid = threadIdx.x;
     const int64_t stride = gridDim.x, c0 = blockIdx.x;
@@ -568,12 +573,14 @@ __global__ void __launch_bounds__(256, 6) conv_kernel(sgb_view v, int src0, int 
         k = E == 8 ? (w >> 7) * 2 + ((w >> 4) & 1) : w / (E * E);
         return i + E * (j + E * k);
     };
+    int pi[NPT], pj[NPT], pk[NPT], pp[NPT];  // this thread's points, worked out once
+#pragma unroll
+    for (int q = 0; q < NPT; ++q) pp[q] = point(q, pi[q], pj[q], pk[q]);
     uint8_t m_cur[NPT], m_next[NPT];
     auto masks_of = [&](int64_t s, uint8_t* m) {
 #pragma unroll
         for (int q = 0; q < NPT; ++q) {
-            int i, j, k;
-            const int pnt = point(q, i, j, k);
+            const int pnt = pp[q];
             m[q] = (s < nmine && (BS % NT == 0 || tid + q * NT < BS)) ? v.mask[pos(s) * BS + pnt] : (uint8_t)0;
         }
     };
@@ -607,12 +614,13 @@ __global__ void __launch_bounds__(256, 6) conv_kernel(sgb_view v, int src0, int 
             }
         }
         const T0* t0 = tile0[b];
-        const int64_t c = pos(it), base = c * BS;
+        const int64_t c = pos(it);
+        U0* const d0 = d0g + c * BS;  // this chunk's destination points
+        U1* const d1 = d1g + c * BS;
 #pragma unroll
         for (int q = 0; q < NPT; ++q) {
             if (BS % NT != 0 && tid + q * NT >= BS) break;
-            int i, j, k;
-            const int pnt = point(q, i, j, k);
+            const int i = pi[q], j = pj[q], k = pk[q], pnt = pp[q];
             bool in;
             if constexpr (BITS) {
                 const uint32_t pm = (1u << i) | (1u << (E + j)) | (1u << (2 * E + k));
@@ -621,7 +629,7 @@ __global__ void __launch_bounds__(256, 6) conv_kernel(sgb_view v, int src0, int 
                 in = i >= lo[0] && i <= hi[0] && j >= lo[1] && j <= hi[1] && k >= lo[2] && k <= hi[2];
             }
             const bool act = (m_cur[q] & 3) == 1 && in;
-            const int64_t g = base + pnt;
+            const int g = pnt;
             if constexpr (MODE == 0) {  // conv_cross: storeBlock of the whole chunk
                 const int cc = L0::index(i, j, k);
                 T0 res = t0[cc];
@@ -1759,11 +1767,11 @@ class SparseGridGpu {
         int dev = 0, sms = 148, per_sm = 1;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, detail::kConvThreads, 0);
         // one wave of resident CTAs, each walking its share of the chunks
         const int64_t cap = (int64_t)sms * (per_sm > 0 ? per_sm : 1);
         const unsigned blocks = (unsigned)(v.n < cap ? v.n : cap);
-        kern<<<blocks, 256>>>(v, (int)s1, (int)s2, (int)d1, (int)d2, box, full_box, b0, b1, f);
+        kern<<<blocks, detail::kConvThreads>>>(v, (int)s1, (int)s2, (int)d1, (int)d2, box, full_box, b0, b1, f);
         check(cudaGetLastError() == cudaSuccess ? SGB_OK : SGB_ECUDA, "conv launch");
         if (MODE == 0) {
             // storeBlock semantics put source values into the destination's
