@@ -565,12 +565,14 @@ __global__ void __launch_bounds__(kConvThreads, 8) conv_kernel(sgb_view v, int s
         }
     };
     // point q of this thread, q = 0 .. NPT - 1 (offset in the chunk; i, j, k its coordinates).  In 8^3
-    // chunks a warp takes x = 0 .. 7 of rows (j, j + 1) in planes (k, k + 1).
+    // chunks a warp takes x = 0 .. 7 of one row j in four planes k: with the tile's 12-element rows and
+    // 120-element planes (24 banks apart) the warp's reads of the points and of each of their six
+    // neighbours fall on 32 distinct banks.
     auto point = [&](int q, int& i, int& j, int& k) {
         const int w = tid + q * NT;
         i = w % E;
-        j = E == 8 ? ((w >> 5) & 3) * 2 + ((w >> 3) & 1) : (w / E) % E;
-        k = E == 8 ? (w >> 7) * 2 + ((w >> 4) & 1) : w / (E * E);
+        j = E == 8 ? (w >> 5) & 7 : (w / E) % E;
+        k = E == 8 ? ((w >> 3) & 3) + 4 * (w >> 8) : w / (E * E);
         return i + E * (j + E * k);
     };
     int pi[NPT], pj[NPT], pk[NPT], pp[NPT];  // this thread's points, worked out once
