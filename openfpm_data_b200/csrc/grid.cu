@@ -4,6 +4,8 @@
 #include <cstring>
 #include <string>
 
+#include <cuda.h>
+
 #include "common.cuh"
 #include "internal.h"
 
@@ -22,31 +24,180 @@ int cuda_status(cudaError_t e, const char* what) {
     return SGB_ECUDA;
 }
 
-int DevBuf::reserve(size_t need) {
-    if (need <= bytes) return SGB_OK;
+// Driver calls for growth in place (virtual memory management), looked up through the runtime so that
+// the library does not link the driver library itself.
+namespace {
+struct VmmApi {
+    CUresult (*reserve)(CUdeviceptr*, size_t, size_t, CUdeviceptr, unsigned long long) = nullptr;
+    CUresult (*free_va)(CUdeviceptr, size_t) = nullptr;
+    CUresult (*create)(CUmemGenericAllocationHandle*, size_t, const CUmemAllocationProp*, unsigned long long) =
+        nullptr;
+    CUresult (*release)(CUmemGenericAllocationHandle) = nullptr;
+    CUresult (*map)(CUdeviceptr, size_t, size_t, CUmemGenericAllocationHandle, unsigned long long) = nullptr;
+    CUresult (*unmap)(CUdeviceptr, size_t) = nullptr;
+    CUresult (*access)(CUdeviceptr, size_t, const CUmemAccessDesc*, size_t) = nullptr;
+    CUresult (*granularity)(size_t*, const CUmemAllocationProp*, CUmemAllocationGranularity_flags) = nullptr;
+    bool ok = false;
+};
+const VmmApi& vmm() {
+    static VmmApi api = [] {
+        VmmApi a;
+        auto get = [](const char* name, void** fn) {
+            cudaDriverEntryPointQueryResult q;
+            return cudaGetDriverEntryPointByVersion(name, fn, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+                   q == cudaDriverEntryPointSuccess && *fn != nullptr;
+        };
+        a.ok = get("cuMemAddressReserve", (void**)&a.reserve) && get("cuMemAddressFree", (void**)&a.free_va) &&
+               get("cuMemCreate", (void**)&a.create) && get("cuMemRelease", (void**)&a.release) &&
+               get("cuMemMap", (void**)&a.map) && get("cuMemUnmap", (void**)&a.unmap) &&
+               get("cuMemSetAccess", (void**)&a.access) &&
+               get("cuMemGetAllocationGranularity", (void**)&a.granularity);
+        return a;
+    }();
+    return api;
+}
+CUmemAllocationProp device_prop(int dev) {
+    CUmemAllocationProp prop = {};
+    prop.type = CU_MEM_ALLOCATION_TYPE_PINNED;
+    prop.location.type = CU_MEM_LOCATION_TYPE_DEVICE;
+    prop.location.id = dev;
+    return prop;
+}
+// map `size` bytes of new physical memory of device `dev` at `at`; the handle goes to `maps`
+int map_more(const VmmApi& api, int dev, unsigned long long at, size_t size,
+             std::vector<std::pair<unsigned long long, size_t>>& maps) {
+    const CUmemAllocationProp prop = device_prop(dev);
+    CUmemGenericAllocationHandle h = 0;
+    if (api.create(&h, size, &prop, 0) != CUDA_SUCCESS) {
+        set_error("cuMemCreate: out of device memory");
+        return SGB_ENOMEM;
+    }
+    if (api.map((CUdeviceptr)at, size, 0, h, 0) != CUDA_SUCCESS) {
+        api.release(h);
+        set_error("cuMemMap failed");
+        return SGB_ECUDA;
+    }
+    CUmemAccessDesc acc = {};
+    acc.location = prop.location;
+    acc.flags = CU_MEM_ACCESS_FLAGS_PROT_READWRITE;
+    if (api.access((CUdeviceptr)at, size, &acc, 1) != CUDA_SUCCESS) {
+        api.unmap((CUdeviceptr)at, size);
+        api.release(h);
+        set_error("cuMemSetAccess failed");
+        return SGB_ECUDA;
+    }
+    maps.emplace_back((unsigned long long)h, size);
+    return SGB_OK;
+}
+// unmap and release every mapping of a reserved range, then the range
+void unmap_all(const VmmApi& api, unsigned long long va, size_t va_bytes,
+               std::vector<std::pair<unsigned long long, size_t>>& maps) {
+    size_t off = 0;
+    for (auto& m : maps) {
+        api.unmap((CUdeviceptr)(va + off), m.second);
+        api.release((CUmemGenericAllocationHandle)m.first);
+        off += m.second;
+    }
+    maps.clear();
+    if (va) api.free_va((CUdeviceptr)va, va_bytes);
+}
+}  // namespace
+
+// a buffer from cudaMalloc grown by allocating a larger one and copying the contents over
+static int realloc_copy(DevBuf& b, size_t need) {
     size_t nb = need + need / 2 + 256;
     void* q = nullptr;
     cudaError_t e = cudaMalloc(&q, nb);
     if (e != cudaSuccess) return cuda_status(e, "cudaMalloc");
-    if (p && bytes) {
+    if (b.p && b.bytes) {
         // work queued on any stream may still write the old buffer
         e = cudaDeviceSynchronize();
-        if (e == cudaSuccess) e = cudaMemcpy(q, p, bytes, cudaMemcpyDeviceToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(q, b.p, b.bytes, cudaMemcpyDeviceToDevice);
         if (e != cudaSuccess) {
             cudaFree(q);
             return cuda_status(e, "cudaMemcpy(grow)");
         }
     }
-    if (p) cudaFree(p);
-    p = q;
-    bytes = nb;
+    if (b.p) cudaFree(b.p);
+    b.p = q;
+    b.bytes = nb;
     return SGB_OK;
+}
+
+int DevBuf::grow_in_place(size_t need) {
+    if (need <= bytes) return SGB_OK;
+    if (!va && need < kInPlaceMinBytes) return realloc_copy(*this, need);
+    const VmmApi& api = vmm();
+    if (!api.ok) {
+        if (va) return SGB_ECUDA;      // cannot happen: the range was made through the same calls
+        return realloc_copy(*this, need);  // no driver support: reallocate and copy
+    }
+    int dev = 0;
+    SGB_CUDA(cudaGetDevice(&dev));
+    const CUmemAllocationProp prop = device_prop(dev);
+    size_t gran = 0;
+    if (api.granularity(&gran, &prop, CU_MEM_ALLOC_GRANULARITY_RECOMMENDED) != CUDA_SUCCESS || gran == 0) {
+        if (va) {
+            set_error("cuMemGetAllocationGranularity failed");
+            return SGB_ECUDA;
+        }
+        return realloc_copy(*this, need);
+    }
+    auto round_up = [gran](size_t x) { return (x + gran - 1) / gran * gran; };
+    const size_t target = round_up(std::max(need, bytes + bytes / 2));
+    if (va && target <= va_bytes) {  // map the difference behind the current end
+        SGB_TRY(map_more(api, dev, va + bytes, target - bytes, maps));
+        bytes = target;
+        return SGB_OK;
+    }
+    // a new range with room for eight times the target (at least 4 GiB, at most the device's memory),
+    // the contents copied over once
+    size_t total = 0, free_b = 0;
+    SGB_CUDA(cudaMemGetInfo(&free_b, &total));
+    size_t want = std::max(target * 8, size_t(4) << 30);
+    want = std::max(target, std::min(want, round_up(total)));
+    want = round_up(want);
+    CUdeviceptr nva = 0;
+    if (api.reserve(&nva, want, 0, 0, 0) != CUDA_SUCCESS) {
+        set_error("cuMemAddressReserve failed");
+        return SGB_ENOMEM;
+    }
+    std::vector<std::pair<unsigned long long, size_t>> nmaps;
+    int st = map_more(api, dev, (unsigned long long)nva, target, nmaps);
+    if (st == SGB_OK && p && bytes) {
+        // work queued on any stream may still write the old buffer
+        cudaError_t e = cudaDeviceSynchronize();
+        if (e == cudaSuccess) e = cudaMemcpy((void*)nva, p, bytes, cudaMemcpyDeviceToDevice);
+        if (e != cudaSuccess) st = cuda_status(e, "cudaMemcpy(grow)");
+    }
+    if (st != SGB_OK) {
+        unmap_all(api, (unsigned long long)nva, want, nmaps);
+        return st;
+    }
+    release();
+    va = (unsigned long long)nva;
+    va_bytes = want;
+    maps = std::move(nmaps);
+    p = (void*)nva;
+    bytes = target;
+    return SGB_OK;
+}
+
+int DevBuf::reserve(size_t need) {
+    if (need <= bytes) return SGB_OK;
+    if (va || need >= kInPlaceMinBytes) return grow_in_place(need);
+    return realloc_copy(*this, need);
 }
 
 int DevBuf::grow(size_t need) { return need <= bytes ? SGB_OK : ensure(2 * need); }
 
 int DevBuf::ensure(size_t need) {
     if (need <= bytes) return SGB_OK;
+    if (va) return grow_in_place(need);
+    if (need >= kInPlaceMinBytes) {
+        release();  // nothing to keep: the new range starts empty
+        return grow_in_place(need);
+    }
     if (p) cudaFree(p);
     p = nullptr;
     bytes = 0;
@@ -61,7 +212,15 @@ int DevBuf::ensure(size_t need) {
 }
 
 void DevBuf::release() {
-    if (p) cudaFree(p);
+    if (va) {
+        // in-place buffers may still be read by queued work, as cudaFree would wait for
+        cudaDeviceSynchronize();
+        unmap_all(vmm(), va, va_bytes, maps);
+        va = 0;
+        va_bytes = 0;
+    } else if (p) {
+        cudaFree(p);
+    }
     p = nullptr;
     bytes = 0;
 }

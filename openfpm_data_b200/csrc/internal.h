@@ -59,13 +59,23 @@ struct DeviceGuard {
 struct DevBuf {
     void* p = nullptr;
     size_t bytes = 0;
+    // Growth in place: an address range reserved once (va, va_bytes) with physical memory mapped behind
+    // p as the buffer grows, so that contents and address stay; `maps` holds the physical allocations
+    // (driver handles and sizes) in address order.  Empty for buffers from cudaMalloc.
+    unsigned long long va = 0;
+    size_t va_bytes = 0;
+    std::vector<std::pair<unsigned long long, size_t>> maps;
     int reserve(size_t need);   // keeps contents
     int ensure(size_t need);    // may drop contents
     int grow(size_t need);      // may drop contents; grows to twice the need (for tables that follow a growing map)
+    // keeps contents; buffers past kInPlaceMinBytes grow in place (no free, no copy, same address) on the
+    // current device, smaller ones as reserve()
+    int grow_in_place(size_t need);
     void release();
     template <typename T>
     T* as() const { return static_cast<T*>(p); }
 };
+constexpr size_t kInPlaceMinBytes = size_t(256) << 20;
 
 // Pinned host staging for small device->host reads.
 struct HostScratch {
