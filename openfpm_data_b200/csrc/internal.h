@@ -65,6 +65,19 @@ struct DevBuf {
     unsigned long long va = 0;
     size_t va_bytes = 0;
     std::vector<std::pair<unsigned long long, size_t>> maps;
+    // one owner per allocation: moves (std::swap of buffer sets) leave the source empty, copies are refused
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    DevBuf(DevBuf&& o) noexcept { take(o); }
+    DevBuf& operator=(DevBuf&& o) noexcept {
+        if (this != &o) {
+            release();
+            take(o);
+        }
+        return *this;
+    }
+    ~DevBuf() = default;  // owners release explicitly (the grid and batch destructors)
     int reserve(size_t need);   // keeps contents
     int ensure(size_t need);    // may drop contents
     int grow(size_t need);      // may drop contents; grows to twice the need (for tables that follow a growing map)
@@ -74,6 +87,20 @@ struct DevBuf {
     void release();
     template <typename T>
     T* as() const { return static_cast<T*>(p); }
+
+   private:
+    void take(DevBuf& o) {
+        p = o.p;
+        bytes = o.bytes;
+        va = o.va;
+        va_bytes = o.va_bytes;
+        maps = std::move(o.maps);
+        o.p = nullptr;
+        o.bytes = 0;
+        o.va = 0;
+        o.va_bytes = 0;
+        o.maps.clear();
+    }
 };
 constexpr size_t kInPlaceMinBytes = size_t(256) << 20;
 
