@@ -129,28 +129,79 @@ def _cuda_ok():
 
 # ---------------------------------------------------------------- clocks
 class ClockSampler:
-    """nvidia-smi samples of SM clock and throttle reasons during a region."""
+    """SM clock and clock-event reasons of one GPU, sampled during a region: by NVML from a
+    background thread every 5 ms (read-only queries), or by `nvidia-smi -lms` where NVML cannot be
+    loaded.  stop() returns the median SM clock under load, the maximum, the reasons seen and the
+    number of samples."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    # NVML clock-event reason bits
+    REASON_BITS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40}
 
     def __init__(self, device_index: int, interval_ms: int = 20):
-        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
         self.proc = None
+        self.thread = None
+        self.samples = []  # (sm MHz, max MHz, reason bits)
+        self.uuid = None
         try:
             import torch
-            uuid = str(torch.cuda.get_device_properties(device_index).uuid)
-            sel = ["-i", uuid if uuid.startswith("GPU-") else "GPU-" + uuid]
+            u = str(torch.cuda.get_device_properties(device_index).uuid)
+            self.uuid = u if u.startswith("GPU-") else "GPU-" + u
         except Exception:
-            sel = ["-i", str(device_index)]
+            pass
+        if self._start_nvml():
+            return
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        sel = ["-i", self.uuid] if self.uuid else ["-i", str(device_index)]
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "--query-gpu=" + self.Q, "--format=csv,noheader,nounits",
                                           "-lms", str(interval_ms)] + sel, stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
 
+    def _start_nvml(self) -> bool:
+        try:
+            import threading
+
+            import pynvml as nv
+            nv.nvmlInit()
+            h = nv.nvmlDeviceGetHandleByUUID(self.uuid) if self.uuid else None
+            if h is None:
+                return False
+            reasons = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+                nv.nvmlDeviceGetCurrentClocksThrottleReasons
+            mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+            self._stop_flag = False
+
+            def run():
+                while not self._stop_flag:
+                    try:
+                        self.samples.append((nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM), mx, int(reasons(h))))
+                    except Exception:
+                        pass
+                    time.sleep(0.005)
+
+            self.samples.append((nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM), mx, int(reasons(h))))
+            self.thread = threading.Thread(target=run, daemon=True)
+            self.thread.start()
+            return True
+        except Exception:
+            return False
+
     def stop(self):
+        if self.thread is not None:
+            self._stop_flag = True
+            self.thread.join(timeout=5)
+            sm = [a for a, _, _ in self.samples]
+            mx = self.samples[-1][1] if self.samples else None
+            bits = 0
+            for _, _, r in self.samples:
+                bits |= r
+            reasons = sorted(n for n, b in self.REASON_BITS.items() if bits & b)
+            return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": reasons,
+                    "samples": len(sm), "source": "nvml"}
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
         self.proc.terminate()
@@ -174,7 +225,7 @@ class ClockSampler:
             except (ValueError, IndexError):
                 continue
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "source": "nvidia-smi"}
 
 
 # ---------------------------------------------------------------- helpers
@@ -727,8 +778,10 @@ def run_conv2b(args, dist: Dist):
         vis = os.environ.get("CUDA_VISIBLE_DEVICES")
         devs = vis.split(",") if vis else [str(i) for i in range(dist.local + 1)]
         env = dict(os.environ, CUDA_VISIBLE_DEVICES=devs[dist.local] if dist.local < len(devs) else str(dist.local))
+        clocks = ClockSampler(dist.local)
         r = subprocess.run([exe, path, str(max(1, args.steps)), str(max(3, args.warmup))], capture_output=True,
                            text=True, timeout=900, env=env)
+        clk = clocks.stop()
     if r.returncode != 0:
         raise RuntimeError(f"bench_conv failed ({r.returncode}): {r.stderr[-500:]}")
     res = json.loads([ln for ln in r.stdout.splitlines() if ln.startswith("{")][-1])
@@ -739,7 +792,7 @@ def run_conv2b(args, dist: Dist):
                                   "fixed_function_gs7_gpts": res["gs7_gpts"],
                                   "conv2_b_over_gs7": res["conv2_b_over_gs7"],
                                   "one_step_bit_equal_to_gs7": res["one_step_bit_equal"]},
-                 roofline=None, cpu_baseline=None, e2e=None, gpu_launches=steps, clocks=None)
+                 roofline=None, cpu_baseline=None, e2e=None, gpu_launches=steps, clocks=clk)
 
 
 def _ghost_boxes(size=512, width=1):

@@ -122,7 +122,13 @@ static int batch_compact(sgb_batch* b, cudaStream_t s) {
     std::swap(b->gid, b->gid2);
     for (int k = 0; k < 2; ++k)
         for (int p = 0; p < b->np; ++p) std::swap(b->field[k][p], b->field2[k][p]);
-    b->cap = std::min<int64_t>((int64_t)(b->keys.bytes / 8), (int64_t)(b->mask.bytes / bs));
+    // the capacity every array holds (their allocations round differently)
+    int64_t cap = std::min<int64_t>((int64_t)(b->keys.bytes / 8), (int64_t)(b->mask.bytes / bs));
+    cap = std::min<int64_t>(cap, (int64_t)(b->nn.bytes / 32));
+    cap = std::min<int64_t>(cap, (int64_t)(b->gid.bytes / 4));
+    for (int k = 0; k < 2; ++k)
+        for (int p = 0; p < b->np; ++p) cap = std::min<int64_t>(cap, (int64_t)(b->field[k][p].bytes / ((size_t)bs * 4)));
+    b->cap = cap;
     b->n = off;
     b->holes = false;
     return SGB_OK;
