@@ -417,6 +417,7 @@ struct tile_plan {
     static constexpr int NVEC = ROWS * VPR;
     static constexpr int NITEM = NVEC + ROWS * (VEC ? 2 : E + 2);
     static constexpr int ITEMS = (NITEM + NT - 1) / NT;
+    static_assert(BS <= 65536, "a chunk's element offsets are kept in 16 bits");
     int toff[ITEMS];  // element offset in the tile; -1: no item
     int soff[ITEMS];  // element offset in the source chunk | slot << 16
 
