@@ -453,11 +453,10 @@ struct tile_plan {
             soff[q] = (lx + E * (ly + E * lz)) | slot_of(kn, dx, dy, dz) << 16;
         }
     }
-    // issue this thread's copies of chunk table `nnrow` (slot SELF: the chunk) into `tile`; with
-    // NF == 2 the same items of a second field of the same type as well
+    // issue this thread's copies of chunk table `nnrow` (slot SELF: the chunk) into tiles[0 .. NF - 1]
+    // from fields srcs[0 .. NF - 1] of this type (background bks[f] where the source chunk is absent)
     template <int NF>
-    __device__ void issue(int tid, const int32_t* nnrow, T* tile, const T* src, T bk, T* tile2, const T* src2,
-                          T bk2) const {
+    __device__ void issue(int tid, const int32_t* nnrow, T* const* tiles, const T* const* srcs, const T* bks) const {
 #pragma unroll
         for (int q = 0; q < ITEMS; ++q) {
             if (toff[q] < 0) continue;
@@ -465,22 +464,21 @@ struct tile_plan {
             const int64_t so = (int64_t)sc * BS + (soff[q] & 0xffff);
             if (VEC && tid + q * NT < NVEC) {
                 if (sc >= 0) {
-                    async_copy16(tile + toff[q], src + so);
-                    if (NF == 2) async_copy16(tile2 + toff[q], src2 + so);
+#pragma unroll
+                    for (int f = 0; f < NF; ++f) async_copy16(tiles[f] + toff[q], srcs[f] + so);
                 } else {
 #pragma unroll
-                    for (int e = 0; e < PER; ++e) {
-                        tile[toff[q] + e] = bk;
-                        if (NF == 2) tile2[toff[q] + e] = bk2;
-                    }
+                    for (int e = 0; e < PER; ++e)
+#pragma unroll
+                        for (int f = 0; f < NF; ++f) tiles[f][toff[q] + e] = bks[f];
                 }
             } else {
                 if (sc >= 0) {
-                    async_copy_elem(tile + toff[q], src + so);
-                    if (NF == 2) async_copy_elem(tile2 + toff[q], src2 + so);
+#pragma unroll
+                    for (int f = 0; f < NF; ++f) async_copy_elem(tiles[f] + toff[q], srcs[f] + so);
                 } else {
-                    tile[toff[q]] = bk;
-                    if (NF == 2) tile2[toff[q]] = bk2;
+#pragma unroll
+                    for (int f = 0; f < NF; ++f) tiles[f][toff[q]] = bks[f];
                 }
             }
         }
@@ -491,27 +489,34 @@ struct tile_plan {
 // instructions on the per-chunk work, and more registers per thread keep more points in flight)
 constexpr int kConvThreads = 64;
 
-template <int E, int NP, int MODE, typename T0, typename T1, typename U0, typename U1, typename F>
-__global__ void __launch_bounds__(kConvThreads, 8) conv_kernel(sgb_view v, int src0, int src1, int dst0, int dst1,
-                                                      Box<3, int> box, int full_box, T0 bk0, T1 bk1, F f) {
+template <int E, int NP, int MODE, typename T0, typename T1, typename T2, typename U0, typename U1, typename U2,
+          typename F>
+__global__ void __launch_bounds__(kConvThreads, 8)
+    conv_kernel(sgb_view v, int src0, int src1, int src2, int dst0, int dst1, int dst2, Box<3, int> box, int full_box,
+                T0 bk0, T1 bk1, T2 bk2, F f) {
     constexpr int NT = kConvThreads;
     using L0 = tile_layout<T0, E>;
     using P0 = tile_plan<T0, E, NT>;
     using P1 = tile_plan<T1, E, NT>;
-    constexpr bool SAME = std::is_same<T0, T1>::value;
+    using P2 = tile_plan<T2, E, NT>;
+    // source fields of one type share their copy items
+    constexpr bool SAME = (NP < 2 || std::is_same<T0, T1>::value) && (NP < 3 || std::is_same<T0, T2>::value);
     constexpr int BS = E * E * E, NPT = (BS + NT - 1) / NT;
     constexpr int NB = 2;  // halo tiles per field: chunks s + 1 .. s + NB - 1 are in flight while s computes
     constexpr int M = NB + 1;    // slots of per-chunk metadata (neighbour row, box)
     constexpr bool BITS = E <= 10;  // box as one bit per in-box x, y and z, or lo / hi per dimension
     constexpr int NBW = BITS ? 1 : 6;
     __shared__ __align__(16) T0 tile0[NB][L0::SIZE];
-    __shared__ __align__(16) T1 tile1[NB][NP == 2 ? tile_layout<T1, E>::SIZE : 16];
+    __shared__ __align__(16) T1 tile1[NB][NP >= 2 ? tile_layout<T1, E>::SIZE : 16];
+    __shared__ __align__(16) T2 tile2[NB][NP >= 3 ? tile_layout<T2, E>::SIZE : 16];
     __shared__ int32_t nnrow[M][28];
     __shared__ int32_t boxc[M][NBW];
     const T0* s0 = static_cast<const T0*>(v.data[src0]);
     const T1* s1 = static_cast<const T1*>(v.data[src1]);
+    const T2* s2 = static_cast<const T2*>(v.data[src2]);
     U0* const d0g = static_cast<U0*>(v.data[dst0]);
     U1* const d1g = static_cast<U1*>(v.data[dst1]);
+    U2* const d2g = static_cast<U2*>(v.data[dst2]);
     const int kn = v.nn_kind == SGB_NN_FULL ? 27 : 8;
     const int tid = threadIdx.x;
     const int64_t stride = gridDim.x, c0 = blockIdx.x;
@@ -521,17 +526,32 @@ __global__ void __launch_bounds__(kConvThreads, 8) conv_kernel(sgb_view v, int s
     auto pos = [&](int64_t s) { return c0 + s * stride; };
     P0 plan0;
     P1 plan1;
+    P2 plan2;
     plan0.init(tid, kn);
-    if (NP == 2 && !SAME) plan1.init(tid, kn);
+    if (NP >= 2 && !SAME) plan1.init(tid, kn);
+    if (NP >= 3 && !SAME) plan2.init(tid, kn);
     auto gather = [&](int64_t s) {  // chunk number s into tile s % NB (its metadata in slot s % M)
         if (s < nmine) {
             const int b = (int)(s % NB), m = (int)(s % M);
-            if constexpr (NP == 2 && SAME) {
-                plan0.template issue<2>(tid, nnrow[m], tile0[b], s0, bk0, reinterpret_cast<T0*>(tile1[b]),
-                                        reinterpret_cast<const T0*>(s1), (T0)bk1);
+            if constexpr (SAME) {
+                T0* const tiles[3] = {tile0[b], reinterpret_cast<T0*>(tile1[b]), reinterpret_cast<T0*>(tile2[b])};
+                const T0* const srcs[3] = {s0, reinterpret_cast<const T0*>(s1), reinterpret_cast<const T0*>(s2)};
+                const T0 bks[3] = {bk0, (T0)bk1, (T0)bk2};
+                plan0.template issue<NP>(tid, nnrow[m], tiles, srcs, bks);
             } else {
-                plan0.template issue<1>(tid, nnrow[m], tile0[b], s0, bk0, nullptr, nullptr, bk0);
-                if constexpr (NP == 2) plan1.template issue<1>(tid, nnrow[m], tile1[b], s1, bk1, nullptr, nullptr, bk1);
+                T0* const t0s[1] = {tile0[b]};
+                const T0* const s0s[1] = {s0};
+                plan0.template issue<1>(tid, nnrow[m], t0s, s0s, &bk0);
+                if constexpr (NP >= 2) {
+                    T1* const t1s[1] = {tile1[b]};
+                    const T1* const s1s[1] = {s1};
+                    plan1.template issue<1>(tid, nnrow[m], t1s, s1s, &bk1);
+                }
+                if constexpr (NP >= 3) {
+                    T2* const t2s[1] = {tile2[b]};
+                    const T2* const s2s[1] = {s2};
+                    plan2.template issue<1>(tid, nnrow[m], t2s, s2s, &bk2);
+                }
             }
         }
         async_commit();  // one group per chunk number, empty past the end
@@ -620,6 +640,7 @@ __global__ void __launch_bounds__(kConvThreads, 8) conv_kernel(sgb_view v, int s
         const int64_t c = pos(it);
         U0* const d0 = d0g + c * BS;  // this chunk's destination points
         U1* const d1 = d1g + c * BS;
+        U2* const d2 = d2g + c * BS;
 #pragma unroll
         for (int q = 0; q < NPT; ++q) {
             if (BS % NT != 0 && tid + q * NT >= BS) break;
@@ -650,7 +671,7 @@ __global__ void __launch_bounds__(kConvThreads, 8) conv_kernel(sgb_view v, int s
                 d0[g] = (U0)res;
             } else if (act) {
                 cp_block<T0, E> u{const_cast<T0*>(t0)};
-                cp_block<T1, E> w{const_cast<T1*>(tile1[NP == 2 ? b : 0])};
+                cp_block<T1, E> w{const_cast<T1*>(tile1[NP >= 2 ? b : 0])};
                 if constexpr (MODE == 1) {  // conv
                     d0[g] = (U0)f(u, i, j, k);
                 } else if constexpr (MODE == 2) {  // conv2
@@ -666,9 +687,19 @@ __global__ void __launch_bounds__(kConvThreads, 8) conv_kernel(sgb_view v, int s
                     f(r1, r2, u, w, blk, pnt, i, j, k);
                     d0[g] = r1;
                     d1[g] = r2;
-                } else {  // conv_cross_b: the chunk's data block and the point's offset as well
+                } else if constexpr (MODE == 4) {  // conv_cross_b: the chunk's data block and the point's offset
                     data_block<8> blk{v.data, c, BS};
                     d0[g] = (U0)f(u, blk, pnt, i, j, k);
+                } else {  // conv3_b: three fields
+                    cp_block<T2, E> x3{const_cast<T2*>(tile2[NP >= 3 ? b : 0])};
+                    U0 r1 = 0;
+                    U1 r2 = 0;
+                    U2 r3 = 0;
+                    data_block<8> blk{v.data, c, BS};
+                    f(r1, r2, r3, u, w, x3, blk, pnt, i, j, k);
+                    d0[g] = r1;
+                    d1[g] = r2;
+                    d2[g] = r3;
                 }
             }
         }
@@ -1309,6 +1340,13 @@ class SparseGridGpu {
     void conv2_b(grid_key_dx<3> start, grid_key_dx<3> stop, F f) {
         launch_conv<2, 3, s1, s2, d1, d2>(start, stop, f);
     }
+    // conv3_b (SparseGridGpu.hpp:2646-2663): f(r1, r2, r3, u, v, w, data_block, offset, i, j, k) over three
+    // source fields, the results written at active points
+    template <unsigned s1, unsigned s2, unsigned s3, unsigned d1, unsigned d2, unsigned d3, unsigned stencil_size,
+              typename F>
+    void conv3_b(grid_key_dx<3> start, grid_key_dx<3> stop, F f) {
+        launch_conv<3, 5, s1, s2, d1, d2, s3, d3>(start, stop, f);
+    }
 
     // deviceToHost<p...>(): the block map and listed properties to host copies
     template <unsigned... prp>
@@ -1748,12 +1786,15 @@ class SparseGridGpu {
         }
     }
 
-    template <int NP, int MODE, unsigned s1, unsigned s2, unsigned d1, unsigned d2, typename F>
+    template <int NP, int MODE, unsigned s1, unsigned s2, unsigned d1, unsigned d2, unsigned s3 = s1, unsigned d3 = d1,
+              typename F>
     void launch_conv(grid_key_dx<3> start, grid_key_dx<3> stop, F f) {
         using T0 = typename std::tuple_element<s1, props>::type;
         using T1 = typename std::tuple_element<s2, props>::type;
+        using T2 = typename std::tuple_element<s3, props>::type;
         using U0 = typename std::tuple_element<d1, props>::type;
         using U1 = typename std::tuple_element<d2, props>::type;
+        using U2 = typename std::tuple_element<d3, props>::type;
         sgb_view v;
         check(sgb_get_view(g_, nn_kind_, &v, nullptr), "conv");
         if (v.n == 0) return;
@@ -1761,12 +1802,14 @@ class SparseGridGpu {
         for (int i = 0; i < 3; ++i) box.lo[i] = (int)start.get(i), box.hi[i] = (int)stop.get(i);
         T0 b0;
         T1 b1;
+        T2 b2;
         std::memcpy(&b0, &bck_raw_[s1], sizeof(T0));
         std::memcpy(&b1, &bck_raw_[s2], sizeof(T1));
+        std::memcpy(&b2, &bck_raw_[s3], sizeof(T2));
         // every existing point lies in [0, size): a box that holds all of it needs no per-chunk test
         int full_box = 1;
         for (int i = 0; i < 3; ++i) full_box &= box.lo[i] <= 0 && (int64_t)box.hi[i] >= (int64_t)size_[i] - 1;
-        auto kern = detail::conv_kernel<blockEdgeSize, NP, MODE, T0, T1, U0, U1, F>;
+        auto kern = detail::conv_kernel<blockEdgeSize, NP, MODE, T0, T1, T2, U0, U1, U2, F>;
         int dev = 0, sms = 148, per_sm = 1;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -1774,7 +1817,8 @@ class SparseGridGpu {
         // one wave of resident CTAs, each walking its share of the chunks
         const int64_t cap = (int64_t)sms * (per_sm > 0 ? per_sm : 1);
         const unsigned blocks = (unsigned)(v.n < cap ? v.n : cap);
-        kern<<<blocks, detail::kConvThreads>>>(v, (int)s1, (int)s2, (int)d1, (int)d2, box, full_box, b0, b1, f);
+        kern<<<blocks, detail::kConvThreads>>>(v, (int)s1, (int)s2, (int)s3, (int)d1, (int)d2, (int)d3, box, full_box,
+                                               b0, b1, b2, f);
         check(cudaGetLastError() == cudaSuccess ? SGB_OK : SGB_ECUDA, "conv launch");
         if (MODE == 0) {
             // storeBlock semantics put source values into the destination's

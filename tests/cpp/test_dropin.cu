@@ -500,6 +500,26 @@ int main() {
     HostMap G2 = download(grid.handle(), 6);
     CHECK(same(G2, 2, G2, 4, active) && same(G2, 3, G2, 5, active), "gs7_vs_conv2_b");
 
+    // conv3_b (SparseGridGpu.hpp:2646-2663): the Gray-Scott pair on u, v plus a third field read with
+    // its halo; the pair must equal GS7, the third result a conv of the same expression
+    auto halo3 = [] __device__(cp_block<float, 8>& w, int i, int j, int k) {
+        return __fadd_rn(__fadd_rn(w(i - 1, j, k), w(i, j + 1, k)), __fadd_rn(w(i, j, k - 1), w(i, j, k)));
+    };
+    grid.conv3_b<0, 1, 2, 4, 5, 3, 1>(lo, hi,
+                                     [=] __device__(float& uo, float& vo, float& wo, cp_block<float, 8>& u,
+                                                    cp_block<float, 8>& v, cp_block<float, 8>& w, data_block<8>&,
+                                                    int, int i, int j, int k) {
+                                         gs(uo, vo, u, v, i, j, k);
+                                         wo = halo3(w, i, j, k);
+                                     });
+    cudaDeviceSynchronize();
+    HostMap G3 = download(grid.handle(), 6);
+    grid.conv<2, 3, 1>(lo, hi, [=] __device__(cp_block<float, 8>& w, int i, int j, int k) { return halo3(w, i, j, k); });
+    cudaDeviceSynchronize();
+    HostMap G4 = download(grid.handle(), 6);
+    CHECK(same(G3, 4, G2, 2, active) && same(G3, 5, G2, 3, active) && same(G3, 3, G4, 3, active),
+          "conv3_b_vs_gs7_and_conv");
+
     // ---------------------------------------------------------------- Conv3x3x3 vs conv over NNFull
     conv_coeff cc;
     for (int a = 0; a < 3; ++a)
@@ -818,6 +838,111 @@ int main() {
                     all3 = all3 && cg.get<0>(k) == 3.0f && cg.get<2>(k) == 3.0f;
                 }
         CHECK(all3, "insertBlock_constant_two_properties");
+    }
+
+    // ---------------------------------------------------------------- conv lambdas on int / double / float
+    {
+        // the shell of in_shape with integer values in int, double and float properties: the 7-point sums
+        // are exact in every type, so each typed result must equal the host's sum (points that do not
+        // exist, and absent chunks, read the background 0)
+        typedef SparseGridGpu<3, aggregate<int, double, float, int, double, float>, 8> GridM;
+        GridM mg(sz);
+        mg.setBackgroundValue<0>(0);
+        mg.setBackgroundValue<1>(0.0);
+        mg.setBackgroundValue<2>(0.0f);
+        mg.setBackgroundValue<3>(0);
+        mg.setBackgroundValue<4>(0.0);
+        mg.setBackgroundValue<5>(0.0f);
+        auto iv = [](int x, int y, int z) { return (x * 7 + y * 13 + z * 29) % 97; };
+        std::vector<int64_t> mk;
+        for (int bz = 0; bz < N / 8; ++bz)
+            for (int by = 0; by < N / 8; ++by)
+                for (int bx = 0; bx < N / 8; ++bx) {
+                    bool any = false;
+                    for (int o = 0; o < 512 && !any; ++o) any = in_shape(bx * 8 + o % 8, by * 8 + (o / 8) % 8, bz * 8 + o / 64);
+                    if (any) mk.push_back(bx + (N / 8) * (by + (N / 8) * (int64_t)bz));
+                }
+        const int64_t mn = (int64_t)mk.size();
+        std::vector<int> mi((mn + 1) * 512, 0);
+        std::vector<double> md((mn + 1) * 512, 0.0);
+        std::vector<float> mf((mn + 1) * 512, 0.0f);
+        std::vector<uint8_t> mm((mn + 1) * 512, 0);
+        auto coord = [&](int64_t c, int o, int& x, int& y, int& z) {
+            x = (int)(mk[c] % (N / 8)) * 8 + o % 8;
+            y = (int)((mk[c] / (N / 8)) % (N / 8)) * 8 + (o / 8) % 8;
+            z = (int)(mk[c] / (N / 8 * N / 8)) * 8 + o / 64;
+        };
+        for (int64_t c = 0; c < mn; ++c)
+            for (int o = 0; o < 512; ++o) {
+                int x, y, z;
+                coord(c, o, x, y, z);
+                if (!in_shape(x, y, z)) continue;
+                mi[c * 512 + o] = iv(x, y, z);
+                md[c * 512 + o] = iv(x, y, z);
+                mf[c * 512 + o] = (float)iv(x, y, z);
+                mm[c * 512 + o] = 1;
+            }
+        auto load = [&] {
+            const void* d[6] = {mi.data(), md.data(), mf.data(), mi.data(), md.data(), mf.data()};
+            check(sgb_load_map(mg.handle(), mn, mk.data(), d, mm.data(), nullptr), "load_map");
+        };
+        // results at the existing points: the host's sum, in each typed property 3, 4, 5
+        auto verify = [&] {
+            std::vector<int64_t> k(mn);
+            std::vector<int> ri((mn + 1) * 512), di((mn + 1) * 512);
+            std::vector<double> rd((mn + 1) * 512), dd((mn + 1) * 512);
+            std::vector<float> rf((mn + 1) * 512), df((mn + 1) * 512);
+            std::vector<uint8_t> m((mn + 1) * 512);
+            void* ptrs[6] = {di.data(), dd.data(), df.data(), ri.data(), rd.data(), rf.data()};
+            check(sgb_download_map(mg.handle(), k.data(), ptrs, m.data(), nullptr), "download");
+            auto at = [&](int x, int y, int z) {
+                return (x >= 0 && y >= 0 && z >= 0 && x < N && y < N && z < N && in_shape(x, y, z)) ? iv(x, y, z) : 0;
+            };
+            bool ok = k == mk;
+            size_t cnt = 0;
+            for (int64_t c = 0; c < mn && ok; ++c)
+                for (int o = 0; o < 512; ++o) {
+                    if (m[c * 512 + o] != 1) continue;
+                    int x, y, z;
+                    coord(c, o, x, y, z);
+                    const int e = at(x, y, z) + at(x - 1, y, z) + at(x + 1, y, z) + at(x, y - 1, z) + at(x, y + 1, z) +
+                                  at(x, y, z - 1) + at(x, y, z + 1);
+                    const int64_t i = c * 512 + o;
+                    ok = ok && ri[i] == e && rd[i] == (double)e && rf[i] == (float)e;
+                    ++cnt;
+                }
+            return ok && cnt > 0;
+        };
+        const grid_key_dx<3> mlo({0, 0, 0}), mhi({N - 1, N - 1, N - 1});
+        load();
+        mg.conv<0, 3, 1>(mlo, mhi, [] __device__(cp_block<int, 8>& u, int i, int j, int k) {
+            return u(i, j, k) + u(i - 1, j, k) + u(i + 1, j, k) + u(i, j - 1, k) + u(i, j + 1, k) + u(i, j, k - 1) +
+                   u(i, j, k + 1);
+        });
+        mg.conv<1, 4, 1>(mlo, mhi, [] __device__(cp_block<double, 8>& u, int i, int j, int k) {
+            return u(i, j, k) + u(i - 1, j, k) + u(i + 1, j, k) + u(i, j - 1, k) + u(i, j + 1, k) + u(i, j, k - 1) +
+                   u(i, j, k + 1);
+        });
+        mg.conv<2, 5, 1>(mlo, mhi, [] __device__(cp_block<float, 8>& u, int i, int j, int k) {
+            return u(i, j, k) + u(i - 1, j, k) + u(i + 1, j, k) + u(i, j - 1, k) + u(i, j + 1, k) + u(i, j, k - 1) +
+                   u(i, j, k + 1);
+        });
+        cudaDeviceSynchronize();
+        CHECK(verify(), "conv_int_double_float");
+        load();  // properties 3, 4, 5 back to the inputs, which differ from the sums
+        mg.conv3_b<0, 1, 2, 3, 4, 5, 1>(
+            mlo, mhi,
+            [] __device__(int& a, double& b, float& c, cp_block<int, 8>& u, cp_block<double, 8>& v,
+                          cp_block<float, 8>& w, data_block<8>&, int, int i, int j, int k) {
+                a = u(i, j, k) + u(i - 1, j, k) + u(i + 1, j, k) + u(i, j - 1, k) + u(i, j + 1, k) + u(i, j, k - 1) +
+                    u(i, j, k + 1);
+                b = v(i, j, k) + v(i - 1, j, k) + v(i + 1, j, k) + v(i, j - 1, k) + v(i, j + 1, k) + v(i, j, k - 1) +
+                    v(i, j, k + 1);
+                c = w(i, j, k) + w(i - 1, j, k) + w(i + 1, j, k) + w(i, j - 1, k) + w(i, j + 1, k) + w(i, j, k - 1) +
+                    w(i, j, k + 1);
+            });
+        cudaDeviceSynchronize();
+        CHECK(verify(), "conv3_b_int_double_float");
     }
 
     // ---------------------------------------------------------------- user stencil functors
