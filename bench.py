@@ -541,11 +541,15 @@ def run_insert1024(args, dist: Dist):
     torch.cuda.synchronize()
     dist.barrier()
     clk = clocks.stop()
-    step_ms = []
+    step_ms, step_phase_ms = [], []
     for ev in recorded:
+        per = []
         for k, name in enumerate(phases):
-            phases[name] += ev[k].elapsed_time(ev[k + 1]) / 1e3
+            dt = ev[k].elapsed_time(ev[k + 1])
+            phases[name] += dt / 1e3
+            per.append(round(dt, 3))
         step_ms.append(round(ev[0].elapsed_time(ev[4]), 3))
+        step_phase_ms.append(per)
     g.check_device_errors()
     t = dist.max(e0.elapsed_time(e1) / 1e3)
     value = dist.world * npts * nsteps / t / 1e6
@@ -559,6 +563,7 @@ def run_insert1024(args, dist: Dist):
                                    "points_per_step": npts, "chunks_at_end": g.nchunks,
                                    "phase_seconds": {k: round(v, 4) for k, v in phases.items()},
                                    "step_ms": step_ms,
+                                   "step_phase_ms": {"order": list(phases), "steps": step_phase_ms},
                                    "l2": "inputs > L2 (48 MiB of points per step, map > 1 GB)"},
                  roofline=roof, cpu_baseline=None, e2e=None, gpu_launches=None, clocks=clk)
 

@@ -80,7 +80,7 @@ struct DevBuf {
     ~DevBuf() = default;  // owners release explicitly (the grid and batch destructors)
     int reserve(size_t need);   // keeps contents
     int ensure(size_t need);    // may drop contents
-    int grow(size_t need);      // may drop contents; grows to twice the need (for tables that follow a growing map)
+    int grow(size_t need);      // may drop contents; grows to four times the need (tables that follow a growing map)
     // keeps contents; buffers past kInPlaceMinBytes grow in place (no free, no copy, same address) on the
     // current device, smaller ones as reserve()
     int grow_in_place(size_t need);
