@@ -944,6 +944,96 @@ int main() {
         cudaDeviceSynchronize();
         CHECK(verify(), "conv3_b_int_double_float");
     }
+    {
+        // the same sums on 4^3 chunks (64 points a chunk, fewer than a CTA's threads)
+        typedef SparseGridGpu<3, aggregate<float, float, float, float, float, float>, 4> Grid4e;
+        Grid4e eg(sz);
+        eg.setBackgroundValue<0>(0.0f);
+        eg.setBackgroundValue<1>(0.0f);
+        eg.setBackgroundValue<2>(0.0f);
+        eg.setBackgroundValue<3>(0.0f);
+        eg.setBackgroundValue<4>(0.0f);
+        eg.setBackgroundValue<5>(0.0f);
+        auto iv = [](int x, int y, int z) { return (x * 7 + y * 13 + z * 29) % 97; };
+        constexpr int B = N / 4;
+        std::vector<int64_t> ek;
+        for (int bz = 0; bz < B; ++bz)
+            for (int by = 0; by < B; ++by)
+                for (int bx = 0; bx < B; ++bx) {
+                    bool any = false;
+                    for (int o = 0; o < 64 && !any; ++o) any = in_shape(bx * 4 + o % 4, by * 4 + (o / 4) % 4, bz * 4 + o / 16);
+                    if (any) ek.push_back(bx + B * (by + B * (int64_t)bz));
+                }
+        const int64_t en = (int64_t)ek.size();
+        std::vector<float> ev((en + 1) * 64, 0.0f);
+        std::vector<uint8_t> em((en + 1) * 64, 0);
+        auto coord = [&](int64_t c, int o, int& x, int& y, int& z) {
+            x = (int)(ek[c] % B) * 4 + o % 4;
+            y = (int)((ek[c] / B) % B) * 4 + (o / 4) % 4;
+            z = (int)(ek[c] / (B * B)) * 4 + o / 16;
+        };
+        for (int64_t c = 0; c < en; ++c)
+            for (int o = 0; o < 64; ++o) {
+                int x, y, z;
+                coord(c, o, x, y, z);
+                if (!in_shape(x, y, z)) continue;
+                ev[c * 64 + o] = (float)iv(x, y, z);
+                em[c * 64 + o] = 1;
+            }
+        const void* d[6] = {ev.data(), ev.data(), ev.data(), ev.data(), ev.data(), ev.data()};
+        check(sgb_load_map(eg.handle(), en, ek.data(), d, em.data(), nullptr), "load_map");
+        const grid_key_dx<3> elo({0, 0, 0}), ehi({N - 1, N - 1, N - 1});
+        auto at = [&](int x, int y, int z) {
+            return (x >= 0 && y >= 0 && z >= 0 && x < N && y < N && z < N && in_shape(x, y, z)) ? iv(x, y, z) : 0;
+        };
+        // every existing point's results in properties 3, 4, 5 against expected(x, y, z, p)
+        auto verify = [&](auto expected) {
+            std::vector<int64_t> k2(en);
+            std::vector<std::vector<float>> r(6, std::vector<float>((en + 1) * 64));
+            std::vector<uint8_t> m2((en + 1) * 64);
+            void* ptrs[6] = {r[0].data(), r[1].data(), r[2].data(), r[3].data(), r[4].data(), r[5].data()};
+            check(sgb_download_map(eg.handle(), k2.data(), ptrs, m2.data(), nullptr), "download");
+            bool ok = k2 == ek;
+            size_t cnt = 0;
+            for (int64_t c = 0; c < en && ok; ++c)
+                for (int o = 0; o < 64; ++o) {
+                    if (m2[c * 64 + o] != 1) continue;
+                    int x, y, z;
+                    coord(c, o, x, y, z);
+                    for (int p = 3; p < 6; ++p) ok = ok && r[p][c * 64 + o] == (float)expected(x, y, z, p);
+                    ++cnt;
+                }
+            return ok && cnt > 0;
+        };
+        // conv3_b: three different reads of the three (equal) source fields
+        eg.conv3_b<0, 1, 2, 3, 4, 5, 1>(
+            elo, ehi,
+            [] __device__(float& a, float& b, float& c, cp_block<float, 4>& u, cp_block<float, 4>& v,
+                          cp_block<float, 4>& w, data_block<8>&, int, int i, int j, int k) {
+                a = u(i + 1, j, k) + u(i, j + 1, k) + u(i, j, k + 1);
+                b = v(i - 1, j, k) + v(i, j - 1, k) + v(i, j, k - 1);
+                c = w(i, j, k);
+            });
+        cudaDeviceSynchronize();
+        const bool ok3 = verify([&](int x, int y, int z, int p) {
+            return p == 3 ? at(x + 1, y, z) + at(x, y + 1, z) + at(x, y, z + 1)
+                 : p == 4 ? at(x - 1, y, z) + at(x, y - 1, z) + at(x, y, z - 1)
+                          : at(x, y, z);
+        });
+        // conv: the 7-point sum into property 3, the others unchanged
+        eg.conv<0, 3, 1>(elo, ehi, [] __device__(cp_block<float, 4>& u, int i, int j, int k) {
+            return u(i, j, k) + u(i - 1, j, k) + u(i + 1, j, k) + u(i, j - 1, k) + u(i, j + 1, k) + u(i, j, k - 1) +
+                   u(i, j, k + 1);
+        });
+        cudaDeviceSynchronize();
+        const bool ok1 = verify([&](int x, int y, int z, int p) {
+            return p == 3 ? at(x, y, z) + at(x - 1, y, z) + at(x + 1, y, z) + at(x, y - 1, z) + at(x, y + 1, z) +
+                                at(x, y, z - 1) + at(x, y, z + 1)
+                 : p == 4 ? at(x - 1, y, z) + at(x, y - 1, z) + at(x, y, z - 1)
+                          : at(x, y, z);
+        });
+        CHECK(ok3 && ok1, "conv_and_conv3_b_on_4x4x4_chunks");
+    }
 
     // ---------------------------------------------------------------- user stencil functors
     {
