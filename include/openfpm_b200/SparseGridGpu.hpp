@@ -384,16 +384,7 @@ __device__ __forceinline__ void async_wait_group() {
     asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
-// Conv kernel for user lambdas: each CTA takes chunks blockIdx.x, + gridDim.x, ... and keeps two
-// halo tiles per source field in shared memory (tile_layout).  While one chunk is computed from one
-// tile, the next chunk's tile is gathered into the other by cp.async copies, row by row: the E
-// interior elements of a row in 16-byte copies from the chunk the row lies in (the chunk itself, a
-// face neighbour, or for rows along a halo edge the edge neighbour under NNFull and neighbour 0, the
-// -x chunk, at the wrapped coordinate under NNStar, as the reference's ghost-layer map gives them),
-// the two x-halo elements one by one.  Absent chunks give the background.  One barrier per chunk:
-// a thread waits for its own copies of the chunk, the barrier makes every thread's copies visible
-// and closes the reads of the other tile, and only then is the next chunk's gather issued.  The
-// lambda runs for every active point inside the box (conv_cross writes every point of the chunk).
+// 16-byte cp.async copy into shared memory (both addresses 16-byte aligned)
 template <typename T>
 __device__ __forceinline__ void async_copy16(T* dst_smem, const T* src) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((unsigned)__cvta_generic_to_shared(dst_smem)),
@@ -489,6 +480,17 @@ struct tile_plan {
 // instructions on the per-chunk work, and more registers per thread keep more points in flight)
 constexpr int kConvThreads = 64;
 
+// Conv kernel for user lambdas, over up to three source fields (NP) of any types: each CTA (two warps,
+// eight points a thread in 8^3 chunks) takes chunks blockIdx.x, + gridDim.x, ... and keeps two halo
+// tiles per source field in shared memory (tile_layout).  While one chunk is computed from one tile,
+// the next chunk's tile is gathered into the other by cp.async copies, row by row: the E interior
+// elements of a row in 16-byte copies from the chunk the row lies in (the chunk itself, a face
+// neighbour, or for rows along a halo edge the edge neighbour under NNFull and neighbour 0, the -x
+// chunk, at the wrapped coordinate under NNStar, as the reference's ghost-layer map gives them), the
+// two x-halo elements one by one.  Absent chunks give the background.  One barrier per chunk: a thread
+// waits for its own copies of the chunk, the barrier makes every thread's copies visible and closes the
+// reads of the other tile, and only then is the next chunk's gather issued.  The lambda runs for every
+// active point inside the box (conv_cross writes every point of the chunk).
 template <int E, int NP, int MODE, typename T0, typename T1, typename T2, typename U0, typename U1, typename U2,
           typename F>
 __global__ void __launch_bounds__(kConvThreads, 8)
